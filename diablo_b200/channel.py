@@ -1,0 +1,239 @@
+"""ctypes binding of libdiablo_gpu.so and the host-side time loop.
+
+`Channel` is the host mirror of the reference's channel solver: it owns the
+/RUNTIME_VARS/ and /RKW3_PARAMS/ scalars (TIME, TIME_STEP, DELTA_T, H_BAR,
+BETA_BAR, ZETA_BAR) like the Fortran host does and calls the library's C ABI
+for everything that runs on the GPU.  Method names follow the reference
+routines they replace.  There is no CPU fallback: a missing or unloadable
+library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .grid import ChannelGrid
+from .layout import new_fourier, physical_shape, fourier_shape
+from .params import DiabloParams, validate
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdiablo_gpu.so")
+
+DIABLO_OK, DIABLO_EINVAL, DIABLO_ERADIX, DIABLO_ECUDA, DIABLO_ENOTSUP, DIABLO_ENAN, DIABLO_ENOMEM = (
+    0, -1, -2, -3, -4, -5, -6)
+NSTATS = 17
+
+# C entry points declared in include/diablo_gpu.h
+EXPORTS = [
+    "diablo_gpu_create", "diablo_gpu_destroy", "diablo_gpu_upload_state", "diablo_gpu_download_state",
+    "diablo_gpu_rk_chan_1", "diablo_gpu_rk_chan_2", "diablo_gpu_fft_xz_to_fourier",
+    "diablo_gpu_fft_xz_to_physical", "diablo_gpu_rem_div_chan", "diablo_gpu_download_phi",
+    "diablo_gpu_poisson_p_chan", "diablo_gpu_apply_bc_vel", "diablo_gpu_courant", "diablo_gpu_stats",
+    "diablo_gpu_synchronize", "diablo_gpu_kernel_launches", "diablo_gpu_last_error",
+]
+
+
+class DiabloError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what} failed with status {code}: {last_error()}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m diablo_b200.build`")
+    L = ctypes.CDLL(path)
+    vp, dp, ip, dd = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double
+    L.diablo_gpu_create.argtypes = [ctypes.POINTER(DiabloParams), dp, dp, dp, dp, ctypes.POINTER(vp)]
+    L.diablo_gpu_destroy.argtypes = [vp]
+    L.diablo_gpu_upload_state.argtypes = [vp] + [dp] * 9
+    L.diablo_gpu_download_state.argtypes = [vp] + [dp] * 9
+    L.diablo_gpu_rk_chan_1.argtypes = [vp, ip, ip, dd, dp, dp, dp, dp]
+    L.diablo_gpu_rk_chan_2.argtypes = [vp]
+    L.diablo_gpu_fft_xz_to_fourier.argtypes = [vp, dp, dp, ip, ip]
+    L.diablo_gpu_fft_xz_to_physical.argtypes = [vp, dp, dp, ip, ip]
+    for name in ("diablo_gpu_rem_div_chan", "diablo_gpu_poisson_p_chan", "diablo_gpu_apply_bc_vel",
+                 "diablo_gpu_synchronize"):
+        getattr(L, name).argtypes = [vp]
+    L.diablo_gpu_download_phi.argtypes = [vp, dp]
+    L.diablo_gpu_courant.argtypes = [vp, dp, dp]
+    L.diablo_gpu_stats.argtypes = [vp, dp]
+    L.diablo_gpu_kernel_launches.argtypes = [vp]
+    L.diablo_gpu_kernel_launches.restype = ctypes.c_longlong
+    L.diablo_gpu_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    if _lib is None:
+        return ""
+    return (_lib.diablo_gpu_last_error() or b"").decode()
+
+
+def _dp(a: np.ndarray | None):
+    if a is None:
+        return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("host arrays must be C-contiguous (Fortran layout viewed in C order)")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != DIABLO_OK:
+        raise DiabloError(rc, what)
+
+
+class Channel:
+    """One channel instance on the current GPU (one library handle)."""
+
+    def __init__(self, p: DiabloParams, grid: ChannelGrid, delta_t: float):
+        validate(p)
+        self.L = load_library()
+        self.p = p.copy()
+        self.grid = grid
+        self._h = ctypes.c_void_p()
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (grid.gy, grid.gyf, grid.dy, grid.dyf)]
+        _check(self.L.diablo_gpu_create(ctypes.byref(self.p), *[_dp(a) for a in arrs], ctypes.byref(self._h)),
+               "diablo_gpu_create")
+        # /RUNTIME_VARS/ and /RKW3_PARAMS/ (diablo_io.f:116-124)
+        self.time = 0.0
+        self.time_step = 0
+        self.delta_t = float(delta_t)
+        self.h_bar = np.array([delta_t * 8.0 / 15.0, delta_t * 2.0 / 15.0, delta_t * 5.0 / 15.0])
+        self.beta_bar = np.array([1.0, 25.0 / 8.0, 9.0 / 4.0])
+        self.zeta_bar = np.array([0.0, -17.0 / 8.0, -5.0 / 4.0])
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self.L.diablo_gpu_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- state transfer ----------------------------------------------------
+    def upload(self, cu: list[np.ndarray], cp: np.ndarray, cth: np.ndarray | None,
+               cf: list[np.ndarray] | None = None, cfth: np.ndarray | None = None) -> None:
+        def f64(a):
+            return None if a is None else np.ascontiguousarray(a).view(np.float64)
+        cfl = cf or [None, None, None]
+        _check(self.L.diablo_gpu_upload_state(
+            self._h, _dp(f64(cu[0])), _dp(f64(cu[1])), _dp(f64(cu[2])), _dp(f64(cp)),
+            _dp(f64(cth)) if self.p.n_th else None,
+            _dp(f64(cfl[0])), _dp(f64(cfl[1])), _dp(f64(cfl[2])),
+            _dp(f64(cfth)) if (cfth is not None and self.p.n_th) else None), "diablo_gpu_upload_state")
+
+    def download(self) -> dict:
+        p = self.p
+        out = {
+            "cu": [new_fourier(p) for _ in range(3)],
+            "cp": new_fourier(p),
+            "cth": new_fourier(p, max(p.n_th, 1)),
+            "cf": [new_fourier(p) for _ in range(3)],
+            "cfth": new_fourier(p, max(p.n_th, 1)),
+        }
+        v = lambda a: _dp(a.view(np.float64))
+        _check(self.L.diablo_gpu_download_state(
+            self._h, v(out["cu"][0]), v(out["cu"][1]), v(out["cu"][2]), v(out["cp"]), v(out["cth"]),
+            v(out["cf"][0]), v(out["cf"][1]), v(out["cf"][2]), v(out["cfth"])), "diablo_gpu_download_state")
+        out["cth"] = out["cth"][: p.n_th]
+        out["cfth"] = out["cfth"][: p.n_th]
+        return out
+
+    def download_phi(self) -> np.ndarray:
+        phi = new_fourier(self.p)
+        _check(self.L.diablo_gpu_download_phi(self._h, _dp(phi.view(np.float64))), "diablo_gpu_download_phi")
+        return phi
+
+    # --- routines of the reference ------------------------------------------
+    def rk_chan_1(self, rk_step: int) -> None:
+        """One RK substage (RK_CHAN_1); DELTA_T/H_BAR change if COURANT ran."""
+        dt = ctypes.c_double(self.delta_t)
+        hb = np.ascontiguousarray(self.h_bar, dtype=np.float64)
+        _check(self.L.diablo_gpu_rk_chan_1(self._h, rk_step, self.time_step, self.time, ctypes.byref(dt),
+                                           _dp(hb), _dp(self.beta_bar), _dp(self.zeta_bar)),
+               "diablo_gpu_rk_chan_1")
+        self.delta_t = dt.value
+        self.h_bar = hb
+
+    def rk_chan_2(self) -> None:
+        _check(self.L.diablo_gpu_rk_chan_2(self._h), "diablo_gpu_rk_chan_2")
+
+    def step(self, n: int = 1) -> None:
+        """n time steps of the loop in diablo.f:66-111 (no statistics or I/O)."""
+        for _ in range(n):
+            self.time_step += 1
+            for rk in (1, 2, 3):
+                self.rk_chan_1(rk)
+            self.time += self.delta_t
+
+    def synchronize(self) -> None:
+        _check(self.L.diablo_gpu_synchronize(self._h), "diablo_gpu_synchronize")
+
+    def rem_div_chan(self) -> None:
+        _check(self.L.diablo_gpu_rem_div_chan(self._h), "diablo_gpu_rem_div_chan")
+
+    def poisson_p_chan(self) -> None:
+        _check(self.L.diablo_gpu_poisson_p_chan(self._h), "diablo_gpu_poisson_p_chan")
+
+    def apply_bc_vel(self) -> None:
+        _check(self.L.diablo_gpu_apply_bc_vel(self._h), "diablo_gpu_apply_bc_vel")
+
+    def courant(self) -> None:
+        dt = ctypes.c_double(self.delta_t)
+        hb = np.zeros(3)
+        _check(self.L.diablo_gpu_courant(self._h, ctypes.byref(dt), _dp(hb)), "diablo_gpu_courant")
+        self.delta_t = dt.value
+        self.h_bar = hb
+
+    def stats(self) -> np.ndarray:
+        out = np.zeros((NSTATS, self.p.ny + 2))
+        _check(self.L.diablo_gpu_stats(self._h, _dp(out)), "diablo_gpu_stats")
+        return out
+
+    def fft_xz_to_fourier(self, v: np.ndarray, vv: np.ndarray, jmin: int, jmax: int) -> None:
+        assert v.shape[-3:] == physical_shape(self.p) and vv.shape[-3:] == fourier_shape(self.p)
+        _check(self.L.diablo_gpu_fft_xz_to_fourier(self._h, _dp(v), _dp(vv.view(np.float64)), jmin, jmax),
+               "diablo_gpu_fft_xz_to_fourier")
+
+    def fft_xz_to_physical(self, vv: np.ndarray, v: np.ndarray, jmin: int, jmax: int) -> None:
+        assert v.shape[-3:] == physical_shape(self.p) and vv.shape[-3:] == fourier_shape(self.p)
+        _check(self.L.diablo_gpu_fft_xz_to_physical(self._h, _dp(vv.view(np.float64)), _dp(v), jmin, jmax),
+               "diablo_gpu_fft_xz_to_physical")
+
+    def kernel_launches(self) -> int:
+        return int(self.L.diablo_gpu_kernel_launches(self._h))
+
+    # --- initial condition (CREATE_TH_CHAN then CREATE_FLOW_CHAN) ------------
+    def init_from_physical(self, u: np.ndarray, th: np.ndarray) -> None:
+        """Transform physical fields with this library, upload with CP = CF = 0,
+        then APPLY_BC_VEL and REM_DIV_CHAN (set_ics.f:125-183, 265-268)."""
+        p = self.p
+        cu = [new_fourier(p) for _ in range(3)]
+        for c in range(3):
+            self.fft_xz_to_fourier(np.ascontiguousarray(u[c]), cu[c], 0, p.ny + 1)
+        cth = new_fourier(p, max(p.n_th, 1))
+        for n in range(p.n_th):
+            self.fft_xz_to_fourier(np.ascontiguousarray(th[n]), cth[n], 0, p.ny + 1)
+        self.upload(cu, new_fourier(p), cth)
+        self.apply_bc_vel()
+        self.rem_div_chan()

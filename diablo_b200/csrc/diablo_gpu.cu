@@ -1,0 +1,656 @@
+// diablo_gpu.cu -- the C ABI (include/diablo_gpu.h): handle, device state,
+// host <-> device layout conversion and the RK_CHAN_1 substage pipeline.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/diablo_gpu.h"
+#include "fft.cuh"
+#include "kernels.cuh"
+#include "launch.h"
+
+using namespace dgpu;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                            \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(DIABLO_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct Handle {
+    diablo_params p;
+    Dims d;
+    int nxp;
+    int jstart, jend, jstart_th[DIABLO_MAX_TH], jend_th[DIABLO_MAX_TH];
+    int jlo_prod;
+    double dx, dz, pi;
+    std::vector<double> gy, gyf, dy, dyf;
+    bool fp32;
+    cudaStream_t st = nullptr;
+    size_t s_plane, s_field;      // elements
+    size_t x_plane, x_field;      // elements
+    // device memory
+    double *d_dy = nullptr, *d_dyf = nullptr, *d_kx = nullptr, *d_kz = nullptr;
+    double2 *cu = nullptr, *cf = nullptr, *cp = nullptr, *phi = nullptr, *api_s = nullptr;
+    void *nl = nullptr, *xb = nullptr, *yb = nullptr;
+    double* bsc = nullptr;
+    double2* gsc = nullptr;
+    double* phys = nullptr;
+    double *mult = nullptr, *piv = nullptr, *cup = nullptr, *bcv = nullptr;
+    signed char* kind = nullptr;
+    double* dtmin = nullptr;
+    FftPlan px, pz;
+    void *twx_d = nullptr, *twz_d = nullptr, *twx_f = nullptr, *twz_f = nullptr;
+    int bc_type[2 * MAXF];
+    double bc_c1[2 * MAXF];
+    long long launches = 0;
+};
+
+bool is_235(int n) {
+    if (n < 2) return false;
+    for (int r : {2, 3, 5})
+        while (n % r == 0) n /= r;
+    return n == 1;
+}
+
+template <typename T>
+void* make_twiddles(int n, cudaError_t* err) {
+    std::vector<T> h(2 * (size_t)n);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < n; ++k) {
+        // angle reduced to the first octant for an accurate table
+        const long double a = -2.0L * pi * (long double)k / (long double)n;
+        h[2 * k] = (T)cosl(a);
+        h[2 * k + 1] = (T)sinl(a);
+    }
+    void* d = nullptr;
+    *err = cudaMalloc(&d, sizeof(T) * h.size());
+    if (*err == cudaSuccess) *err = cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
+    return d;
+}
+
+void free_handle(Handle* h) {
+    if (!h) return;
+    void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
+                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->mult, h->piv, h->cup,
+                    h->bcv, h->kind, h->dtmin, h->twx_d, h->twz_d, h->twx_f, h->twz_f};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+// Host Fortran complex array (0:NXP,0:NZ+1,0:NY+1) <-> device spectral field.
+cudaError_t copy_fourier(Handle* h, double2* dev, const double* host_in, double* host_out, int j0,
+                         int nplanes) {
+    const Dims& d = h->d;
+    cudaMemcpy3DParms c = {};
+    const size_t hpitch = sizeof(double2) * (size_t)(h->nxp + 1);
+    const size_t dpitch = sizeof(double2) * (size_t)d.ldx;
+    cudaPitchedPtr hp = make_cudaPitchedPtr((void*)(host_in ? host_in : host_out), hpitch,
+                                            (size_t)(h->nxp + 1), (size_t)(d.nz + 2));
+    cudaPitchedPtr dp = make_cudaPitchedPtr((void*)dev, dpitch, (size_t)d.ldx, (size_t)d.nkzt);
+    c.extent = make_cudaExtent(sizeof(double2) * (size_t)d.nkxp, (size_t)d.nkzt, (size_t)nplanes);
+    if (host_in) {
+        c.srcPtr = hp; c.dstPtr = dp;
+        c.srcPos = make_cudaPos(0, 0, j0); c.dstPos = make_cudaPos(0, 0, j0);
+        c.kind = cudaMemcpyHostToDevice;
+    } else {
+        c.srcPtr = dp; c.dstPtr = hp;
+        c.srcPos = make_cudaPos(0, 0, j0); c.dstPos = make_cudaPos(0, 0, j0);
+        c.kind = cudaMemcpyDeviceToHost;
+    }
+    return cudaMemcpy3DAsync(&c, h->st);
+}
+
+// Host Fortran physical array (0:NX+1,0:NZ+1,0:NY+1) <-> device P[J][z][x].
+cudaError_t copy_physical(Handle* h, double* dev, const double* host_in, double* host_out, int j0,
+                          int nplanes) {
+    const Dims& d = h->d;
+    cudaMemcpy3DParms c = {};
+    cudaPitchedPtr hp = make_cudaPitchedPtr((void*)(host_in ? host_in : host_out),
+                                            sizeof(double) * (size_t)(d.nx + 2), (size_t)(d.nx + 2),
+                                            (size_t)(d.nz + 2));
+    cudaPitchedPtr dp = make_cudaPitchedPtr((void*)dev, sizeof(double) * (size_t)d.nx, (size_t)d.nx,
+                                            (size_t)d.nz);
+    c.extent = make_cudaExtent(sizeof(double) * (size_t)d.nx, (size_t)d.nz, (size_t)nplanes);
+    c.srcPos = make_cudaPos(0, 0, j0);
+    c.dstPos = make_cudaPos(0, 0, j0);
+    if (host_in) { c.srcPtr = hp; c.dstPtr = dp; c.kind = cudaMemcpyHostToDevice; }
+    else { c.srcPtr = dp; c.dstPtr = hp; c.kind = cudaMemcpyDeviceToHost; }
+    return cudaMemcpy3DAsync(&c, h->st);
+}
+
+// APPLY_BC_VEL_LOWER / _UPPER (channel.f:2285-2492) on the device state.
+__global__ void k_apply_bc_vel(Dims d, double2* cu, const double* dy, const double* dyf, diablo_params p) {
+    const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    if (kx >= d.nkxp || m >= d.nkzt) return;
+    const size_t ps = (size_t)d.nkzt * d.ldx, fs = ps * d.nyp, col = (size_t)m * d.ldx + kx;
+    const bool z0 = (kx == 0 && m == 0);
+    const int ny = d.ny;
+    double2* u1 = cu + col;
+    double2* u2 = cu + fs + col;
+    double2* u3 = cu + 2 * fs + col;
+    const double2 zero = make_double2(0, 0);
+    auto at = [&](double2* f, int j) -> double2& { return f[(size_t)j * ps]; };
+    // lower wall
+    if (p.u_bc_ymin == 0) {
+        at(u1, 0) = zero; at(u1, 1) = zero;
+        if (z0) { at(u1, 1) = make_double2(p.u_bc_ymin_c1, 0); at(u1, 0) = make_double2(p.u_bc_ymin_c1, 0); }
+    } else {
+        at(u1, 1) = at(u1, 2); at(u1, 0) = at(u1, 1);
+        if (z0) {
+            at(u1, 1).x = at(u1, 2).x - dy[2] * p.u_bc_ymin_c1;
+            at(u1, 0).x = at(u1, 1).x - dy[1] * p.u_bc_ymin_c1;
+        }
+    }
+    if (p.w_bc_ymin == 0) {
+        at(u3, 0) = zero; at(u3, 1) = zero;
+        if (z0) { at(u3, 1) = make_double2(p.w_bc_ymin_c1, 0); at(u3, 0) = make_double2(p.w_bc_ymin_c1, 0); }
+    } else {
+        at(u3, 1) = at(u3, 2); at(u3, 0) = at(u3, 1);
+        if (z0) {
+            at(u3, 1).x = at(u3, 2).x - dy[2] * p.w_bc_ymin_c1;
+            at(u3, 0).x = at(u3, 1).x - dy[1] * p.w_bc_ymin_c1;
+        }
+    }
+    if (p.v_bc_ymin == 0) {
+        const double2 v2 = at(u2, 2);
+        at(u2, 1) = make_double2(2.0 * p.v_bc_ymin_c1 - v2.x, -v2.y);
+        at(u2, 0) = at(u2, 1);
+    } else if (p.v_bc_ymin == 1) {
+        at(u2, 1) = at(u2, 2); at(u2, 0) = at(u2, 1);
+        if (z0) {
+            at(u2, 1).x = at(u2, 2).x - dyf[1] * p.v_bc_ymin_c1;
+            at(u2, 0).x = at(u2, 1).x - dyf[1] * p.v_bc_ymin_c1;
+        }
+    }
+    // upper wall
+    if (p.u_bc_ymax == 0) {
+        at(u1, ny) = zero; at(u1, ny + 1) = zero;
+        if (z0) { at(u1, ny) = make_double2(p.u_bc_ymax_c1, 0); at(u1, ny + 1) = make_double2(p.u_bc_ymax_c1, 0); }
+    } else {
+        at(u1, ny) = at(u1, ny - 1); at(u1, ny + 1) = at(u1, ny);
+        if (z0) {
+            at(u1, ny).x = at(u1, ny - 1).x + dy[ny] * p.u_bc_ymax_c1;
+            at(u1, ny + 1).x = at(u1, ny).x + dy[ny] * p.u_bc_ymax_c1;
+        }
+    }
+    if (p.w_bc_ymax == 0) {
+        at(u3, ny) = zero; at(u3, ny + 1) = zero;
+        if (z0) { at(u3, ny) = make_double2(p.w_bc_ymax_c1, 0); at(u3, ny + 1) = zero; }
+    } else {
+        at(u3, ny) = at(u3, ny - 1); at(u3, ny + 1) = at(u3, ny);
+        if (z0) {
+            at(u3, ny).x = at(u3, ny - 1).x + dy[ny] * p.w_bc_ymax_c1;
+            at(u3, ny + 1).x = at(u3, ny).x + dy[ny] * p.w_bc_ymax_c1;
+        }
+    }
+    if (p.v_bc_ymax == 0) {
+        // only the (0,0) entry is written by the reference (channel.f:2463-2467)
+        if (z0) {
+            const double2 v = at(u2, ny);
+            at(u2, ny + 1) = make_double2(2.0 * p.v_bc_ymax_c1 - v.x, -v.y);
+        }
+    } else if (p.v_bc_ymax == 1) {
+        at(u2, ny) = at(u2, ny - 1); at(u2, ny + 1) = at(u2, ny);
+        if (z0) at(u2, ny + 1).x = at(u2, ny).x + dy[ny] * p.v_bc_ymax_c1;
+    }
+}
+
+int validate(const diablo_params* p) {
+    if (!p) return fail(DIABLO_EINVAL, "null params");
+    if (p->nx < 8 || p->nz < 8 || (p->nx % 2)) return fail(DIABLO_EINVAL, "NX and NZ must be >= 8, NX even");
+    if (!is_235(p->nx) || !is_235(p->nz)) return fail(DIABLO_ERADIX, "NX and NZ must be products of 2, 3 and 5");
+    if (p->nx > 1536 || p->nz > 512) return fail(DIABLO_EINVAL, "NX <= 1536 and NZ <= 512 are supported");
+    if (p->ny < 4) return fail(DIABLO_EINVAL, "NY must be >= 4");
+    if (p->n_th < 0 || p->n_th > DIABLO_MAX_TH) return fail(DIABLO_EINVAL, "N_TH must be in 0..4");
+    if (p->les) return fail(DIABLO_ENOTSUP, "LES is not supported");
+    auto bc01 = [](int t) { return t == 0 || t == 1; };
+    if (!bc01(p->u_bc_ymin) || !bc01(p->u_bc_ymax) || !bc01(p->w_bc_ymin) || !bc01(p->w_bc_ymax) ||
+        !bc01(p->v_bc_ymin) || !bc01(p->v_bc_ymax))
+        return fail(DIABLO_EINVAL, "velocity BC types must be 0 (Dirichlet) or 1 (Neumann)");
+    for (int n = 0; n < p->n_th; ++n) {
+        if (!bc01(p->th_bc_ymin[n]) || !bc01(p->th_bc_ymax[n]))
+            return fail(DIABLO_EINVAL, "scalar BC types must be 0 or 1");
+        if (p->pr[n] == 0.0) return fail(DIABLO_EINVAL, "PR must be non-zero");
+    }
+    if (p->precision != DIABLO_PREC_FP64 && p->precision != DIABLO_PREC_FP32SPLIT)
+        return fail(DIABLO_EINVAL, "precision must be DIABLO_PREC_FP64 or DIABLO_PREC_FP32SPLIT");
+    if (p->variable_dt && p->update_dt <= 0) return fail(DIABLO_EINVAL, "UPDATE_DT must be > 0");
+    return DIABLO_OK;
+}
+
+int fp32_limits(const Handle* h) {
+    // shared memory and register budgets of the transform kernels
+    const int npair_in = (h->d.nf + 1) / 2;
+    int group = (12 * 256) / h->d.nx;
+    if (group > 6) group = 6;
+    if (npair_in > group) return fail(DIABLO_EINVAL, "too many fields for NX");
+    return DIABLO_OK;
+}
+
+template <typename T>
+int run_transforms(Handle* h) {
+    const Dims& d = h->d;
+    const void* twx = std::is_same<T, float>::value ? h->twx_f : h->twx_d;
+    const void* twz = std::is_same<T, float>::value ? h->twz_f : h->twz_d;
+    CK(launch_zinv<T>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, twz, h->st));
+    CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, 32, h->d_dy, h->d_dyf, h->px, twx, h->st));
+    CK(launch_zfwd_nl<T>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->d_kx, h->d_kz, h->pz, twz, h->st));
+    h->launches += 3;
+    return DIABLO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* diablo_gpu_last_error(void) { return g_err.c_str(); }
+
+int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gyf, const double* dy,
+                      const double* dyf, void** handle) {
+    if (!handle || !gy || !gyf || !dy || !dyf) return fail(DIABLO_EINVAL, "null pointer argument");
+    *handle = nullptr;
+    int rc = validate(p);
+    if (rc) return rc;
+    Handle* h = new Handle();
+    h->p = *p;
+    Dims& d = h->d;
+    d.nx = p->nx; d.ny = p->ny; d.nz = p->nz; d.nth = p->n_th;
+    d.nf = 3 + p->n_th;
+    d.np = 8 + 3 * p->n_th;
+    d.nkx = p->nx / 3; d.nkz = p->nz / 3; d.tnkz = 2 * d.nkz;
+    d.nkxp = d.nkx + 1; d.nkzt = d.tnkz + 1;
+    d.ldx = (d.nkxp + 15) / 16 * 16;
+    d.nyp = p->ny + 2;
+    h->nxp = p->nx / 2;
+    h->fp32 = p->precision == DIABLO_PREC_FP32SPLIT;
+    h->pi = 4.0 * std::atan(1.0);
+    h->dx = p->lx / p->nx;
+    h->dz = p->lz / p->nz;
+    h->gy.assign(gy, gy + d.nyp);
+    h->gyf.assign(gyf, gyf + d.nyp);
+    h->dy.assign(dy, dy + d.nyp);
+    h->dyf.assign(dyf, dyf + d.nyp);
+    // INIT_CHAN_MPI, RANKY = 0 branch (mpi.f:1024-1044)
+    h->jstart = 2;
+    h->jend = p->ny;
+    h->jlo_prod = 2;
+    for (int n = 0; n < p->n_th; ++n) {
+        h->jend_th[n] = p->ny;
+        h->jstart_th[n] = p->th_bc_ymin[n] == 1 ? 1 : 2;
+        if (h->jstart_th[n] < h->jlo_prod) h->jlo_prod = h->jstart_th[n];
+    }
+    if ((rc = fp32_limits(h))) { delete h; return rc; }
+    if (!make_plan(d.nx, &h->px) || !make_plan(d.nz, &h->pz)) { delete h; return fail(DIABLO_ERADIX, "bad radix"); }
+    // BC table: [field][lower, upper]
+    for (int f = 0; f < 2 * MAXF; ++f) { h->bc_type[f] = 0; h->bc_c1[f] = 0.0; }
+    h->bc_type[0] = p->u_bc_ymin; h->bc_type[1] = p->u_bc_ymax;
+    h->bc_c1[0] = p->u_bc_ymin_c1; h->bc_c1[1] = p->u_bc_ymax_c1;
+    h->bc_type[2] = p->v_bc_ymin; h->bc_type[3] = p->v_bc_ymax;
+    h->bc_c1[2] = p->v_bc_ymin_c1; h->bc_c1[3] = p->v_bc_ymax_c1;
+    h->bc_type[4] = p->w_bc_ymin; h->bc_type[5] = p->w_bc_ymax;
+    h->bc_c1[4] = p->w_bc_ymin_c1; h->bc_c1[5] = p->w_bc_ymax_c1;
+    for (int n = 0; n < p->n_th; ++n) {
+        h->bc_type[2 * (3 + n)] = p->th_bc_ymin[n]; h->bc_type[2 * (3 + n) + 1] = p->th_bc_ymax[n];
+        h->bc_c1[2 * (3 + n)] = p->th_bc_ymin_c1[n]; h->bc_c1[2 * (3 + n) + 1] = p->th_bc_ymax_c1[n];
+    }
+
+    h->s_plane = (size_t)d.nkzt * d.ldx;
+    h->s_field = h->s_plane * d.nyp;
+    h->x_plane = (size_t)d.nz * d.ldx;
+    h->x_field = h->x_plane * d.nyp;
+    auto dmalloc = [&](void** ptr, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(ptr, bytes);
+        if (e == cudaSuccess) e = cudaMemset(*ptr, 0, bytes);
+        return e;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+    const size_t sb = sizeof(double2) * h->s_field;
+    const size_t nyp = (size_t)d.nyp;
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_dy, sizeof(double) * nyp);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_dyf, sizeof(double) * nyp);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_kx, sizeof(double) * d.ldx);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_kz, sizeof(double) * d.nkzt);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->cu, sb * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->cf, sb * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->cp, sb);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->phi, sb);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->api_s, sb);
+    if (e == cudaSuccess) e = dmalloc(&h->nl, sb * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->bsc, sizeof(double) * h->s_field);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->gsc, sb);
+    if (e == cudaSuccess) e = dmalloc(&h->xb, sizeof(double2) * h->x_field * d.nf);
+    if (e == cudaSuccess) e = dmalloc(&h->yb, sizeof(double2) * h->x_field * d.np);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->mult, sizeof(double) * nyp * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->piv, sizeof(double) * nyp * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->cup, sizeof(double) * nyp * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->bcv, sizeof(double) * nyp * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->kind, nyp * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->dtmin, sizeof(double));
+    if (e != cudaSuccess) {
+        free_handle(h);
+        return fail(e == cudaErrorMemoryAllocation ? DIABLO_ENOMEM : DIABLO_ECUDA,
+                    std::string("device set-up: ") + cudaGetErrorString(e));
+    }
+    // wavenumbers (fft.f:77-100)
+    std::vector<double> kx(d.ldx, 0.0), kz(d.nkzt, 0.0);
+    for (int i = 0; i <= d.nkx; ++i) kx[i] = (double)i * (2.0 * h->pi) / p->lx;
+    for (int k = 0; k <= d.nkz; ++k) kz[k] = (double)k * (2.0 * h->pi) / p->lz;
+    for (int k = 1; k <= d.nkz; ++k) kz[d.tnkz + 1 - k] = -(double)k * (2.0 * h->pi) / p->lz;
+    e = cudaMemcpy(h->d_kx, kx.data(), sizeof(double) * d.ldx, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_kz, kz.data(), sizeof(double) * d.nkzt, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_dy, dy, sizeof(double) * nyp, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_dyf, dyf, sizeof(double) * nyp, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) h->twx_d = make_twiddles<double>(d.nx, &e);
+    if (e == cudaSuccess) h->twz_d = make_twiddles<double>(d.nz, &e);
+    if (e == cudaSuccess) h->twx_f = make_twiddles<float>(d.nx, &e);
+    if (e == cudaSuccess) h->twz_f = make_twiddles<float>(d.nz, &e);
+    if (e != cudaSuccess) {
+        free_handle(h);
+        return fail(DIABLO_ECUDA, std::string("device set-up: ") + cudaGetErrorString(e));
+    }
+    *handle = h;
+    return DIABLO_OK;
+}
+
+int diablo_gpu_destroy(void* handle) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    cudaStreamSynchronize(h->st);
+    free_handle(h);
+    return DIABLO_OK;
+}
+
+int diablo_gpu_upload_state(void* handle, const double* cu1, const double* cu2, const double* cu3,
+                            const double* cp, const double* cth, const double* cf1, const double* cf2,
+                            const double* cf3, const double* cfth) {
+    Handle* h = (Handle*)handle;
+    if (!h || !cu1 || !cu2 || !cu3 || !cp || (h->d.nth > 0 && !cth))
+        return fail(DIABLO_EINVAL, "null pointer argument");
+    const Dims& d = h->d;
+    const size_t fstride = (size_t)(h->nxp + 1) * (d.nz + 2) * d.nyp * 2;   // doubles per host field
+    const double* cus[3] = {cu1, cu2, cu3};
+    for (int f = 0; f < 3; ++f) CK(copy_fourier(h, h->cu + f * h->s_field, cus[f], nullptr, 0, d.nyp));
+    for (int n = 0; n < d.nth; ++n)
+        CK(copy_fourier(h, h->cu + (3 + n) * h->s_field, cth + n * fstride, nullptr, 0, d.nyp));
+    CK(copy_fourier(h, h->cp, cp, nullptr, 0, d.nyp));
+    const double* cfs[3] = {cf1, cf2, cf3};
+    for (int f = 0; f < 3; ++f) {
+        if (cfs[f]) CK(copy_fourier(h, h->cf + f * h->s_field, cfs[f], nullptr, 0, d.nyp));
+        else CK(cudaMemsetAsync(h->cf + f * h->s_field, 0, sizeof(double2) * h->s_field, h->st));
+    }
+    for (int n = 0; n < d.nth; ++n) {
+        if (cfth) CK(copy_fourier(h, h->cf + (3 + n) * h->s_field, cfth + n * fstride, nullptr, 0, d.nyp));
+        else CK(cudaMemsetAsync(h->cf + (3 + n) * h->s_field, 0, sizeof(double2) * h->s_field, h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
+}
+
+int diablo_gpu_download_state(void* handle, double* cu1, double* cu2, double* cu3, double* cp, double* cth,
+                              double* cf1, double* cf2, double* cf3, double* cfth) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    const Dims& d = h->d;
+    const size_t fstride = (size_t)(h->nxp + 1) * (d.nz + 2) * d.nyp * 2;
+    double* cus[3] = {cu1, cu2, cu3};
+    double* cfs[3] = {cf1, cf2, cf3};
+    for (int f = 0; f < 3; ++f) {
+        if (cus[f]) CK(copy_fourier(h, h->cu + f * h->s_field, nullptr, cus[f], 0, d.nyp));
+        if (cfs[f]) CK(copy_fourier(h, h->cf + f * h->s_field, nullptr, cfs[f], 0, d.nyp));
+    }
+    for (int n = 0; n < d.nth; ++n) {
+        if (cth) CK(copy_fourier(h, h->cu + (3 + n) * h->s_field, nullptr, cth + n * fstride, 0, d.nyp));
+        if (cfth) CK(copy_fourier(h, h->cf + (3 + n) * h->s_field, nullptr, cfth + n * fstride, 0, d.nyp));
+    }
+    if (cp) CK(copy_fourier(h, h->cp, nullptr, cp, 0, d.nyp));
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
+}
+
+int diablo_gpu_download_phi(void* handle, double* phi) {
+    Handle* h = (Handle*)handle;
+    if (!h || !phi) return fail(DIABLO_EINVAL, "null pointer argument");
+    CK(copy_fourier(h, h->phi, nullptr, phi, 0, h->d.nyp));
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
+}
+
+static int rem_div(Handle* h, int update_cp, double inv_h) {
+    RemDivArgs a;
+    a.d = h->d;
+    a.cu = h->cu;
+    a.cp = h->cp;
+    a.phi = h->phi;
+    a.bsc = h->bsc;
+    a.gsc = h->gsc;
+    a.kx = h->d_kx;
+    a.kz = h->d_kz;
+    a.dy = h->d_dy;
+    a.dyf = h->d_dyf;
+    a.inv_h = inv_h;
+    a.update_cp = update_cp;
+    CK(launch_remdiv(a, h->st));
+    h->launches += 1;
+    return DIABLO_OK;
+}
+
+// COURANT (courant.f:1-66): the a-priori limits on the host, the velocity
+// minimum on the device from the state's current CU1..CU3.
+static int courant(Handle* h, double* delta_t, double* h_bar) {
+    const diablo_params& p = h->p;
+    const Dims& d = h->d;
+    double dt = 999.0;
+    dt = std::fmin(dt, 0.5 * std::pow(std::fmin(h->dx, h->dy[1]), 2.0) / p.nu);
+    for (int n = 0; n < d.nth; ++n) dt = std::fmin(dt, dt * p.nu / (p.nu / p.pr[n]));
+    if (p.i_ro != 0.0) dt = std::fmin(dt, 2.0 * h->pi / std::fabs(p.i_ro) / 20.0);
+    for (int n = 0; n < d.nth; ++n)
+        if (p.ri[n] != 0.0) {
+            const double Nmax = std::sqrt(std::fabs(p.ri[n] * p.th_bc_ymin_c1[n]));
+            dt = std::fmin(dt, (double)0.1f * 2.0 * h->pi / Nmax);   // single-precision 0.1 (courant.f:32)
+        }
+    const double inf = HUGE_VAL;
+    CK(cudaMemcpyAsync(h->dtmin, &inf, sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(launch_zinv<double>(d, h->cu, h->s_field, h->xb, h->x_field, 3, 0, d.nyp, h->pz, h->twz_d, h->st));
+    CK(launch_cfl(d, h->xb, h->x_field, h->px, h->twx_d, h->d_dy, p.cfl, h->dx, h->dz, h->dtmin, h->st));
+    h->launches += 2;
+    double vmin = inf;
+    CK(cudaMemcpyAsync(&vmin, h->dtmin, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    dt = std::fmin(dt, vmin);
+    double DELTA_T;
+    if (dt <= 0) DELTA_T = 0.0001;
+    else if (dt >= 999.) DELTA_T = 999.0;
+    else DELTA_T = dt;
+    *delta_t = DELTA_T;
+    h_bar[0] = DELTA_T * (8.0 / 15.0);
+    h_bar[1] = DELTA_T * (2.0 / 15.0);
+    h_bar[2] = DELTA_T * (5.0 / 15.0);
+    return DIABLO_OK;
+}
+
+int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, double* delta_t,
+                         double* h_bar, const double* beta_bar, const double* zeta_bar) {
+    Handle* h = (Handle*)handle;
+    if (!h || !delta_t || !h_bar || !beta_bar || !zeta_bar) return fail(DIABLO_EINVAL, "null pointer argument");
+    if (rk_step < 1 || rk_step > 3) return fail(DIABLO_EINVAL, "rk_step must be 1, 2 or 3");
+    const diablo_params& p = h->p;
+    const Dims& d = h->d;
+    const int r = rk_step - 1;
+    // constants of channel.f:77-81
+    const double TEMP1 = p.nu * h_bar[r] / 2.0;
+    const double TEMP3 = zeta_bar[r] * h_bar[r];
+    const double TEMP4 = h_bar[r];
+    const double TEMP5 = beta_bar[r] * h_bar[r];
+    int rc;
+    if (h->fp32) rc = run_transforms<float>(h);
+    else rc = run_transforms<double>(h);
+    if (rc) return rc;
+    CnArgs a;
+    a.d = d;
+    a.cu = h->cu;
+    a.cf = h->cf;
+    a.cp = h->cp;
+    a.kx = h->d_kx;
+    a.kz = h->d_kz;
+    a.dy = h->d_dy;
+    a.dyf = h->d_dyf;
+    a.mult = h->mult;
+    a.piv = h->piv;
+    a.cup = h->cup;
+    a.bcv = h->bcv;
+    a.kind = h->kind;
+    for (int f = 0; f < MAXF; ++f) { a.cf_lo[f] = 2; a.cf_hi[f] = d.ny; a.cb_lo[f] = 1; }
+    for (int n = 0; n < d.nth; ++n) {
+        a.cf_lo[3 + n] = h->jstart_th[n];
+        a.cf_hi[3 + n] = h->jend_th[n];
+        a.cb_lo[3 + n] = h->jstart_th[n] - 1;
+    }
+    a.temp1 = TEMP1; a.temp3 = TEMP3; a.temp4 = TEMP4; a.temp5 = TEMP5;
+    a.nu = p.nu; a.beta = p.beta; a.nu_v_scale = p.nu_v_scale; a.i_ro = p.i_ro;
+    a.grav_x = p.grav_x; a.grav_y = p.grav_y; a.grav_z = p.grav_z;
+    for (int n = 0; n < 4; ++n) {
+        a.ri[n] = n < d.nth ? p.ri[n] : 0.0;
+        a.pr[n] = n < d.nth ? p.pr[n] : 1.0;
+        a.drhodx[n] = n < d.nth ? p.drhodx[n] : 0.0;
+        a.drhodz[n] = n < d.nth ? p.drhodz[n] : 0.0;
+    }
+    a.forcing = 0.0;
+    if (p.f_type == 1) a.forcing = TEMP4 * p.px0;
+    else if (p.f_type == 2) a.forcing = TEMP4 * (p.px0 + p.amp_omega0 * std::cos(p.omega0 * time));
+    a.rk_step = rk_step;
+    a.store_cf = 1;
+    CK(launch_cn_coef(d, a, h->mult, h->piv, h->cup, h->bcv, h->kind, h->bc_type, h->bc_c1, h->st));
+    if (h->fp32) CK(launch_cn<cpx<float>>(a, (const cpx<float>*)h->nl, h->st));
+    else CK(launch_cn<cpx<double>>(a, (const cpx<double>*)h->nl, h->st));
+    h->launches += 2;
+    if (p.variable_dt && rk_step == 3 && (time_step % p.update_dt) == 0) {
+        if ((rc = courant(h, delta_t, h_bar))) return rc;
+    }
+    return rem_div(h, 1, 1.0 / TEMP4);
+}
+
+int diablo_gpu_rk_chan_2(void* handle) {
+    (void)handle;
+    return fail(DIABLO_ENOTSUP, "RK_CHAN_2 is not supported (the reference stops here too)");
+}
+
+int diablo_gpu_rem_div_chan(void* handle) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    int rc = rem_div(h, 0, 0.0);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
+}
+
+int diablo_gpu_apply_bc_vel(void* handle) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    dim3 grid((h->d.nkxp + 127) / 128, h->d.nkzt);
+    k_apply_bc_vel<<<grid, 128, 0, h->st>>>(h->d, h->cu, h->d_dy, h->d_dyf, h->p);
+    CK(cudaGetLastError());
+    h->launches += 1;
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
+}
+
+int diablo_gpu_courant(void* handle, double* delta_t, double* h_bar) {
+    Handle* h = (Handle*)handle;
+    if (!h || !delta_t || !h_bar) return fail(DIABLO_EINVAL, "null pointer argument");
+    return courant(h, delta_t, h_bar);
+}
+
+static int ensure_phys(Handle* h) {
+    if (h->phys) return DIABLO_OK;
+    const size_t bytes = sizeof(double) * (size_t)h->d.nyp * h->d.nz * h->d.nx;
+    cudaError_t e = cudaMalloc((void**)&h->phys, bytes);
+    if (e != cudaSuccess) return fail(DIABLO_ENOMEM, "physical buffer allocation failed");
+    return DIABLO_OK;
+}
+
+int diablo_gpu_fft_xz_to_fourier(void* handle, const double* v, double* vv, int jmin, int jmax) {
+    Handle* h = (Handle*)handle;
+    if (!h || !v || !vv) return fail(DIABLO_EINVAL, "null pointer argument");
+    const Dims& d = h->d;
+    if (jmin < 0 || jmax > d.ny + 1) return fail(DIABLO_EINVAL, "plane range outside 0..NY+1");
+    if (jmax < jmin) return DIABLO_OK;
+    int rc = ensure_phys(h);
+    if (rc) return rc;
+    const int np = jmax - jmin + 1;
+    CK(copy_physical(h, h->phys, v, nullptr, jmin, np));
+    CK(launch_xfwd(d, h->phys, h->xb, jmin, np, h->px, h->twx_d, h->st));
+    CK(launch_zfwd_pack(d, h->xb, h->api_s, jmin, np, h->pz, h->twz_d, h->st));
+    h->launches += 2;
+    CK(copy_fourier(h, h->api_s, nullptr, vv, jmin, np));
+    CK(cudaStreamSynchronize(h->st));
+    // modes NKX < I <= NXP are zero, as the reference writes them (mpi.f:1503-1517)
+    const size_t cx = (size_t)h->nxp + 1, cz = (size_t)d.nz + 2;
+    for (int j = jmin; j <= jmax; ++j)
+        for (int k = 0; k <= d.tnkz; ++k)
+            std::memset(vv + 2 * ((size_t)j * cz * cx + (size_t)k * cx + d.nkxp), 0,
+                        sizeof(double) * 2 * (cx - d.nkxp));
+    return DIABLO_OK;
+}
+
+int diablo_gpu_fft_xz_to_physical(void* handle, const double* vv, double* v, int jmin, int jmax) {
+    Handle* h = (Handle*)handle;
+    if (!h || !v || !vv) return fail(DIABLO_EINVAL, "null pointer argument");
+    const Dims& d = h->d;
+    if (jmin < 0 || jmax > d.ny + 1) return fail(DIABLO_EINVAL, "plane range outside 0..NY+1");
+    if (jmax < jmin) return DIABLO_OK;
+    int rc = ensure_phys(h);
+    if (rc) return rc;
+    const int np = jmax - jmin + 1;
+    CK(copy_fourier(h, h->api_s, vv, nullptr, jmin, np));
+    CK(launch_zinv<double>(d, h->api_s, h->s_field, h->xb, h->x_field, 1, jmin, np, h->pz, h->twz_d, h->st));
+    CK(launch_xinv(d, h->xb, h->phys, jmin, np, h->px, h->twx_d, h->st));
+    h->launches += 2;
+    CK(copy_physical(h, h->phys, nullptr, v, jmin, np));
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
+}
+
+int diablo_gpu_poisson_p_chan(void* handle) {
+    (void)handle;
+    return fail(DIABLO_ENOTSUP, "POISSON_P_CHAN is not built yet");
+}
+
+int diablo_gpu_stats(void* handle, double* profiles) {
+    (void)handle;
+    (void)profiles;
+    return fail(DIABLO_ENOTSUP, "statistics are not built yet");
+}
+
+int diablo_gpu_synchronize(void* handle) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
+}
+
+long long diablo_gpu_kernel_launches(void* handle) {
+    Handle* h = (Handle*)handle;
+    return h ? h->launches : -1;
+}
+
+}  // extern "C"

@@ -1,0 +1,66 @@
+// kernels.cuh -- device data layouts and kernel argument blocks.
+//
+// Device layouts (all row-major, fastest index last):
+//   spectral  S[f][J][m][kx]   complex, J in [0,NY+1], m in [0,TNKZ] (the
+//             packed kz of FFT_XZ_TO_FOURIER, mpi.f:1530-1539), kx in
+//             [0,NKX]; rows padded to ldx (a multiple of 16) with zeros.
+//             State (CU, CP, CF) is FP64; the nonlinear term NL is the
+//             transform type T.
+//   x-spectrum X[f][J][z][kx]  complex<T>: after the inverse z transform,
+//             kx in [0,NKX] (+ zero padding to ldx), z in [0,NZ).
+//   products  Y[p][J][z][kx]   complex<T>: x spectra of the products.
+//   physical  P[J][z][x]       real, pitch NX (transform API only).
+#pragma once
+
+#include "fft.cuh"
+
+namespace dgpu {
+
+constexpr int MAXF = 3 + 4;   // fields: U1, U2, U3, TH(1..N_TH)
+
+struct Dims {
+    int nx, ny, nz, nth, nf, np;
+    int nkx, nkz, tnkz, nkxp, nkzt, ldx, nyp;
+};
+
+// Everything K4 (the column kernel) needs besides the arrays.
+struct CnArgs {
+    Dims d;
+    double2* cu;          // S, nf fields (in: CU old, out: CU after the CN solves)
+    double2* cf;          // S, nf fields (in: CF old, out: CF new)
+    const double2* cp;    // S, 1 field
+    const double* kx;     // KX(0..ldx-1), zero beyond NKX
+    const double* kz;     // KZ(0..TNKZ)
+    const double* dy;     // DY(0..NY+1)
+    const double* dyf;    // DYF(0..NY+1)
+    const double* mult;   // [nf][nyp] forward multipliers -A(j)/B'(j-1)
+    const double* piv;    // [nf][nyp] pivots B'(j)
+    const double* cup;    // [nf][nyp] upper diagonal C(j)
+    const double* bcv;    // [nf][nyp] RHS of BC rows for the (0,0) mode
+    const signed char* kind;  // [nf][nyp] 0: interior row, 1: BC row
+    int cf_lo[MAXF], cf_hi[MAXF];   // rows where CF is formed
+    int cb_lo[MAXF];                // first row copied back (last is NY+1)
+    double temp1, temp3, temp4, temp5;
+    double nu, beta, nu_v_scale, i_ro, grav_x, grav_y, grav_z;
+    double ri[4], pr[4], drhodx[4], drhodz[4];
+    double forcing;       // value subtracted from CR1(0,0,j) (F_TYPE 1/2), already * TEMP4
+    int rk_step;
+    int store_cf;
+};
+
+struct RemDivArgs {
+    Dims d;
+    double2* cu;          // S, velocity fields 0..2
+    double2* cp;          // S
+    double2* phi;         // S, phi (J = 1..NY)
+    double* bsc;          // scratch pivots  [J][m][kx]
+    double2* gsc;         // scratch RHS     [J][m][kx]
+    const double* kx;
+    const double* kz;
+    const double* dy;
+    const double* dyf;
+    double inv_h;         // 1/TEMP4 for the pressure update
+    int update_cp;        // CP += phi/h on J = 2..NY
+};
+
+}  // namespace dgpu

@@ -1,0 +1,168 @@
+/*
+ * diablo_gpu.h -- C ABI of the B200 (sm_100a) channel timestep library.
+ *
+ * The library replaces the body of DIABLO's channel solver step for the
+ * Fortran host: RK_CHAN_1 (for/channel.f:62-1073) together with the x/z
+ * transform wrappers FFT_XZ_TO_FOURIER / FFT_XZ_TO_PHYSICAL
+ * (for/mpi.f:1477-1606), the projection REM_DIV_CHAN (for/channel.f:1103-1214),
+ * the restart pressure solve POISSON_P_CHAN (for/channel.f:1217-1453) and the
+ * CFL step COURANT (for/courant.f:1-66).  In the reference all of these take
+ * no arguments and talk through COMMON blocks; here the COMMON state that
+ * RK_CHAN_1 reads and writes lives on the device inside an opaque handle, and
+ * the host moves it in and out with the upload / download calls.
+ *
+ * Conventions
+ *  - Every pointer argument is a HOST pointer.  No torch or CUDA types appear.
+ *  - Fourier-space arrays use the Fortran layout of the COMMON arrays
+ *    CU1(0:NXP,0:NZ+1,0:NY+1) (for/header:236-249): COMPLEX*16 stored as
+ *    interleaved (re,im) doubles, column-major, NXP = NX/2.  Only the
+ *    dealiased block I in [0,NKX], K in [0,TNKZ] (NKX=NX/3, TNKZ=2*(NZ/3)) is
+ *    read or written; the other entries of a host array are left untouched
+ *    on download and ignored on upload, as every Fourier-space loop of the
+ *    reference only visits that block.
+ *  - Physical-space arrays use the layout U1(0:NX+1,0:NZ+1,0:NY+1) REAL*8
+ *    (for/header:222-229, NPROCZ=1 so NZP=NZ).
+ *  - Return value: 0 on success, a negative DIABLO_E* code on failure.
+ *    diablo_gpu_last_error() gives a one-line message for the last failure
+ *    on the calling thread.
+ *  - One handle = one channel instance = one CUDA stream.  Calls on the same
+ *    handle must not overlap in time (the reference is single-threaded).
+ */
+#ifndef DIABLO_GPU_H
+#define DIABLO_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DIABLO_OK            0
+#define DIABLO_EINVAL       -1   /* bad dimensions or parameters, null pointer */
+#define DIABLO_ERADIX       -2   /* NX or NZ is not a product of 2, 3 and 5 */
+#define DIABLO_ECUDA        -3   /* a CUDA runtime call failed */
+#define DIABLO_ENOTSUP      -4   /* feature not supported (RK_CHAN_2, LES) */
+#define DIABLO_ENAN         -5   /* a non-finite value was found in the state */
+#define DIABLO_ENOMEM       -6   /* device allocation failed */
+
+#define DIABLO_MAX_TH        4   /* largest N_TH the library accepts */
+
+#define DIABLO_PREC_FP64     0   /* every kernel in FP64 */
+#define DIABLO_PREC_FP32SPLIT 1  /* transforms + products in FP32; solves, state, (0,0) mode in FP64 */
+
+/* Run parameters: grid_def + input.dat + input_chan.dat (for/diablo_io.f:11-46,
+ * for/channel.f:1466-1509).  Names follow the Fortran variables. */
+typedef struct diablo_params {
+    /* grid_def (for/grid_def) */
+    int nx, ny, nz, n_th;
+    /* input.dat */
+    double nu, beta, lx, ly, lz;
+    double nu_v_scale;
+    int variable_dt, update_dt;
+    double cfl;
+    int les;                       /* must be 0: the LES branch is not built */
+    int create_new_flow;
+    /* input_chan.dat */
+    double i_ro;
+    double grav_x, grav_y, grav_z;
+    int f_type;
+    double ubulk0, px0, omega0, amp_omega0;
+    int u_bc_ymin, v_bc_ymin, w_bc_ymin;
+    int u_bc_ymax, v_bc_ymax, w_bc_ymax;
+    double u_bc_ymin_c1, v_bc_ymin_c1, w_bc_ymin_c1;
+    double u_bc_ymax_c1, v_bc_ymax_c1, w_bc_ymax_c1;
+    int th_bc_ymin[DIABLO_MAX_TH], th_bc_ymax[DIABLO_MAX_TH];
+    double th_bc_ymin_c1[DIABLO_MAX_TH], th_bc_ymax_c1[DIABLO_MAX_TH];
+    double ri[DIABLO_MAX_TH], pr[DIABLO_MAX_TH];
+    double drhodx[DIABLO_MAX_TH], drhodz[DIABLO_MAX_TH];
+    /* library options */
+    int precision;                 /* DIABLO_PREC_* */
+} diablo_params;
+
+/* Create a channel instance on the current CUDA device.
+ * gy, gyf, dy, dyf: GY(0:NY+1), GYF(0:NY+1), DY(0:NY+1), DYF(0:NY+1) of
+ * /GRID_PARAMS/ (for/header:205-207) as set by CREATE_GRID_CHAN
+ * (for/channel.f:1564-1655).  Replaces INIT_FFT's plans and wavenumbers
+ * (for/fft.f:55-143) and INIT_CHAN_MPI's JSTART/JEND (for/mpi.f:1013-1081). */
+int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gyf,
+                      const double* dy, const double* dyf, void** handle);
+int diablo_gpu_destroy(void* handle);
+
+/* Copy the RK_CHAN_1 inputs from host COMMON arrays to the device.
+ * cu1..cp: CU1, CU2, CU3, CP; cth: CTH(...,1:N_TH) (N_TH consecutive arrays);
+ * cf1..cfth: CF1, CF2, CF3, CFTH (may be NULL: the device copy is zeroed,
+ * which is what RK_STEP=1 needs). */
+int diablo_gpu_upload_state(void* handle, const double* cu1, const double* cu2,
+                            const double* cu3, const double* cp, const double* cth,
+                            const double* cf1, const double* cf2, const double* cf3,
+                            const double* cfth);
+/* Copy the device state back into host COMMON arrays (any pointer may be NULL). */
+int diablo_gpu_download_state(void* handle, double* cu1, double* cu2, double* cu3,
+                              double* cp, double* cth, double* cf1, double* cf2,
+                              double* cf3, double* cfth);
+
+/* One RK substage: the body of RK_CHAN_1 (for/channel.f:62-1073), including
+ * the REM_DIV_CHAN projection and the pressure update (channel.f:1055-1065),
+ * and COURANT at rk_step 3 when variable_dt and mod(time_step,update_dt)==0
+ * (channel.f:1037-1040).  h_bar/beta_bar/zeta_bar are /RKW3_PARAMS/
+ * (for/header:173-174).  delta_t and h_bar are updated in place when
+ * COURANT runs, exactly as courant.f:49-62 updates DELTA_T and H_BAR. */
+int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time,
+                         double* delta_t, double* h_bar, const double* beta_bar,
+                         const double* zeta_bar);
+/* RK_CHAN_2 (for/channel.f:1076-1100) is a stub in the reference that prints
+ * "not supported" and stops; this returns DIABLO_ENOTSUP. */
+int diablo_gpu_rk_chan_2(void* handle);
+
+/* FFT_XZ_TO_FOURIER(V,VV,JMIN,JMAX) (for/mpi.f:1477-1542) on host arrays:
+ * v is a physical array, vv a Fourier array; planes jmin..jmax. */
+int diablo_gpu_fft_xz_to_fourier(void* handle, const double* v, double* vv,
+                                 int jmin, int jmax);
+/* FFT_XZ_TO_PHYSICAL(VV,V,JMIN,JMAX) (for/mpi.f:1547-1606) on host arrays. */
+int diablo_gpu_fft_xz_to_physical(void* handle, const double* vv, double* v,
+                                  int jmin, int jmax);
+
+/* REM_DIV_CHAN (for/channel.f:1103-1214) on the device state; phi is kept
+ * on the device and returned by diablo_gpu_download_phi. */
+int diablo_gpu_rem_div_chan(void* handle);
+int diablo_gpu_download_phi(void* handle, double* phi);
+/* POISSON_P_CHAN (for/channel.f:1217-1453) on the device state (CU -> CP). */
+int diablo_gpu_poisson_p_chan(void* handle);
+/* APPLY_BC_VEL_MPI (for/mpi.f:1317-1331) on the device state. */
+int diablo_gpu_apply_bc_vel(void* handle);
+/* COURANT (for/courant.f:1-66) on the device state's physical velocity. */
+int diablo_gpu_courant(void* handle, double* delta_t, double* h_bar);
+
+/* Plane statistics of SAVE_STATS_CHAN (for/save_stats.f:104-347,452-536) in
+ * FP64 for the current state.  profiles receives DIABLO_NSTATS*(NY+2)
+ * doubles, profile s at [s*(NY+2) + j]; see DIABLO_STAT_* for s. */
+#define DIABLO_STAT_UME     0
+#define DIABLO_STAT_VME     1
+#define DIABLO_STAT_WME     2
+#define DIABLO_STAT_URMS    3
+#define DIABLO_STAT_VRMS    4
+#define DIABLO_STAT_WRMS    5
+#define DIABLO_STAT_UV      6
+#define DIABLO_STAT_UW      7
+#define DIABLO_STAT_WV      8
+#define DIABLO_STAT_DUDY    9
+#define DIABLO_STAT_DWDY   10
+#define DIABLO_STAT_CP     11
+#define DIABLO_STAT_SHEAR  12
+#define DIABLO_STAT_THME   13   /* scalar 1 */
+#define DIABLO_STAT_DTHDY  14
+#define DIABLO_STAT_THRMS  15
+#define DIABLO_STAT_THV    16
+#define DIABLO_NSTATS      17
+int diablo_gpu_stats(void* handle, double* profiles);
+
+/* Wait for all work queued on the handle's stream. */
+int diablo_gpu_synchronize(void* handle);
+/* Sum over the last launches of the handle: number of kernels launched by
+ * the library since creation (the counter is cumulative). */
+long long diablo_gpu_kernel_launches(void* handle);
+/* Short description of the last error on this thread. */
+const char* diablo_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DIABLO_GPU_H */

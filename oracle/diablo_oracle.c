@@ -1,0 +1,1327 @@
+/*
+ * diablo_oracle.c -- CPU FP64 restatement of DIABLO's channel timestep.
+ *
+ * TEST INFRASTRUCTURE ONLY (see diablo_oracle.h): the checker for the GPU
+ * library, never linked into it.  Each routine cites the reference routine
+ * it restates; the loop structure, ranges, aliasing and in-place updates
+ * follow the reference's NPROCY = NPROCZ = 1 MPI build so that round-off
+ * aside the oracle produces the reference's numbers.
+ */
+#include "diablo_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef double complex cplx;
+
+/* ------------------------------------------------------------------------ */
+/* FFT: mixed-radix (2,3,4,5,8) self-sorting Stockham transform, FP64.        */
+/* Restates the DFT that FFTW 3.3.10 computes (fft.f:73-89 plans,             */
+/* mpi.f:1494,1528,1575,1602 executions): X_k = sum_j x_j exp(s 2 pi i jk/n). */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int n, nr, radix[40];
+    cplx* w;          /* w[k] = exp(-2 pi i k / n) */
+} fftplan;
+
+static int plan_init(fftplan* P, int n) {
+    P->n = n;
+    P->nr = 0;
+    int m = n;
+    const int rads[5] = {8, 4, 2, 3, 5};
+    for (int q = 0; q < 5; ++q)
+        while (m % rads[q] == 0) { P->radix[P->nr++] = rads[q]; m /= rads[q]; }
+    if (m != 1) return -1;
+    P->w = (cplx*)malloc(sizeof(cplx) * (size_t)n);
+    const double pi = 4.0 * atan(1.0);
+    for (int k = 0; k < n; ++k) {
+        double a = -2.0 * pi * (double)k / (double)n;
+        P->w[k] = cos(a) + I * sin(a);
+    }
+    return 0;
+}
+static void plan_free(fftplan* P) { free(P->w); P->w = NULL; }
+
+/* In-place transform of x (length n, contiguous); work has n entries. */
+static void cfft(const fftplan* P, cplx* x, cplx* work, int sign) {
+    const int n = P->n;
+    cplx* d0 = x;
+    cplx* d1 = work;
+    int Ns = 1;
+    for (int s = 0; s < P->nr; ++s) {
+        const int R = P->radix[s];
+        const int nR = n / R;
+        const int tw = n / (Ns * R);      /* table step for the stage twiddle */
+        const int rw = n / R;             /* table step for the radix-R kernel */
+        for (int j = 0; j < nR; ++j) {
+            cplx v[8], V[8];
+            const int k = j % Ns;
+            for (int r = 0; r < R; ++r) {
+                cplx t = P->w[(k * r * tw) % n];
+                if (sign > 0) t = conj(t);
+                v[r] = d0[j + r * nR] * t;
+            }
+            for (int p = 0; p < R; ++p) {
+                cplx acc = 0;
+                for (int q = 0; q < R; ++q) {
+                    cplx t = P->w[((p * q) % R) * rw];
+                    if (sign > 0) t = conj(t);
+                    acc += v[q] * t;
+                }
+                V[p] = acc;
+            }
+            const int idxD = (j / Ns) * Ns * R + k;
+            for (int r = 0; r < R; ++r) d1[idxD + r * Ns] = V[r];
+        }
+        cplx* t = d0; d0 = d1; d1 = t;
+        Ns *= R;
+    }
+    if (d0 != x) memcpy(x, d0, sizeof(cplx) * (size_t)n);
+}
+
+int orc_cdft(int n, double* data, int sign) {
+    fftplan P;
+    if (plan_init(&P, n)) return -1;
+    cplx* work = (cplx*)malloc(sizeof(cplx) * (size_t)n);
+    cfft(&P, (cplx*)data, work, sign);
+    free(work);
+    plan_free(&P);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* State: the COMMON blocks that the channel timestep touches.               */
+/* ------------------------------------------------------------------------ */
+struct orc_state {
+    diablo_params p;
+    int NX, NY, NZ, NTH, NXP, NZP, NKX, NKZ, TNKZ, NXM;
+    int px, pz;           /* physical leading dims: NX+2, NZP+2 */
+    int cx, cz;           /* complex leading dims: NXP+1, NZ+2 */
+    size_t nreal;         /* doubles per 3-D field */
+    double PI;
+    double *GY, *GYF, *DY, *DYF;      /* 0..NY+1 */
+    double DX, DZ;
+    double *KX, *KX2, *KZ, *KZ2;      /* 0..NXP, 0..TNKZ */
+    double H_BAR[3], BETA_BAR[3], ZETA_BAR[3];
+    double DELTA_T, TIME;
+    int TIME_STEP, RK_STEP;
+    int JSTART, JEND, JSTART_TH[DIABLO_MAX_TH], JEND_TH[DIABLO_MAX_TH];
+    /* EQUIVALENCE'd pairs share one buffer: U1<->CU1 etc. (header:245-255) */
+    double *U1, *U2, *U3, *P, *R1, *R2, *R3, *F1, *F2, *F3, *S1;
+    /* not equivalenced (header:256-258) */
+    double *TH, *CTH, *FTH, *CFTH, *RTH, *CRTH;
+    fftplan px_plan, pz_plan;
+};
+
+#define PH(a, i, k, j) ((a)[(size_t)(i) + (size_t)s->px * ((size_t)(k) + (size_t)s->pz * (size_t)(j))])
+#define CX(a, i, k, j) (((cplx*)(a))[(size_t)(i) + (size_t)s->cx * ((size_t)(k) + (size_t)s->cz * (size_t)(j))])
+
+static int g_threads = 0;
+void orc_set_threads(int n) { g_threads = n; }
+static int nthreads(void) {
+#ifdef _OPENMP
+    return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+orc_state* orc_create(const diablo_params* p, const double* gy, const double* gyf,
+                      double delta_t) {
+    orc_state* s = (orc_state*)calloc(1, sizeof(orc_state));
+    s->p = *p;
+    s->NX = p->nx; s->NY = p->ny; s->NZ = p->nz; s->NTH = p->n_th;
+    s->NXP = p->nx / 2; s->NZP = p->nz;
+    s->NKX = p->nx / 3; s->NKZ = p->nz / 3; s->TNKZ = 2 * s->NKZ;
+    s->NXM = p->nx - 1;
+    s->px = s->NX + 2; s->pz = s->NZP + 2;
+    s->cx = s->NXP + 1; s->cz = s->NZ + 2;
+    s->nreal = (size_t)s->px * s->pz * (s->NY + 2);
+    s->PI = 4.0 * atan(1.0);
+    if (plan_init(&s->px_plan, s->NX) || plan_init(&s->pz_plan, s->NZ)) {
+        free(s);
+        return NULL;
+    }
+    const int NY = s->NY;
+    s->GY = (double*)calloc(NY + 2, sizeof(double));
+    s->GYF = (double*)calloc(NY + 2, sizeof(double));
+    s->DY = (double*)calloc(NY + 2, sizeof(double));
+    s->DYF = (double*)calloc(NY + 2, sizeof(double));
+    memcpy(s->GY, gy, sizeof(double) * (NY + 2));
+    memcpy(s->GYF, gyf, sizeof(double) * (NY + 2));
+    /* CREATE_GRID_CHAN grid spacing (channel.f:1566-1578, 1646-1652) */
+    s->DX = p->lx / s->NX;
+    s->DZ = p->lz / s->NZ;
+    for (int j = 1; j <= NY + 1; ++j) s->DY[j] = s->GYF[j] - s->GYF[j - 1];
+    for (int j = 1; j <= NY; ++j) s->DYF[j] = s->GY[j + 1] - s->GY[j];
+    s->DYF[NY + 1] = s->DYF[NY];
+    /* INIT_FFT wavenumbers (fft.f:77-100); NXPP = NXP for NPROCZ = 1 */
+    s->KX = (double*)calloc(s->NXP + 1, sizeof(double));
+    s->KX2 = (double*)calloc(s->NXP + 1, sizeof(double));
+    s->KZ = (double*)calloc(s->TNKZ + 1, sizeof(double));
+    s->KZ2 = (double*)calloc(s->TNKZ + 1, sizeof(double));
+    for (int i = 0; i <= s->NXP - 1; ++i) {
+        s->KX[i] = (double)i * (2.0 * s->PI) / p->lx;
+        s->KX2[i] = s->KX[i] * s->KX[i];
+    }
+    for (int k = 0; k <= s->NKZ; ++k) s->KZ[k] = (double)k * (2.0 * s->PI) / p->lz;
+    for (int k = 1; k <= s->NKZ; ++k) s->KZ[s->TNKZ + 1 - k] = -(double)k * (2.0 * s->PI) / p->lz;
+    for (int k = 0; k <= s->TNKZ; ++k) s->KZ2[k] = s->KZ[k] * s->KZ[k];
+    /* INIT_CHAN_MPI, RANKY = 0 branch (mpi.f:1024-1044): with NPROCY = 1 the
+     * first branch is taken, so JEND = NY and JSTART = 2 whatever the BCs. */
+    s->JSTART = 2;
+    s->JEND = NY;
+    for (int n = 0; n < s->NTH; ++n) {
+        s->JEND_TH[n] = NY;
+        s->JSTART_TH[n] = (p->th_bc_ymin[n] == 1) ? 1 : 2;
+    }
+    /* RK coefficients (diablo_io.f:116-124) */
+    s->DELTA_T = delta_t;
+    s->H_BAR[0] = delta_t * (8.0 / 15.0);
+    s->H_BAR[1] = delta_t * (2.0 / 15.0);
+    s->H_BAR[2] = delta_t * (5.0 / 15.0);
+    s->BETA_BAR[0] = 1.0; s->BETA_BAR[1] = 25.0 / 8.0; s->BETA_BAR[2] = 9.0 / 4.0;
+    s->ZETA_BAR[0] = 0.0; s->ZETA_BAR[1] = -17.0 / 8.0; s->ZETA_BAR[2] = -5.0 / 4.0;
+    s->TIME = 0.0;
+    s->TIME_STEP = 0;
+    double** fields[11] = {&s->U1, &s->U2, &s->U3, &s->P, &s->R1, &s->R2, &s->R3,
+                           &s->F1, &s->F2, &s->F3, &s->S1};
+    for (int f = 0; f < 11; ++f) *fields[f] = (double*)calloc(s->nreal, sizeof(double));
+    size_t nth = (size_t)(s->NTH > 0 ? s->NTH : 1);
+    s->TH = (double*)calloc(s->nreal * nth, sizeof(double));
+    s->CTH = (double*)calloc(s->nreal * nth, sizeof(double));
+    s->FTH = (double*)calloc(s->nreal * nth, sizeof(double));
+    s->CFTH = (double*)calloc(s->nreal * nth, sizeof(double));
+    s->RTH = (double*)calloc(s->nreal * nth, sizeof(double));
+    s->CRTH = (double*)calloc(s->nreal * nth, sizeof(double));
+    return s;
+}
+
+void orc_destroy(orc_state* s) {
+    if (!s) return;
+    double* bufs[] = {s->GY, s->GYF, s->DY, s->DYF, s->KX, s->KX2, s->KZ, s->KZ2,
+                      s->U1, s->U2, s->U3, s->P, s->R1, s->R2, s->R3, s->F1, s->F2,
+                      s->F3, s->S1, s->TH, s->CTH, s->FTH, s->CFTH, s->RTH, s->CRTH};
+    for (size_t q = 0; q < sizeof(bufs) / sizeof(bufs[0]); ++q) free(bufs[q]);
+    plan_free(&s->px_plan);
+    plan_free(&s->pz_plan);
+    free(s);
+}
+
+double* orc_array(orc_state* s, int which) {
+    switch (which) {
+        case ORC_U1: return s->U1;   case ORC_U2: return s->U2;
+        case ORC_U3: return s->U3;   case ORC_P: return s->P;
+        case ORC_R1: return s->R1;   case ORC_R2: return s->R2;
+        case ORC_R3: return s->R3;   case ORC_F1: return s->F1;
+        case ORC_F2: return s->F2;   case ORC_F3: return s->F3;
+        case ORC_S1: return s->S1;   case ORC_TH: return s->TH;
+        case ORC_CTH: return s->CTH; case ORC_FTH: return s->FTH;
+        case ORC_CFTH: return s->CFTH; case ORC_RTH: return s->RTH;
+        case ORC_CRTH: return s->CRTH; case ORC_GY: return s->GY;
+        case ORC_GYF: return s->GYF; case ORC_DY: return s->DY;
+        case ORC_DYF: return s->DYF; case ORC_KX: return s->KX;
+        case ORC_KZ: return s->KZ;
+    }
+    return NULL;
+}
+
+size_t orc_array_doubles(orc_state* s, int which) {
+    if (which <= ORC_S1) return s->nreal;
+    if (which <= ORC_CRTH) return s->nreal * (size_t)(s->NTH > 0 ? s->NTH : 1);
+    if (which <= ORC_DYF) return (size_t)s->NY + 2;
+    if (which == ORC_KX) return (size_t)s->NXP + 1;
+    if (which == ORC_KZ) return (size_t)s->TNKZ + 1;
+    return 0;
+}
+
+void orc_get_time(orc_state* s, double* time, double* delta_t, int* time_step,
+                  double* h_bar) {
+    if (time) *time = s->TIME;
+    if (delta_t) *delta_t = s->DELTA_T;
+    if (time_step) *time_step = s->TIME_STEP;
+    if (h_bar) memcpy(h_bar, s->H_BAR, sizeof(s->H_BAR));
+}
+
+void orc_set_time(orc_state* s, double time, double delta_t, int time_step) {
+    s->TIME = time;
+    s->TIME_STEP = time_step;
+    s->DELTA_T = delta_t;
+    s->H_BAR[0] = delta_t * (8.0 / 15.0);
+    s->H_BAR[1] = delta_t * (2.0 / 15.0);
+    s->H_BAR[2] = delta_t * (5.0 / 15.0);
+}
+
+/* ------------------------------------------------------------------------ */
+/* FFT_XZ_TO_FOURIER (mpi.f:1477-1542) with NPROCZ = 1: the all-to-all is a  */
+/* plain copy.  V and VV may alias (EQUIVALENCE), so the x transforms of all */
+/* planes finish before VV is written, as in the reference.                  */
+/* ------------------------------------------------------------------------ */
+void orc_fft_xz_to_fourier(orc_state* s, double* V, double* VVd, int jmin, int jmax) {
+    const int NX = s->NX, NZ = s->NZ, NZP = s->NZP, NXP = s->NXP;
+    const int NKX = s->NKX, NKZ = s->NKZ;
+    const int nh = NX / 2 + 1;
+    const int nplanes = jmax - jmin + 1;
+    if (nplanes <= 0) return;
+    /* TMP(0:NX/2, 0:NZP-1, JMIN:JMAX) */
+    cplx* TMP = (cplx*)malloc(sizeof(cplx) * (size_t)nh * NZP * nplanes);
+#pragma omp parallel num_threads(nthreads())
+    {
+        cplx* row = (cplx*)malloc(sizeof(cplx) * NX);
+        cplx* work = (cplx*)malloc(sizeof(cplx) * NX);
+#pragma omp for collapse(2) schedule(static)
+        for (int j = jmin; j <= jmax; ++j)
+            for (int k = 0; k < NZP; ++k) {
+                for (int i = 0; i < NX; ++i) row[i] = PH(V, i, k, j);
+                cfft(&s->px_plan, row, work, -1);
+                cplx* t = TMP + ((size_t)(j - jmin) * NZP + k) * nh;
+                for (int i = 0; i <= NKX; ++i) t[i] = row[i] / NX;
+                for (int i = NKX + 1; i <= NX / 2; ++i) t[i] = 0.0;
+            }
+        free(row);
+        free(work);
+    }
+    cplx* VV = (cplx*)VVd;
+    (void)VV;
+#pragma omp parallel num_threads(nthreads())
+    {
+        cplx* col = (cplx*)malloc(sizeof(cplx) * NZ);
+        cplx* work = (cplx*)malloc(sizeof(cplx) * NZ);
+#pragma omp for schedule(static)
+        for (int j = jmin; j <= jmax; ++j) {
+            /* all-to-all copy: TMP2(I,K)=TMP_1A(I,K,J), I<NXP, K<NZ */
+            for (int k = 0; k <= NZ - 1; ++k) {
+                const cplx* t = TMP + ((size_t)(j - jmin) * NZP + k) * nh;
+                for (int i = 0; i <= NXP - 1; ++i) CX(VVd, i, k, j) = t[i];
+                CX(VVd, NXP, k, j) = 0.0;
+            }
+            for (int k = NZ; k <= NZ + 1; ++k)
+                for (int i = 0; i <= NXP; ++i) CX(VVd, i, k, j) = 0.0;
+            /* z transform (howmany NXP, stride NXP+1), forward */
+            for (int i = 0; i <= NXP - 1; ++i) {
+                for (int k = 0; k < NZ; ++k) col[k] = CX(VVd, i, k, j);
+                cfft(&s->pz_plan, col, work, -1);
+                for (int k = 0; k < NZ; ++k) CX(VVd, i, k, j) = col[k];
+            }
+            for (int k = 0; k <= NKZ; ++k)
+                for (int i = 0; i <= NXP; ++i) CX(VVd, i, k, j) = CX(VVd, i, k, j) / NZ;
+            for (int k = 1; k <= NKZ; ++k)
+                for (int i = 0; i <= NXP; ++i)
+                    CX(VVd, i, NKZ + k, j) = CX(VVd, i, NZ - 1 + k - NKZ, j) / NZ;
+        }
+        free(col);
+        free(work);
+    }
+    free(TMP);
+}
+
+/* FFT_XZ_TO_PHYSICAL (mpi.f:1547-1606).  The kz unpacking happens in place
+ * on the input array, as in the reference. */
+void orc_fft_xz_to_physical(orc_state* s, double* VVd, double* V, int jmin, int jmax) {
+    const int NX = s->NX, NZ = s->NZ, NZP = s->NZP, NXP = s->NXP;
+    const int NKZ = s->NKZ;
+    const int nh = NX / 2 + 1;
+    const int nplanes = jmax - jmin + 1;
+    if (nplanes <= 0) return;
+    cplx* TMP = (cplx*)malloc(sizeof(cplx) * (size_t)nh * NZP * nplanes);
+#pragma omp parallel num_threads(nthreads())
+    {
+        cplx* col = (cplx*)malloc(sizeof(cplx) * NZ);
+        cplx* work = (cplx*)malloc(sizeof(cplx) * NZ);
+#pragma omp for schedule(static)
+        for (int j = jmin; j <= jmax; ++j) {
+            for (int k = NKZ; k >= 1; --k)
+                for (int i = 0; i <= NXP; ++i)
+                    CX(VVd, i, NZ - 1 + k - NKZ, j) = CX(VVd, i, NKZ + k, j);
+            for (int k = NKZ + 1; k <= NZ - NKZ - 1; ++k)
+                for (int i = 0; i <= NXP; ++i) CX(VVd, i, k, j) = 0.0;
+            for (int i = 0; i <= NXP - 1; ++i) {
+                for (int k = 0; k < NZ; ++k) col[k] = CX(VVd, i, k, j);
+                cfft(&s->pz_plan, col, work, +1);
+                for (int k = 0; k < NZ; ++k) CX(VVd, i, k, j) = col[k];
+            }
+            /* all-to-all copy into TMP(0:NX/2, K, J); Nyquist zeroed */
+            for (int k = 0; k <= NZP - 1; ++k) {
+                cplx* t = TMP + ((size_t)(j - jmin) * NZP + k) * nh;
+                for (int i = 0; i <= NX / 2 - 1; ++i) t[i] = CX(VVd, i, k, j);
+                t[NX / 2] = 0.0;
+            }
+        }
+        free(col);
+        free(work);
+    }
+#pragma omp parallel num_threads(nthreads())
+    {
+        cplx* row = (cplx*)malloc(sizeof(cplx) * NX);
+        cplx* work = (cplx*)malloc(sizeof(cplx) * NX);
+#pragma omp for collapse(2) schedule(static)
+        for (int j = jmin; j <= jmax; ++j)
+            for (int k = 0; k < NZP; ++k) {
+                const cplx* t = TMP + ((size_t)(j - jmin) * NZP + k) * nh;
+                /* c2r: Hermitian extension; imaginary parts of the DC and
+                 * Nyquist bins do not contribute to a real output. */
+                row[0] = creal(t[0]);
+                for (int i = 1; i < NX / 2; ++i) {
+                    row[i] = t[i];
+                    row[NX - i] = conj(t[i]);
+                }
+                row[NX / 2] = creal(t[NX / 2]);
+                cfft(&s->px_plan, row, work, +1);
+                for (int i = 0; i < NX; ++i) PH(V, i, k, j) = creal(row[i]);
+            }
+        free(row);
+        free(work);
+    }
+    free(TMP);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Tridiagonal solvers of the MPI build with NPROCY = 1.                      */
+/* ------------------------------------------------------------------------ */
+/* THOMAS_FORWARD_REAL_MPI + THOMAS_BACKWARD_REAL_MPI (mpi.f:630-697,         */
+/* 757-809) for RANKY = 0 = NPROCY-1, INY = NY, columns i < inx.  Arrays are  */
+/* (0:INX-1, 0:INY+1) column-major.                                           */
+static void thomas_real_mpi(double* A, double* B, double* C, double* G, int iny, int inx) {
+#define M2(a, i, j) (a)[(size_t)(i) + (size_t)inx * (size_t)(j)]
+    for (int j = 1; j <= iny; ++j)
+        for (int i = 0; i < inx; ++i) {
+            M2(A, i, j) = -M2(A, i, j) / M2(B, i, j - 1);
+            M2(B, i, j) = M2(B, i, j) + M2(A, i, j) * M2(C, i, j - 1);
+            M2(G, i, j) = M2(G, i, j) + M2(A, i, j) * M2(G, i, j - 1);
+        }
+    {
+        const int j = iny + 1;
+        for (int i = 0; i < inx; ++i) {
+            M2(A, i, j) = -M2(A, i, j) / M2(B, i, j - 1);
+            M2(B, i, j) = M2(B, i, j) + M2(A, i, j) * M2(C, i, j - 1);
+            M2(G, i, j) = M2(G, i, j) + M2(A, i, j) * M2(G, i, j - 1);
+        }
+    }
+    for (int i = 0; i < inx; ++i) {
+        M2(G, i, iny + 1) = M2(G, i, iny + 1) / M2(B, i, iny + 1);
+        for (int j = iny; j >= 0; --j) {
+            if (M2(B, i, j) != 0.0)
+                M2(G, i, j) = (M2(G, i, j) - M2(C, i, j) * M2(G, i, j + 1)) / M2(B, i, j);
+            else
+                M2(G, i, j) = 0.0;
+        }
+    }
+#undef M2
+}
+
+/* THOMAS_FORWARD_COMPLEX_MPI + THOMAS_BACKWARD_COMPLEX_MPI (mpi.f:700-754,
+ * 812-865) for RANKY = 0 = NPROCY-1: forward rows 2..INY with the B != 0
+ * guard, backward from INY down to 1.  Columns 0..inx (inclusive). */
+static void thomas_complex_mpi(double* A, double* B, double* C, cplx* G, int iny, int inx) {
+    const int ld = inx + 1;
+#define M2(a, i, j) (a)[(size_t)(i) + (size_t)ld * (size_t)(j)]
+    for (int i = 0; i <= inx; ++i) {
+        for (int j = 2; j <= iny; ++j) {
+            if (M2(B, i, j - 1) != 0.0)
+                M2(A, i, j) = -M2(A, i, j) / M2(B, i, j - 1);
+            else
+                M2(A, i, j) = 0.0;
+            M2(B, i, j) = M2(B, i, j) + M2(A, i, j) * M2(C, i, j - 1);
+            M2(G, i, j) = M2(G, i, j) + M2(A, i, j) * M2(G, i, j - 1);
+        }
+        if (M2(B, i, iny) != 0.0)
+            M2(G, i, iny) = M2(G, i, iny) / M2(B, i, iny);
+        else
+            M2(G, i, iny) = 0.0;
+        for (int j = iny - 1; j >= 1; --j) {
+            if (M2(B, i, j) != 0.0)
+                M2(G, i, j) = (M2(G, i, j) - M2(C, i, j) * M2(G, i, j + 1)) / M2(B, i, j);
+            else
+                M2(G, i, j) = 0.0;
+        }
+    }
+#undef M2
+}
+
+/* ------------------------------------------------------------------------ */
+/* Boundary-condition rows (channel.f:1660-2282), both walls applied since    */
+/* NPROCY = 1 makes rank 0 both the lowest and the highest (mpi.f:1083-1237). */
+/* Arrays (0:NX-1, 0:NY+1).                                                   */
+/* ------------------------------------------------------------------------ */
+#define MR(a, i, j) (a)[(size_t)(i) + (size_t)s->NX * (size_t)(j)]
+static void set_row(orc_state* s, double* L, double* D, double* U, double* V, int j,
+                    double l, double d, double u, double v) {
+    for (int i = 0; i <= s->NXM; ++i) {
+        MR(L, i, j) = l; MR(D, i, j) = d; MR(U, i, j) = u; MR(V, i, j) = v;
+    }
+}
+
+/* APPLY_BC_1_LOWER / _UPPER and APPLY_BC_3_* share the same rows: U and W
+ * are both at GYF points (channel.f:1660-1778, 1967-2086). */
+static void bc_u13(orc_state* s, double* L, double* D, double* U, double* V,
+                   int bmin, double cmin, int bmax, double cmax) {
+    const int NY = s->NY;
+    if (bmin == 0) {
+        set_row(s, L, D, U, V, 0, 0.0, 1.0, 0.0, 0.0);
+        set_row(s, L, D, U, V, 1, 0.0, 1.0, 0.0, cmin);
+    } else {
+        set_row(s, L, D, U, V, 0, 0.0, 1.0, 0.0, 0.0);
+        set_row(s, L, D, U, V, 1, 0.0, -1.0, 1.0, s->DY[2] * cmin);
+    }
+    if (bmax == 0) {
+        set_row(s, L, D, U, V, NY + 1, 0.0, 1.0, 0.0, 0.0);
+        set_row(s, L, D, U, V, NY, 0.0, 1.0, 0.0, cmax);
+    } else {
+        set_row(s, L, D, U, V, NY, -1.0, 1.0, 0.0, s->DY[NY] * cmax);
+        set_row(s, L, D, U, V, NY + 1, 0.0, 1.0, 0.0, 0.0);
+    }
+}
+
+/* APPLY_BC_2_LOWER / APPLY_BC_2_UPPER (channel.f:1822-1934). */
+static void bc_u2(orc_state* s, double* L, double* D, double* U, double* V) {
+    const int NY = s->NY;
+    const diablo_params* p = &s->p;
+    if (p->v_bc_ymin == 0) {
+        set_row(s, L, D, U, V, 1, 0.0, 1.0, 0.0, p->v_bc_ymin_c1);
+        set_row(s, L, D, U, V, 2, 0.0, 1.0, 0.0, p->v_bc_ymin_c1);
+    } else if (p->v_bc_ymin == 1) {
+        set_row(s, L, D, U, V, 1, 0.0, -1.0, 1.0, s->DYF[1] * p->v_bc_ymin_c1);
+    }
+    set_row(s, L, D, U, V, 0, 0.0, 1.0, 0.0, 0.0);
+    if (p->v_bc_ymax == 0) {
+        set_row(s, L, D, U, V, NY + 1, 0.0, 1.0, 0.0, p->v_bc_ymax_c1);
+        set_row(s, L, D, U, V, NY, 0.0, 1.0, 0.0, p->v_bc_ymax_c1);
+    } else if (p->v_bc_ymax == 1) {
+        set_row(s, L, D, U, V, NY + 1, -1.0, 1.0, 0.0, s->DYF[NY] * p->v_bc_ymax_c1);
+    }
+}
+
+/* APPLY_BC_TH_LOWER / APPLY_BC_TH_UPPER (channel.f:2129-2202). */
+static void bc_th(orc_state* s, double* L, double* D, double* U, double* V, int n) {
+    const int NY = s->NY;
+    const diablo_params* p = &s->p;
+    if (p->th_bc_ymin[n] == 0) {
+        set_row(s, L, D, U, V, 0, 0.0, 1.0, 0.0, 0.0);
+        set_row(s, L, D, U, V, 1, 0.0, 1.0, 0.0, p->th_bc_ymin_c1[n]);
+    } else {
+        set_row(s, L, D, U, V, 1, 0.0, -1.0, 1.0, s->DY[2] * p->th_bc_ymin_c1[n]);
+        set_row(s, L, D, U, V, 0, 0.0, 1.0, 0.0, 0.0);
+    }
+    if (p->th_bc_ymax[n] == 0) {
+        set_row(s, L, D, U, V, NY + 1, 0.0, 1.0, 0.0, 0.0);
+        set_row(s, L, D, U, V, NY, 0.0, 1.0, 0.0, p->th_bc_ymax_c1[n]);
+    } else {
+        set_row(s, L, D, U, V, NY, -1.0, 1.0, 0.0, s->DY[NY] * p->th_bc_ymax_c1[n]);
+        set_row(s, L, D, U, V, NY + 1, 0.0, 1.0, 0.0, 0.0);
+    }
+}
+
+/* Matrices persist across k (they are initialised once before the k loop
+ * in the reference and rows not rewritten keep the previous k's factors).
+ * That only matters when a BC type leaves a row unset (V_BC = 2); the loop
+ * over k runs serially then so that the persistence is reproduced. */
+static int serial_k(orc_state* s) {
+    return s->p.v_bc_ymin == 2 || s->p.v_bc_ymax == 2;
+}
+
+typedef enum { SOLVE_TH, SOLVE_U2, SOLVE_U1, SOLVE_U3 } solve_kind;
+
+/* One implicit CN solve over all (x,z) columns (channel.f:762-1029). */
+static void cn_solve(orc_state* s, solve_kind kind, int n, double TEMP1) {
+    const int NX = s->NX, NY = s->NY, NZP = s->NZP;
+    const size_t msz = (size_t)NX * (NY + 2);
+    double* field = kind == SOLVE_TH ? s->TH + (size_t)n * s->nreal
+                  : kind == SOLVE_U2 ? s->U2 : kind == SOLVE_U1 ? s->U1 : s->U3;
+    const double* rhs = kind == SOLVE_TH ? s->RTH + (size_t)n * s->nreal
+                      : kind == SOLVE_U2 ? s->R2 : kind == SOLVE_U1 ? s->R1 : s->R3;
+    const double nuv = s->p.nu_v_scale;
+    const int nt = serial_k(s) ? 1 : nthreads();
+#pragma omp parallel num_threads(nt)
+    {
+        double* L = (double*)malloc(sizeof(double) * msz);
+        double* D = (double*)malloc(sizeof(double) * msz);
+        double* U = (double*)malloc(sizeof(double) * msz);
+        double* V = (double*)malloc(sizeof(double) * msz);
+        for (size_t q = 0; q < msz; ++q) { L[q] = 0.0; D[q] = 1.0; U[q] = 0.0; V[q] = 0.0; }
+#pragma omp for schedule(static)
+        for (int k = 0; k <= NZP - 1; ++k) {
+            int jlo, jhi, jc0, jc1;
+            if (kind == SOLVE_TH) {
+                const double c = TEMP1 / s->p.pr[n] * nuv;
+                jlo = s->JSTART_TH[n]; jhi = s->JEND_TH[n];
+                for (int j = jlo; j <= jhi; ++j)
+                    for (int i = 0; i <= s->NXM; ++i) {
+                        MR(L, i, j) = -c / (s->DY[j] * s->DYF[j]);
+                        MR(D, i, j) = 1. + c / (s->DY[j + 1] * s->DYF[j]) + c / (s->DY[j] * s->DYF[j]);
+                        MR(U, i, j) = -c / (s->DY[j + 1] * s->DYF[j]);
+                        MR(V, i, j) = PH(rhs, i, k, j);
+                    }
+                bc_th(s, L, D, U, V, n);
+                jc0 = jlo - 1; jc1 = jhi + 1;
+            } else if (kind == SOLVE_U2) {
+                for (int j = 2; j <= NY; ++j)
+                    for (int i = 0; i <= s->NXM; ++i) {
+                        MR(L, i, j) = -TEMP1 * nuv / (s->DYF[j - 1] * s->DY[j]);
+                        MR(D, i, j) = 1. + TEMP1 * nuv / (s->DYF[j] * s->DY[j]) +
+                                      TEMP1 * nuv / (s->DYF[j - 1] * s->DY[j]);
+                        MR(U, i, j) = -TEMP1 * nuv / (s->DYF[j] * s->DY[j]);
+                        MR(V, i, j) = PH(rhs, i, k, j);
+                    }
+                bc_u2(s, L, D, U, V);
+                jc0 = 1; jc1 = NY + 1;
+            } else {
+                jlo = s->JSTART; jhi = s->JEND;
+                for (int j = jlo; j <= jhi; ++j)
+                    for (int i = 0; i <= s->NXM; ++i) {
+                        MR(L, i, j) = -TEMP1 * nuv / (s->DY[j] * s->DYF[j]);
+                        MR(D, i, j) = 1. - TEMP1 * nuv * (-1. / (s->DY[j + 1] * s->DYF[j]) -
+                                                          1. / (s->DY[j] * s->DYF[j]));
+                        MR(U, i, j) = -TEMP1 * nuv / (s->DY[j + 1] * s->DYF[j]);
+                        MR(V, i, j) = PH(rhs, i, k, j);
+                    }
+                if (kind == SOLVE_U1)
+                    bc_u13(s, L, D, U, V, s->p.u_bc_ymin, s->p.u_bc_ymin_c1, s->p.u_bc_ymax,
+                           s->p.u_bc_ymax_c1);
+                else
+                    bc_u13(s, L, D, U, V, s->p.w_bc_ymin, s->p.w_bc_ymin_c1, s->p.w_bc_ymax,
+                           s->p.w_bc_ymax_c1);
+                jc0 = jlo - 1; jc1 = jhi + 1;
+            }
+            thomas_real_mpi(L, D, U, V, NY, NX);
+            for (int j = jc0; j <= jc1; ++j)
+                for (int i = 0; i <= s->NXM; ++i) PH(field, i, k, j) = MR(V, i, j);
+        }
+        free(L); free(D); free(U); free(V);
+    }
+}
+#undef MR
+
+/* ------------------------------------------------------------------------ */
+/* RK_CHAN_1 (channel.f:62-1073), non-LES branch.                             */
+/* ------------------------------------------------------------------------ */
+void orc_rk_chan_1(orc_state* s, int rk_step) {
+    const int NY = s->NY, NXP = s->NXP, TNKZ = s->TNKZ, NZP = s->NZP, NXM = s->NXM;
+    const int JSTART = s->JSTART, JEND = s->JEND;
+    const diablo_params* p = &s->p;
+    s->RK_STEP = rk_step;
+    const int r = rk_step - 1;
+    const double TEMP1 = p->nu * s->H_BAR[r] / 2.0;
+    const double TEMP2 = s->H_BAR[r] / 2.0;
+    const double TEMP3 = s->ZETA_BAR[r] * s->H_BAR[r];
+    const double TEMP4 = s->H_BAR[r];
+    const double TEMP5 = s->BETA_BAR[r] * s->H_BAR[r];
+    (void)TEMP2;
+    double *CU1 = s->U1, *CU2 = s->U2, *CU3 = s->U3, *CP = s->P;
+    double *CR1 = s->R1, *CR2 = s->R2, *CR3 = s->R3;
+    double *CF1 = s->F1, *CF2 = s->F2, *CF3 = s->F3, *CS1 = s->S1;
+    double *U1 = s->U1, *U2 = s->U2, *U3 = s->U3;
+    double *R1 = s->R1, *R2 = s->R2, *R3 = s->R3, *S1 = s->S1;
+    const cplx CI = I;
+
+    /* CR <- CU (channel.f:88-103) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = JSTART; j <= JEND; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CR1, i, k, j) = CX(CU1, i, k, j);
+                CX(CR3, i, k, j) = CX(CU3, i, k, j);
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) CX(CR2, i, k, j) = CX(CU2, i, k, j);
+    /* + zeta h CF (channel.f:106-121) */
+    if (rk_step > 1) {
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = JSTART; j <= JEND; ++j)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i) {
+                    CX(CR1, i, k, j) = CX(CR1, i, k, j) + TEMP3 * CX(CF1, i, k, j);
+                    CX(CR3, i, k, j) = CX(CR3, i, k, j) + TEMP3 * CX(CF3, i, k, j);
+                }
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = 2; j <= NY; ++j)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i)
+                    CX(CR2, i, k, j) = CX(CR2, i, k, j) + TEMP3 * CX(CF2, i, k, j);
+    }
+    /* pressure gradient (channel.f:124-148) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i)
+                CX(CS1, i, k, j) = (CX(CP, i, k, j) - CX(CP, i, k, j - 1)) / s->DY[j];
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = JSTART; j <= JEND; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CR1, i, k, j) = CX(CR1, i, k, j) - TEMP4 * (CI * s->KX[i] * CX(CP, i, k, j));
+                CX(CR3, i, k, j) = CX(CR3, i, k, j) - TEMP4 * (CI * s->KZ[k] * CX(CP, i, k, j));
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i)
+                CX(CR2, i, k, j) = CX(CR2, i, k, j) - TEMP4 * CX(CS1, i, k, j);
+    /* forcing (channel.f:155-167) */
+    if (p->f_type == 1) {
+        for (int j = JSTART; j <= JEND; ++j) CX(CR1, 0, 0, j) = CX(CR1, 0, 0, j) - TEMP4 * p->px0;
+    } else if (p->f_type == 2) {
+        for (int j = JSTART; j <= JEND; ++j)
+            CX(CR1, 0, 0, j) =
+                CX(CR1, 0, 0, j) - TEMP4 * (p->px0 + p->amp_omega0 * cos(p->omega0 * s->TIME));
+    }
+    /* horizontal viscous terms (channel.f:175-189) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = JSTART; j <= JEND; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                const double kk = pow(s->KX2[i] + s->KZ2[k], p->beta);
+                CX(CF1, i, k, j) = -p->nu * kk * CX(CU1, i, k, j);
+                CX(CF3, i, k, j) = -p->nu * kk * CX(CU3, i, k, j);
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i)
+                CX(CF2, i, k, j) = -p->nu * pow(s->KX2[i] + s->KZ2[k], p->beta) * CX(CU2, i, k, j);
+    /* Coriolis (channel.f:193-200) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int k = 0; k <= TNKZ; ++k)
+        for (int i = 0; i <= NXP - 1; ++i)
+            for (int j = JSTART; j <= JEND; ++j) {
+                CX(CF1, i, k, j) = CX(CF1, i, k, j) + p->i_ro * CX(CU3, i, k, j);
+                CX(CF3, i, k, j) = CX(CF3, i, k, j) - p->i_ro * CX(CU1, i, k, j);
+            }
+    for (int n = 0; n < s->NTH; ++n) {
+        double* CTHn = s->CTH + (size_t)n * s->nreal;
+        double* CRTHn = s->CRTH + (size_t)n * s->nreal;
+        double* CFTHn = s->CFTH + (size_t)n * s->nreal;
+        /* buoyancy into CF2, (0,0) mode skipped (channel.f:209-227) */
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = 2; j <= NY; ++j) {
+            for (int k = 1; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i)
+                    CX(CF2, i, k, j) = CX(CF2, i, k, j) +
+                        p->ri[n] * p->grav_y *
+                            (CX(CTHn, i, k, j) * s->DYF[j - 1] + CX(CTHn, i, k, j - 1) * s->DYF[j]) /
+                            (2.0 * s->DY[j]);
+            for (int i = 1; i <= NXP - 1; ++i)
+                CX(CF2, i, 0, j) = CX(CF2, i, 0, j) +
+                    p->ri[n] * p->grav_y *
+                        (CX(CTHn, i, 0, j) * s->DYF[j - 1] + CX(CTHn, i, 0, j - 1) * s->DYF[j]) /
+                        (2.0 * s->DY[j]);
+        }
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = JSTART; j <= JEND; ++j)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i) {
+                    CX(CF1, i, k, j) = CX(CF1, i, k, j) + p->ri[n] * p->grav_x * CX(CTHn, i, k, j);
+                }
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = JSTART; j <= JEND; ++j)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i)
+                    CX(CF3, i, k, j) = CX(CF3, i, k, j) + p->ri[n] * p->grav_z * CX(CTHn, i, k, j);
+        /* scalar RHS (channel.f:254-290) */
+        const int j0 = s->JSTART_TH[n], j1 = s->JEND_TH[n];
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = j0; j <= j1; ++j)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i) CX(CRTHn, i, k, j) = CX(CTHn, i, k, j);
+        if (rk_step > 1) {
+#pragma omp parallel for num_threads(nthreads())
+            for (int j = j0; j <= j1; ++j)
+                for (int k = 0; k <= TNKZ; ++k)
+                    for (int i = 0; i <= NXP - 1; ++i)
+                        CX(CRTHn, i, k, j) = CX(CRTHn, i, k, j) + TEMP3 * CX(CFTHn, i, k, j);
+        }
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = j0; j <= j1; ++j)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i)
+                    CX(CFTHn, i, k, j) = -(p->nu / p->pr[n]) * pow(s->KX2[i] + s->KZ2[k], p->beta) *
+                                         CX(CTHn, i, k, j);
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = j0; j <= j1; ++j)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i)
+                    CX(CFTHn, i, k, j) = CX(CFTHn, i, k, j) - CX(CU1, i, k, j) * p->drhodx[n] -
+                                         CX(CU3, i, k, j) * p->drhodz[n];
+    }
+    /* USER_RHS_CHAN_FOURIER: empty hook (user_rhs.f:77-121). */
+    /* non-LES branch: transforms to physical space (channel.f:389-399) */
+    orc_fft_xz_to_physical(s, CU1, U1, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CU2, U2, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CU3, U3, 0, NY + 1);
+    for (int n = 0; n < s->NTH; ++n) {
+        memcpy(CS1, s->CTH + (size_t)n * s->nreal, sizeof(double) * s->nreal);
+        orc_fft_xz_to_physical(s, CS1, S1, 0, NY + 1);
+        memcpy(s->TH + (size_t)n * s->nreal, S1, sizeof(double) * s->nreal);
+    }
+
+    /* nonlinear terms, one product at a time (channel.f:410-571) */
+#define PRODUCT(J0, J1, EXPR)                                                  \
+    do {                                                                       \
+        _Pragma("omp parallel for num_threads(nthreads())")                    \
+        for (int j = (J0); j <= (J1); ++j)                                     \
+            for (int k = 0; k <= NZP - 1; ++k)                                 \
+                for (int i = 0; i <= NXM; ++i) PH(S1, i, k, j) = (EXPR);       \
+        orc_fft_xz_to_fourier(s, S1, CS1, 0, NY + 1);                          \
+    } while (0)
+#define ACCUM(J0, J1, STMT)                                                    \
+    do {                                                                       \
+        _Pragma("omp parallel for num_threads(nthreads())")                    \
+        for (int j = (J0); j <= (J1); ++j)                                     \
+            for (int k = 0; k <= TNKZ; ++k)                                    \
+                for (int i = 0; i <= NXP - 1; ++i) { STMT; }                   \
+    } while (0)
+    const double* DY = s->DY;
+    const double* DYF = s->DYF;
+    /* U1*U3 */
+    PRODUCT(JSTART, JEND, PH(U3, i, k, j) * PH(U1, i, k, j));
+    ACCUM(JSTART, JEND,
+          CX(CF1, i, k, j) = CX(CF1, i, k, j) - CI * s->KZ[k] * CX(CS1, i, k, j);
+          CX(CF3, i, k, j) = CX(CF3, i, k, j) - CI * s->KX[i] * CX(CS1, i, k, j));
+    /* U1*U1 */
+    PRODUCT(JSTART, JEND, PH(U1, i, k, j) * PH(U1, i, k, j));
+    ACCUM(JSTART, JEND, CX(CF1, i, k, j) = CX(CF1, i, k, j) - CI * s->KX[i] * CX(CS1, i, k, j));
+    /* U3*U3 */
+    PRODUCT(JSTART, JEND, PH(U3, i, k, j) * PH(U3, i, k, j));
+    ACCUM(JSTART, JEND, CX(CF3, i, k, j) = CX(CF3, i, k, j) - CI * s->KZ[k] * CX(CS1, i, k, j));
+    /* U1*U2 (U1 interpolated to GY) */
+    PRODUCT(2, NY, ((DYF[j] * PH(U1, i, k, j) + DYF[j - 1] * PH(U1, i, k, j - 1)) / (2. * DY[j])) *
+                       PH(U2, i, k, j));
+    ACCUM(2, NY, CX(CF2, i, k, j) = CX(CF2, i, k, j) - CI * s->KX[i] * CX(CS1, i, k, j));
+    /* U3*U2 */
+    PRODUCT(2, NY, ((DYF[j] * PH(U3, i, k, j) + DYF[j - 1] * PH(U3, i, k, j - 1)) / (2. * DY[j])) *
+                       PH(U2, i, k, j));
+    ACCUM(2, NY, CX(CF2, i, k, j) = CX(CF2, i, k, j) - CI * s->KZ[k] * CX(CS1, i, k, j));
+    /* d/dy(U1 U2) */
+    PRODUCT(JSTART, JEND,
+            (PH(U1, i, k, j + 1) * PH(U2, i, k, j + 1) + PH(U1, i, k, j) * PH(U2, i, k, j + 1) -
+             PH(U1, i, k, j) * PH(U2, i, k, j) - PH(U1, i, k, j - 1) * PH(U2, i, k, j)) /
+                (2.0 * DYF[j]));
+    ACCUM(JSTART, JEND, CX(CF1, i, k, j) = CX(CF1, i, k, j) - CX(CS1, i, k, j));
+    /* d/dy(U3 U2) */
+    PRODUCT(JSTART, JEND,
+            (PH(U3, i, k, j + 1) * PH(U2, i, k, j + 1) + PH(U3, i, k, j) * PH(U2, i, k, j + 1) -
+             PH(U3, i, k, j) * PH(U2, i, k, j) - PH(U3, i, k, j - 1) * PH(U2, i, k, j)) /
+                (2.0 * DYF[j]));
+    ACCUM(JSTART, JEND, CX(CF3, i, k, j) = CX(CF3, i, k, j) - CX(CS1, i, k, j));
+    /* d/dy(U2 U2) */
+    PRODUCT(2, NY,
+            (0.25 * pow(PH(U2, i, k, j) + PH(U2, i, k, j + 1), 2.0) -
+             0.25 * pow(PH(U2, i, k, j) + PH(U2, i, k, j - 1), 2.0)) /
+                DY[j]);
+    ACCUM(2, NY, CX(CF2, i, k, j) = CX(CF2, i, k, j) - CX(CS1, i, k, j));
+    /* USER_RHS_CHAN_PHYSICAL: empty hook (user_rhs.f:1-74). */
+
+    /* CR += beta h CF (channel.f:581-595) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = JSTART; j <= JEND; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CR1, i, k, j) = CX(CR1, i, k, j) + TEMP5 * CX(CF1, i, k, j);
+                CX(CR3, i, k, j) = CX(CR3, i, k, j) + TEMP5 * CX(CF3, i, k, j);
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i)
+                CX(CR2, i, k, j) = CX(CR2, i, k, j) + TEMP5 * CX(CF2, i, k, j);
+    orc_fft_xz_to_physical(s, CR1, R1, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CR2, R2, 2, NY);
+    orc_fft_xz_to_physical(s, CR3, R3, 0, NY + 1);
+    /* explicit half of CN in y (channel.f:606-626) */
+    const double nuv = p->nu_v_scale;
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = JSTART; j <= JEND; ++j)
+        for (int k = 0; k <= NZP - 1; ++k)
+            for (int i = 0; i <= NXM; ++i) {
+                PH(R1, i, k, j) = PH(R1, i, k, j) + TEMP1 * nuv *
+                    (((PH(U1, i, k, j + 1) - PH(U1, i, k, j)) / DY[j + 1] -
+                      (PH(U1, i, k, j) - PH(U1, i, k, j - 1)) / DY[j]) / DYF[j]);
+                PH(R3, i, k, j) = PH(R3, i, k, j) + TEMP1 * nuv *
+                    (((PH(U3, i, k, j + 1) - PH(U3, i, k, j)) / DY[j + 1] -
+                      (PH(U3, i, k, j) - PH(U3, i, k, j - 1)) / DY[j]) / DYF[j]);
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= NZP - 1; ++k)
+            for (int i = 0; i <= NXM; ++i)
+                PH(R2, i, k, j) = PH(R2, i, k, j) + TEMP1 * nuv *
+                    (((PH(U2, i, k, j + 1) - PH(U2, i, k, j)) / DYF[j] -
+                      (PH(U2, i, k, j) - PH(U2, i, k, j - 1)) / DYF[j - 1]) / DY[j]);
+
+    /* scalars (channel.f:666-840) */
+    for (int n = 0; n < s->NTH; ++n) {
+        double* THn = s->TH + (size_t)n * s->nreal;
+        double* CFTHn = s->CFTH + (size_t)n * s->nreal;
+        double* CRTHn = s->CRTH + (size_t)n * s->nreal;
+        double* RTHn = s->RTH + (size_t)n * s->nreal;
+        const int j0 = s->JSTART_TH[n], j1 = s->JEND_TH[n];
+        PRODUCT(j0, j1, PH(THn, i, k, j) * PH(U1, i, k, j));
+        ACCUM(j0, j1, CX(CFTHn, i, k, j) = CX(CFTHn, i, k, j) - CI * s->KX[i] * CX(CS1, i, k, j));
+        PRODUCT(j0, j1, PH(THn, i, k, j) * PH(U3, i, k, j));
+        ACCUM(j0, j1, CX(CFTHn, i, k, j) = CX(CFTHn, i, k, j) - CI * s->KZ[k] * CX(CS1, i, k, j));
+        PRODUCT(j0, j1,
+                (PH(THn, i, k, j + 1) * PH(U2, i, k, j + 1) + PH(THn, i, k, j) * PH(U2, i, k, j + 1) -
+                 PH(THn, i, k, j) * PH(U2, i, k, j) - PH(THn, i, k, j - 1) * PH(U2, i, k, j)) /
+                    (2.0 * DYF[j]));
+        ACCUM(j0, j1, CX(CFTHn, i, k, j) = CX(CFTHn, i, k, j) - CX(CS1, i, k, j));
+        ACCUM(j0, j1, CX(CRTHn, i, k, j) = CX(CRTHn, i, k, j) + TEMP5 * CX(CFTHn, i, k, j));
+        memcpy(CS1, CRTHn, sizeof(double) * s->nreal);
+        orc_fft_xz_to_physical(s, CS1, S1, 0, NY + 1);
+        memcpy(RTHn, S1, sizeof(double) * s->nreal);
+        const double c = (TEMP1 / p->pr[n]) * nuv;
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = j0; j <= j1; ++j)
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i)
+                    PH(RTHn, i, k, j) = PH(RTHn, i, k, j) + c *
+                        (((PH(THn, i, k, j + 1) - PH(THn, i, k, j)) / DY[j + 1] -
+                          (PH(THn, i, k, j) - PH(THn, i, k, j - 1)) / DY[j]) / DYF[j]);
+        cn_solve(s, SOLVE_TH, n, TEMP1);
+    }
+#undef PRODUCT
+#undef ACCUM
+    /* velocity solves: U2, U1, U3 (channel.f:842-1029) */
+    cn_solve(s, SOLVE_U2, 0, TEMP1);
+    cn_solve(s, SOLVE_U1, 0, TEMP1);
+    cn_solve(s, SOLVE_U3, 0, TEMP1);
+    /* CFL (channel.f:1037-1040) */
+    if (p->variable_dt && rk_step == 3 && (s->TIME_STEP % p->update_dt) == 0) orc_courant(s);
+    /* back to Fourier space (channel.f:1043-1050) */
+    orc_fft_xz_to_fourier(s, U1, CU1, 0, NY + 1);
+    orc_fft_xz_to_fourier(s, U2, CU2, 0, NY + 1);
+    orc_fft_xz_to_fourier(s, U3, CU3, 0, NY + 1);
+    for (int n = 0; n < s->NTH; ++n) {
+        memcpy(S1, s->TH + (size_t)n * s->nreal, sizeof(double) * s->nreal);
+        orc_fft_xz_to_fourier(s, S1, CS1, 0, NY + 1);
+        memcpy(s->CTH + (size_t)n * s->nreal, CS1, sizeof(double) * s->nreal);
+    }
+    orc_rem_div_chan(s);
+    /* pressure update with phi in CR1 (channel.f:1059-1065) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = JSTART; j <= JEND; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i)
+                CX(CP, i, k, j) = CX(CP, i, k, j) + CX(CR1, i, k, j) / TEMP4;
+    /* GHOST_CHAN_MPI: no-op for NPROCY = 1 */
+}
+
+/* ------------------------------------------------------------------------ */
+/* REM_DIV_CHAN (channel.f:1103-1214) with APPLY_BC_REM_DIV_MPI               */
+/* (mpi.f:1239-1278) and the complex MPI Thomas.  phi -> CR1 (J = 1..NY).     */
+/* ------------------------------------------------------------------------ */
+void orc_rem_div_chan(orc_state* s) {
+    const int NY = s->NY, NXP = s->NXP, TNKZ = s->TNKZ;
+    double *CU1 = s->U1, *CU2 = s->U2, *CU3 = s->U3, *CR1 = s->R1;
+    const int ld = NXP + 1;
+    const size_t msz = (size_t)ld * (NY + 2);
+#define MC(a, i, j) (a)[(size_t)(i) + (size_t)ld * (size_t)(j)]
+#pragma omp parallel num_threads(nthreads())
+    {
+        double* A = (double*)malloc(sizeof(double) * msz);
+        double* B = (double*)malloc(sizeof(double) * msz);
+        double* C = (double*)malloc(sizeof(double) * msz);
+        cplx* G = (cplx*)malloc(sizeof(cplx) * msz);
+        /* Column I = NXP is never initialised by the reference (local array,
+         * loops to NXP-1) yet is swept by the MPI Thomas; its result is never
+         * copied out.  Zero/identity here keeps it inert. */
+        for (size_t q = 0; q < msz; ++q) { A[q] = 0.0; B[q] = 1.0; C[q] = 0.0; G[q] = 0.0; }
+#pragma omp for schedule(static)
+        for (int k = 0; k <= TNKZ; ++k) {
+            for (int j = 1; j <= NY; ++j)
+                for (int i = 0; i <= NXP - 1; ++i) {
+                    MC(A, i, j) = 1. / (s->DY[j] * s->DYF[j]);
+                    MC(B, i, j) = -s->KX2[i] - s->KZ2[k] - 1. / (s->DY[j + 1] * s->DYF[j]) -
+                                  1. / (s->DY[j] * s->DYF[j]);
+                    MC(C, i, j) = 1. / (s->DY[j + 1] * s->DYF[j]);
+                }
+            for (int j = 1; j <= NY; ++j)
+                for (int i = 0; i <= NXP - 1; ++i)
+                    MC(G, i, j) = I * s->KX[i] * CX(CU1, i, k, j) +
+                                  (CX(CU2, i, k, j + 1) - CX(CU2, i, k, j)) / s->DYF[j] +
+                                  I * s->KZ[k] * CX(CU3, i, k, j);
+            for (int i = 0; i <= NXP - 1; ++i) {
+                if (k == 0 && i == 0) {
+                    MC(A, i, 1) = 0.; MC(B, i, 1) = 1.; MC(C, i, 1) = 0.; MC(G, i, 1) = 0.;
+                } else {
+                    MC(A, i, 1) = 0.; MC(B, i, 1) = 1.; MC(C, i, 1) = -1.; MC(G, i, 1) = 0.;
+                }
+                MC(A, i, NY) = 1.; MC(B, i, NY) = -1.; MC(C, i, NY) = 0.; MC(G, i, NY) = 0.;
+            }
+            thomas_complex_mpi(A, B, C, G, NY, NXP);
+            for (int j = 1; j <= NY; ++j)
+                for (int i = 0; i <= NXP - 1; ++i) CX(CR1, i, k, j) = MC(G, i, j);
+        }
+        free(A); free(B); free(C); free(G);
+    }
+#undef MC
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 1; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CU1, i, k, j) = CX(CU1, i, k, j) - I * s->KX[i] * CX(CR1, i, k, j);
+                CX(CU3, i, k, j) = CX(CU3, i, k, j) - I * s->KZ[k] * CX(CR1, i, k, j);
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i)
+                CX(CU2, i, k, j) = CX(CU2, i, k, j) - (CX(CR1, i, k, j) - CX(CR1, i, k, j - 1)) / s->DY[j];
+}
+
+/* ------------------------------------------------------------------------ */
+/* POISSON_P_CHAN (channel.f:1217-1453) with APPLY_BC_POISSON_MPI             */
+/* (mpi.f:1280-1315).                                                         */
+/* ------------------------------------------------------------------------ */
+void orc_poisson_p_chan(orc_state* s) {
+    const int NY = s->NY, NXP = s->NXP, TNKZ = s->TNKZ, NZP = s->NZP, NXM = s->NXM;
+    double *CU1 = s->U1, *CU2 = s->U2, *CU3 = s->U3, *CP = s->P;
+    double *CF1 = s->F1, *CF2 = s->F2, *CF3 = s->F3, *CS1 = s->S1;
+    double *F1 = s->F1, *F2 = s->F2, *F3 = s->F3;
+    const double* DYF = s->DYF;
+#define LOOPF(STMT)                                                           \
+    _Pragma("omp parallel for num_threads(nthreads())")                       \
+    for (int j = 2; j <= NY; ++j)                                             \
+        for (int k = 0; k <= TNKZ; ++k)                                       \
+            for (int i = 0; i <= NXP - 1; ++i) { STMT; }
+#define LOOPP(STMT)                                                           \
+    _Pragma("omp parallel for num_threads(nthreads())")                       \
+    for (int j = 2; j <= NY; ++j)                                             \
+        for (int k = 0; k <= NZP - 1; ++k)                                    \
+            for (int i = 0; i <= NXM; ++i) { STMT; }
+    LOOPF(CX(CF1, i, k, j) = I * s->KX[i] * CX(CU1, i, k, j);
+          CX(CF2, i, k, j) = (CX(CU2, i, k, j + 1) - CX(CU2, i, k, j)) / DYF[j];
+          CX(CF3, i, k, j) = I * s->KZ[k] * CX(CU3, i, k, j));
+    orc_fft_xz_to_physical(s, CF1, F1, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CF2, F2, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CF3, F3, 0, NY + 1);
+    LOOPP(PH(F1, i, k, j) = pow(PH(F1, i, k, j), 2.); PH(F2, i, k, j) = pow(PH(F2, i, k, j), 2.);
+          PH(F3, i, k, j) = pow(PH(F3, i, k, j), 2.));
+    orc_fft_xz_to_fourier(s, F1, CF1, 0, NY + 1);
+    orc_fft_xz_to_fourier(s, F2, CF2, 0, NY + 1);
+    orc_fft_xz_to_fourier(s, F3, CF3, 0, NY + 1);
+    LOOPF(CX(CS1, i, k, j) = CX(CF1, i, k, j) + CX(CF2, i, k, j) + CX(CF3, i, k, j));
+    LOOPF(CX(CF1, i, k, j) = (CX(CU1, i, k, j + 1) - CX(CU1, i, k, j - 1)) / (2. * DYF[j]);
+          CX(CF2, i, k, j) = I * s->KX[i] * 0.5 * (CX(CU2, i, k, j) + CX(CU2, i, k, j + 1)));
+    orc_fft_xz_to_physical(s, CF1, F1, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CF2, F2, 0, NY + 1);
+    LOOPP(PH(F1, i, k, j) = 2. * PH(F1, i, k, j) * PH(F2, i, k, j));
+    orc_fft_xz_to_fourier(s, F1, CF1, 0, NY + 1);
+    LOOPF(CX(CS1, i, k, j) = CX(CS1, i, k, j) + CX(CF1, i, k, j));
+    LOOPF(CX(CF1, i, k, j) = (CX(CU3, i, k, j + 1) - CX(CU3, i, k, j - 1)) / (2. * DYF[j]);
+          CX(CF2, i, k, j) = I * s->KZ[k] * 0.5 * (CX(CU2, i, k, j) + CX(CU2, i, k, j + 1)));
+    orc_fft_xz_to_physical(s, CF1, F1, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CF2, F2, 0, NY + 1);
+    LOOPP(PH(F1, i, k, j) = 2. * PH(F1, i, k, j) * PH(F2, i, k, j));
+    orc_fft_xz_to_fourier(s, F1, CF1, 0, NY + 1);
+    LOOPF(CX(CS1, i, k, j) = CX(CS1, i, k, j) + CX(CF1, i, k, j));
+    LOOPF(CX(CF1, i, k, j) = I * s->KZ[k] * CX(CU1, i, k, j);
+          CX(CF2, i, k, j) = I * s->KX[i] * CX(CU3, i, k, j));
+    orc_fft_xz_to_physical(s, CF1, F1, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CF2, F2, 0, NY + 1);
+    LOOPP(PH(F1, i, k, j) = 2. * PH(F1, i, k, j) * PH(F2, i, k, j));
+    orc_fft_xz_to_fourier(s, F1, CF1, 0, NY + 1);
+    LOOPF(CX(CS1, i, k, j) = CX(CS1, i, k, j) + CX(CF1, i, k, j));
+    for (int n = 0; n < s->NTH; ++n) {
+        double* CTHn = s->CTH + (size_t)n * s->nreal;
+        LOOPF(if (i != 0 || k != 0) CX(CS1, i, k, j) = CX(CS1, i, k, j) +
+                  s->p.ri[n] * (CX(CTHn, i, k, j + 1) - CX(CTHn, i, k, j - 1)) /
+                      (s->GYF[j + 1] - s->GYF[j - 1]));
+    }
+#undef LOOPF
+#undef LOOPP
+    const int ld = NXP + 1;
+    const size_t msz = (size_t)ld * (NY + 2);
+#define MC(a, i, j) (a)[(size_t)(i) + (size_t)ld * (size_t)(j)]
+#pragma omp parallel num_threads(nthreads())
+    {
+        double* A = (double*)malloc(sizeof(double) * msz);
+        double* B = (double*)malloc(sizeof(double) * msz);
+        double* C = (double*)malloc(sizeof(double) * msz);
+        cplx* G = (cplx*)malloc(sizeof(cplx) * msz);
+        for (size_t q = 0; q < msz; ++q) { A[q] = 0.0; B[q] = 1.0; C[q] = 0.0; G[q] = 0.0; }
+#pragma omp for schedule(static)
+        for (int k = 0; k <= TNKZ; ++k) {
+            for (int j = 2; j <= NY; ++j)
+                for (int i = 0; i <= NXP - 1; ++i) {
+                    MC(A, i, j) = 1. / (s->DY[j] * s->DYF[j]);
+                    MC(B, i, j) = -s->KX2[i] - s->KZ2[k] - 1. / (s->DY[j + 1] * s->DYF[j]) -
+                                  1. / (s->DY[j] * s->DYF[j]);
+                    MC(C, i, j) = 1. / (s->DY[j + 1] * s->DYF[j]);
+                    MC(G, i, j) = -1. * CX(CS1, i, k, j);
+                }
+            for (int i = 0; i <= NXP - 1; ++i) {
+                if (i == 0 && k == 0) {
+                    MC(B, i, 1) = 1.; MC(C, i, 1) = 0.; MC(G, i, 1) = 0.;
+                } else {
+                    MC(B, i, 1) = 1.; MC(C, i, 1) = -1.; MC(G, i, 1) = 0.;
+                }
+                MC(B, i, NY) = -1.; MC(A, i, NY) = 1.; MC(G, i, NY) = 0.;
+            }
+            thomas_complex_mpi(A, B, C, G, NY, NXP);
+            for (int j = 1; j <= NY; ++j)
+                for (int i = 0; i <= NXP - 1; ++i) CX(CP, i, k, j) = MC(G, i, j);
+        }
+        free(A); free(B); free(C); free(G);
+    }
+#undef MC
+}
+
+/* ------------------------------------------------------------------------ */
+/* COURANT (courant.f:1-66) on the physical velocity.                          */
+/* ------------------------------------------------------------------------ */
+void orc_courant(orc_state* s) {
+    const diablo_params* p = &s->p;
+    double dt = 999.0;
+    /* dx(1), dy(1): DX is uniform (channel.f:1566-1570) */
+    dt = fmin(dt, 0.5 * pow(fmin(s->DX, s->DY[1]), 2.0) / p->nu);
+    for (int n = 0; n < s->NTH; ++n) dt = fmin(dt, dt * p->nu / (p->nu / p->pr[n]));
+    if (p->i_ro != 0.0) dt = fmin(dt, 2.0 * s->PI / fabs(p->i_ro) / 20.0);
+    for (int n = 0; n < s->NTH; ++n)
+        if (p->ri[n] != 0.0) {
+            const double Nmax = sqrt(fabs(p->ri[n] * p->th_bc_ymin_c1[n]));
+            /* 0.1 is a default-real (single precision) literal in courant.f:32 */
+            dt = fmin(dt, (double)0.1f * 2.0 * s->PI / Nmax);
+        }
+    double dtv = dt;
+#pragma omp parallel for reduction(min : dtv) num_threads(nthreads())
+    for (int j = 1; j <= s->NY; ++j)
+        for (int k = 0; k <= s->NZP - 1; ++k)
+            for (int i = 0; i <= s->NXM; ++i) {
+                const double dt_x = p->cfl * s->DX / fabs(PH(s->U1, i, k, j));
+                const double dt_y = p->cfl * s->DY[j] / fabs(PH(s->U2, i, k, j));
+                const double dt_z = p->cfl * s->DZ / fabs(PH(s->U3, i, k, j));
+                dtv = fmin(dtv, fmin(dt_x, fmin(dt_y, dt_z)));
+            }
+    dt = dtv;
+    if (dt <= 0) s->DELTA_T = 0.0001;
+    else if (dt >= 999.) s->DELTA_T = 999.0;
+    else s->DELTA_T = dt;
+    s->H_BAR[0] = s->DELTA_T * (8.0 / 15.0);
+    s->H_BAR[1] = s->DELTA_T * (2.0 / 15.0);
+    s->H_BAR[2] = s->DELTA_T * (5.0 / 15.0);
+}
+
+/* ------------------------------------------------------------------------ */
+/* APPLY_BC_VEL_LOWER / _UPPER (channel.f:2285-2492), Fourier space.          */
+/* ------------------------------------------------------------------------ */
+void orc_apply_bc_vel(orc_state* s) {
+    const int NY = s->NY, NXP = s->NXP, TNKZ = s->TNKZ;
+    const diablo_params* p = &s->p;
+    double *CU1 = s->U1, *CU2 = s->U2, *CU3 = s->U3;
+    const double* DY = s->DY;
+    const double* DYF = s->DYF;
+    /* lower */
+    if (p->u_bc_ymin == 0) {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) { CX(CU1, i, k, 0) = 0; CX(CU1, i, k, 1) = 0; }
+        CX(CU1, 0, 0, 1) = p->u_bc_ymin_c1;
+        CX(CU1, 0, 0, 0) = p->u_bc_ymin_c1;
+    } else {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CU1, i, k, 1) = CX(CU1, i, k, 2);
+                CX(CU1, i, k, 0) = CX(CU1, i, k, 1);
+            }
+        CX(CU1, 0, 0, 1) = CX(CU1, 0, 0, 2) - DY[2] * p->u_bc_ymin_c1;
+        CX(CU1, 0, 0, 0) = CX(CU1, 0, 0, 1) - DY[1] * p->u_bc_ymin_c1;
+    }
+    if (p->w_bc_ymin == 0) {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) { CX(CU3, i, k, 0) = 0; CX(CU3, i, k, 1) = 0; }
+        CX(CU3, 0, 0, 1) = p->w_bc_ymin_c1;
+        CX(CU3, 0, 0, 0) = p->w_bc_ymin_c1;
+    } else {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CU3, i, k, 1) = CX(CU3, i, k, 2);
+                CX(CU3, i, k, 0) = CX(CU3, i, k, 1);
+            }
+        CX(CU3, 0, 0, 1) = CX(CU3, 0, 0, 2) - DY[2] * p->w_bc_ymin_c1;
+        CX(CU3, 0, 0, 0) = CX(CU3, 0, 0, 1) - DY[1] * p->w_bc_ymin_c1;
+    }
+    if (p->v_bc_ymin == 0) {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CU2, i, k, 1) = 2.0 * p->v_bc_ymin_c1 - CX(CU2, i, k, 2);
+                CX(CU2, i, k, 0) = CX(CU2, i, k, 1);
+            }
+    } else if (p->v_bc_ymin == 1) {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CU2, i, k, 1) = CX(CU2, i, k, 2);
+                CX(CU2, i, k, 0) = CX(CU2, i, k, 1);
+            }
+        CX(CU2, 0, 0, 1) = CX(CU2, 0, 0, 2) - DYF[1] * p->v_bc_ymin_c1;
+        CX(CU2, 0, 0, 0) = CX(CU2, 0, 0, 1) - DYF[1] * p->v_bc_ymin_c1;
+    } else if (p->v_bc_ymin == 2) {
+        CX(CU2, 0, 0, 1) = -CX(CU2, 0, 0, 2);
+    }
+    /* upper */
+    if (p->u_bc_ymax == 0) {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) { CX(CU1, i, k, NY) = 0; CX(CU1, i, k, NY + 1) = 0; }
+        CX(CU1, 0, 0, NY) = p->u_bc_ymax_c1;
+        CX(CU1, 0, 0, NY + 1) = p->u_bc_ymax_c1;
+    } else {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CU1, i, k, NY) = CX(CU1, i, k, NY - 1);
+                CX(CU1, i, k, NY + 1) = CX(CU1, i, k, NY);
+            }
+        CX(CU1, 0, 0, NY) = CX(CU1, 0, 0, NY - 1) + DY[NY] * p->u_bc_ymax_c1;
+        CX(CU1, 0, 0, NY + 1) = CX(CU1, 0, 0, NY) + DY[NY] * p->u_bc_ymax_c1;
+    }
+    if (p->w_bc_ymax == 0) {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) { CX(CU3, i, k, NY) = 0; CX(CU3, i, k, NY + 1) = 0; }
+        CX(CU3, 0, 0, NY) = p->w_bc_ymax_c1;
+        CX(CU3, 0, 0, NY + 1) = p->w_bc_ymax_c1;
+        CX(CU3, 0, 0, NY + 1) = 0.0;   /* "ghost cell not used" (channel.f:2434) */
+    } else {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CU3, i, k, NY) = CX(CU3, i, k, NY - 1);
+                CX(CU3, i, k, NY + 1) = CX(CU3, i, k, NY);
+            }
+        CX(CU3, 0, 0, NY) = CX(CU3, 0, 0, NY - 1) + DY[NY] * p->w_bc_ymax_c1;
+        CX(CU3, 0, 0, NY + 1) = CX(CU3, 0, 0, NY) + DY[NY] * p->w_bc_ymax_c1;
+    }
+    if (p->v_bc_ymax == 0) {
+        /* the reference loops over (k,i) but only ever writes the (0,0) entry
+         * (channel.f:2463-2467) */
+        CX(CU2, 0, 0, NY + 1) = 2.0 * p->v_bc_ymax_c1 - CX(CU2, 0, 0, NY);
+    } else if (p->v_bc_ymax == 1) {
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CU2, i, k, NY) = CX(CU2, i, k, NY - 1);
+                CX(CU2, i, k, NY + 1) = CX(CU2, i, k, NY);
+            }
+        CX(CU2, 0, 0, NY + 1) = CX(CU2, 0, 0, NY) + DY[NY] * p->v_bc_ymax_c1;
+    } else if (p->v_bc_ymax == 2) {
+        CX(CU2, 0, 0, NY + 1) = -CX(CU2, 0, 0, NY);
+    }
+}
+
+/* APPLY_BC_SCALAR_LOWER / _UPPER (channel.f:2723-2807). */
+void orc_apply_bc_scalar(orc_state* s) {
+    const int NY = s->NY, NXP = s->NXP, TNKZ = s->TNKZ;
+    const diablo_params* p = &s->p;
+    for (int n = 0; n < s->NTH; ++n) {
+        double* C = s->CTH + (size_t)n * s->nreal;
+        if (p->th_bc_ymin[n] == 0) {
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i) { CX(C, i, k, 0) = 0; CX(C, i, k, 1) = 0; }
+            CX(C, 0, 0, 1) = p->th_bc_ymin_c1[n];
+            CX(C, 0, 0, 0) = p->th_bc_ymin_c1[n];
+        } else {
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i) {
+                    CX(C, i, k, 1) = CX(C, i, k, 2);
+                    CX(C, i, k, 0) = CX(C, i, k, 1);
+                }
+            CX(C, 0, 0, 1) = CX(C, 0, 0, 2) - s->DY[2] * p->th_bc_ymin_c1[n];
+            CX(C, 0, 0, 0) = CX(C, 0, 0, 1) - s->DY[1] * p->th_bc_ymin_c1[n];
+        }
+        if (p->th_bc_ymax[n] == 0) {
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i) { CX(C, i, k, NY) = 0; CX(C, i, k, NY + 1) = 0; }
+            CX(C, 0, 0, NY) = p->th_bc_ymax_c1[n];
+            CX(C, 0, 0, NY + 1) = p->th_bc_ymax_c1[n];
+        } else {
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i) {
+                    CX(C, i, k, NY) = CX(C, i, k, NY - 1);
+                    CX(C, i, k, NY + 1) = CX(C, i, k, NY);
+                }
+            CX(C, 0, 0, NY) = CX(C, 0, 0, NY - 1) + s->DY[NY] * p->th_bc_ymax_c1[n];
+            CX(C, 0, 0, NY + 1) = CX(C, 0, 0, NY) + s->DY[NY] * p->th_bc_ymax_c1[n];
+        }
+    }
+}
+
+/* The time loop body of diablo.f:70-110 without statistics or I/O. */
+void orc_step(orc_state* s) {
+    s->TIME_STEP += 1;
+    for (int rk = 1; rk <= 3; ++rk) orc_rk_chan_1(s, rk);
+    s->TIME += s->DELTA_T;
+}
+
+/* ------------------------------------------------------------------------ */
+/* SAVE_STATS_CHAN profiles (save_stats.f:104-347, 452-536).  Computed from   */
+/* copies after APPLY_BC_VEL (save_stats.f:28-36), which is the only state    */
+/* change kept; the reference's FFT round trips only add round-off.           */
+/* ------------------------------------------------------------------------ */
+void orc_stats(orc_state* s, double* out) {
+    const int NY = s->NY, NX = s->NX, NZ = s->NZ, NZP = s->NZP, NXM = s->NXM;
+    const size_t ny2 = (size_t)NY + 2;
+    memset(out, 0, sizeof(double) * DIABLO_NSTATS * ny2);
+    orc_apply_bc_vel(s);
+    double* u[3];
+    for (int c = 0; c < 3; ++c) {
+        u[c] = (double*)malloc(sizeof(double) * s->nreal);
+        memcpy(u[c], c == 0 ? s->U1 : c == 1 ? s->U2 : s->U3, sizeof(double) * s->nreal);
+    }
+    double *ume = out + DIABLO_STAT_UME * ny2, *vme = out + DIABLO_STAT_VME * ny2,
+           *wme = out + DIABLO_STAT_WME * ny2;
+    for (size_t j = 0; j < ny2; ++j) {
+        ume[j] = creal(CX(s->U1, 0, 0, j));
+        vme[j] = creal(CX(s->U2, 0, 0, j));
+        wme[j] = creal(CX(s->U3, 0, 0, j));
+        out[DIABLO_STAT_CP * ny2 + j] = creal(CX(s->P, 0, 0, j));
+    }
+    for (int c = 0; c < 3; ++c) orc_fft_xz_to_physical(s, u[c], u[c], 0, NY + 1);
+    double* U1 = u[0]; double* U2 = u[1]; double* U3 = u[2];
+    const double nn = (double)((float)NZ * (float)NX);
+    for (int j = 1; j <= NY; ++j) {
+        double ur = 0, vr = 0, wr = 0, uv = 0, wv = 0, uw = 0, sh = 0;
+        for (int k = 0; k <= NZP - 1; ++k)
+            for (int i = 0; i <= NXM; ++i) {
+                ur += pow(PH(U1, i, k, j) - ume[j], 2.);
+                vr += 0.5 * (pow(PH(U2, i, k, j) - vme[j], 2.) + pow(PH(U2, i, k, j + 1) - vme[j + 1], 2.));
+                wr += pow(PH(U3, i, k, j) - wme[j], 2.);
+                uv += (s->DYF[j - 1] * (PH(U1, i, k, j) - ume[j]) + s->DYF[j] * (PH(U1, i, k, j - 1) - ume[j - 1])) /
+                      (2.0 * s->DY[j]) * (PH(U2, i, k, j) - vme[j]);
+                wv += (s->DYF[j - 1] * (PH(U3, i, k, j) - wme[j]) + s->DYF[j] * (PH(U3, i, k, j - 1) - wme[j - 1])) /
+                      (2.0 * s->DY[j]) * (PH(U2, i, k, j) - vme[j]);
+                uw += (PH(U1, i, k, j) - ume[j]) * (PH(U3, i, k, j) - wme[j]);
+                sh += pow((PH(U1, i, k, j + 1) - PH(U1, i, k, j - 1)) / (2.0 * s->DYF[j]), 2.0) +
+                      pow((PH(U3, i, k, j + 1) - PH(U3, i, k, j - 1)) / (2.0 * s->DYF[j]), 2.0);
+            }
+        out[DIABLO_STAT_URMS * ny2 + j] = sqrt(ur / nn);
+        out[DIABLO_STAT_VRMS * ny2 + j] = sqrt(vr / nn);
+        out[DIABLO_STAT_WRMS * ny2 + j] = sqrt(wr / nn);
+        out[DIABLO_STAT_UV * ny2 + j] = uv / nn;
+        out[DIABLO_STAT_UW * ny2 + j] = uw / nn;
+        out[DIABLO_STAT_WV * ny2 + j] = wv / nn;
+        out[DIABLO_STAT_DUDY * ny2 + j] = (ume[j] - ume[j - 1]) / (s->GYF[j] - s->GYF[j - 1]);
+        out[DIABLO_STAT_DWDY * ny2 + j] = (wme[j] - wme[j - 1]) / (s->GYF[j] - s->GYF[j - 1]);
+        out[DIABLO_STAT_SHEAR * ny2 + j] = sh / (double)(NX * NZ);
+    }
+    if (s->NTH > 0) {
+        double* th = (double*)malloc(sizeof(double) * s->nreal);
+        memcpy(th, s->CTH, sizeof(double) * s->nreal);
+        double* thme = out + DIABLO_STAT_THME * ny2;
+        for (size_t j = 0; j < ny2; ++j) thme[j] = creal(CX(s->CTH, 0, 0, j));
+        orc_fft_xz_to_physical(s, th, th, 0, NY + 1);
+        for (int j = 1; j <= NY; ++j) {
+            double a = 0, b = 0;
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i) {
+                    a += pow(fabs(PH(th, i, k, j) - thme[j]), 2.);
+                    b += (PH(th, i, k, j) - thme[j]) *
+                         (0.5 * (PH(U2, i, k, j) + PH(U2, i, k, j + 1)) - 0.5 * (vme[j] + vme[j + 1]));
+                }
+            out[DIABLO_STAT_THRMS * ny2 + j] = sqrt(a / nn);
+            out[DIABLO_STAT_THV * ny2 + j] = b / nn;
+            out[DIABLO_STAT_DTHDY * ny2 + j] = (thme[j] - thme[j - 1]) / (s->GYF[j] - s->GYF[j - 1]);
+        }
+        free(th);
+    }
+    for (int c = 0; c < 3; ++c) free(u[c]);
+}

@@ -1,0 +1,203 @@
+"""GPU parity: the CUDA library, called through its C ABI, against the CPU
+FP64 oracle on identical seeded inputs.
+
+Tolerances: the all-FP64 GPU path must agree with the oracle to 1e-10
+relative L2 per field (the GPU solves the CN systems per Fourier mode
+instead of per physical column, so agreement is to round-off, not bitwise);
+the FP32-split path to 1e-5 relative L2."""
+import os
+
+import numpy as np
+import pytest
+
+from diablo_b200 import grid as G, ics, layout, params as P
+from diablo_b200.channel import Channel, DiabloError
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL64 = 1e-10
+TOL32 = 1e-5
+
+
+def relerr(a, b):
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def blk(p, a):
+    return layout.dealiased(p, a)
+
+
+def state_errors(p, gpu: Channel, o: Oracle, with_cf=True):
+    s = gpu.download()
+    err = {}
+    for c in range(3):
+        err[f"cu{c + 1}"] = relerr(blk(p, s["cu"][c]), blk(p, o.cu[c]))
+    for n in range(p.n_th):
+        err[f"cth{n + 1}"] = relerr(blk(p, s["cth"][n]), blk(p, o.cth[n]))
+    err["cp"] = relerr(blk(p, s["cp"]), blk(p, o.cp))
+    if with_cf:
+        # CF rows outside the ranges the reference writes are not compared
+        for c in range(3):
+            err[f"cf{c + 1}"] = relerr(blk(p, s["cf"][c])[2:p.ny + 1], blk(p, o.cf[c])[2:p.ny + 1])
+    return err
+
+
+def kh_case(nx, ny, nz, precision=P.PREC_FP64, seed=7, amp=1e-2, stretched=False, dt=0.02):
+    p = P.kelvin_helmholtz(nx, ny, nz, precision=precision)
+    gy = G.create_grid(2, ny, 20.0, 1.5) if stretched else G.uniform_gy(ny, -10.0, 10.0)
+    g = G.channel_grid(gy)
+    u, th = ics.shear_layer(p, g, seed=seed, amp=amp)
+    return p, g, u, th, dt
+
+
+def start_pair(p, g, u, th, dt):
+    o = Oracle(p, g, dt)
+    o.init_from_physical(u, th)
+    gpu = Channel(p, g, dt)
+    gpu.upload([o.cu[0].copy(), o.cu[1].copy(), o.cu[2].copy()], o.cp.copy(), o.cth.copy())
+    return o, gpu
+
+
+@pytest.mark.parametrize("dims", [(32, 9, 24), (48, 7, 40), (64, 11, 96), (96, 5, 64), (160, 5, 160)])
+def test_fft_xz_to_fourier_and_back(dims):
+    nx, ny, nz = dims
+    p = P.kelvin_helmholtz(nx, ny, nz)
+    g = G.channel_grid(G.uniform_gy(ny, -1.0, 1.0))
+    o = Oracle(p, g, 0.01)
+    rng = np.random.default_rng(nx + nz)
+    v = layout.new_physical(p)
+    v[:, :nz, :nx] = rng.standard_normal((ny + 2, nz, nx))
+    ref = layout.new_fourier(p)
+    o.fft_xz_to_fourier(v.copy(), ref, 0, ny + 1)
+    with Channel(p, g, 0.01) as c:
+        vv = layout.new_fourier(p)
+        c.fft_xz_to_fourier(v, vv, 0, ny + 1)
+        assert relerr(blk(p, vv), blk(p, ref)) < 1e-13
+        assert np.all(vv[:, : p.tnkz + 1, p.nkx + 1:] == 0)
+        back = layout.new_physical(p)
+        c.fft_xz_to_physical(vv, back, 1, ny)
+        oback = layout.new_physical(p)
+        o.fft_xz_to_physical(ref.copy(), oback, 1, ny)
+        assert relerr(back[1:ny + 1, :nz, :nx], oback[1:ny + 1, :nz, :nx]) < 1e-13
+        assert np.all(back[0] == 0) and np.all(back[ny + 1] == 0)   # planes outside the range untouched
+
+
+def test_initial_projection_matches_oracle():
+    p, g, u, th, dt = kh_case(32, 17, 24, amp=0.1)
+    o = Oracle(p, g, dt)
+    o.init_from_physical(u, th)
+    with Channel(p, g, dt) as c:
+        c.init_from_physical(u, th)
+        err = state_errors(p, c, o, with_cf=False)
+        assert max(err.values()) < 1e-12, err
+        phi = c.download_phi()
+        assert relerr(blk(p, phi)[1:p.ny + 1], blk(p, o.phi)[1:p.ny + 1]) < 1e-10
+
+
+def test_apply_bc_vel_matches_oracle():
+    p, g, u, th, dt = kh_case(32, 17, 24)
+    p.u_bc_ymin, p.u_bc_ymin_c1, p.w_bc_ymax, p.w_bc_ymax_c1 = 0, 0.3, 0, -0.2
+    p.v_bc_ymax = 1
+    p.v_bc_ymax_c1 = 0.1
+    o = Oracle(p, g, dt)
+    o.init_from_physical(u, th)
+    with Channel(p, g, dt) as c:
+        c.upload([x.copy() for x in o.cu], o.cp.copy(), o.cth.copy())
+        c.apply_bc_vel()
+        o.apply_bc_vel()
+        err = state_errors(p, c, o, with_cf=False)
+        assert max(err.values()) < 1e-14, err
+
+
+@pytest.mark.parametrize("rk", [1, 2, 3])
+def test_single_substage_matches_oracle(rk):
+    p, g, u, th, dt = kh_case(48, 33, 36, amp=0.05, stretched=True)
+    o, c = start_pair(p, g, u, th, dt)
+    with c:
+        for r in range(1, rk + 1):
+            o.rk_chan_1(r)
+            c.rk_chan_1(r)
+        err = state_errors(p, c, o)
+        assert max(err.values()) < 1e-12, err
+
+
+def test_kh_steps_fp64_matches_oracle():
+    """Config-1 shear layer (64x65x64, Re=1000, Pr=1, Ri=0.1), 20 steps."""
+    p, g, u, th, dt = kh_case(64, 65, 64, amp=1e-3, dt=0.01)
+    o, c = start_pair(p, g, u, th, dt)
+    with c:
+        o.step(20)
+        c.step(20)
+        err = state_errors(p, c, o)
+        assert max(err.values()) < TOL64, err
+
+
+def test_channel_variable_dt_matches_oracle():
+    """Wall-bounded channel: Dirichlet walls, constant pressure gradient,
+    Dirichlet scalar, CFL-adaptive dt (COURANT at every third substage)."""
+    p = P.turbulent_channel(48, 33, 40, re_tau=180.0)
+    g = G.channel_grid(G.create_grid(1, p.ny, 2.0, 1.75))
+    u, th = ics.poiseuille(p, g, u_center=10.0, seed=3, noise=0.1)
+    o = Oracle(p, g, 1e-3)
+    o.init_from_physical(u, th)
+    with Channel(p, g, 1e-3) as c:
+        c.upload([x.copy() for x in o.cu], o.cp.copy(), o.cth.copy())
+        for _ in range(6):
+            o.step()
+            c.step()
+            _, dto, _, _ = o.time()
+            assert c.delta_t == pytest.approx(dto, rel=1e-12)
+        err = state_errors(p, c, o)
+        assert max(err.values()) < TOL64, err
+
+
+def test_fp32_split_error_bound():
+    p, g, u, th, dt = kh_case(64, 65, 64, precision=P.PREC_FP32SPLIT, amp=1e-3, dt=0.01)
+    p64 = p.copy()
+    p64.precision = P.PREC_FP64
+    o = Oracle(p64, g, dt)
+    o.init_from_physical(u, th)
+    with Channel(p, g, dt) as c:
+        c.upload([x.copy() for x in o.cu], o.cp.copy(), o.cth.copy())
+        o.step(20)
+        c.step(20)
+        err = state_errors(p, c, o, with_cf=False)
+        for k in ("cu1", "cu3", "cth1"):
+            assert err[k] < TOL32, err
+        assert err["cu2"] < 1e-3, err   # O(1e-3) noise field: relative error is larger
+
+
+def test_golden_regression_vectors():
+    ref = np.load(os.path.join(GOLDEN, "oracle_kh_small.npz"))
+    p = P.kelvin_helmholtz(24, 17, 16)
+    g = G.channel_grid(G.uniform_gy(p.ny, -10.0, 10.0))
+    with Channel(p, g, 0.05) as c:
+        cu = []
+        for k in range(3):
+            a = layout.new_fourier(p)
+            a[:, : p.tnkz + 1, : p.nkx + 1] = ref[f"init_cu{k}"]
+            cu.append(a)
+        cth = layout.new_fourier(p, 1)
+        cth[:, :, : p.tnkz + 1, : p.nkx + 1] = ref["init_cth"]
+        c.upload(cu, layout.new_fourier(p), cth)
+        c.step(3)
+        s = c.download()
+        for k in range(3):
+            assert relerr(blk(p, s["cu"][k]), ref[f"cu{k}"]) < TOL64
+        assert relerr(blk(p, s["cth"]), ref["cth"]) < TOL64
+        assert relerr(blk(p, s["cp"]), ref["cp"]) < TOL64
+
+
+def test_kernel_launch_counter_and_errors():
+    p, g, u, th, dt = kh_case(32, 17, 24)
+    with Channel(p, g, dt) as c:
+        c.init_from_physical(u, th)
+        n0 = c.kernel_launches()
+        c.rk_chan_1(1)
+        assert c.kernel_launches() - n0 >= 5
+        with pytest.raises(DiabloError):
+            c.rk_chan_2()
+        with pytest.raises(DiabloError):
+            c.fft_xz_to_physical(layout.new_fourier(p), layout.new_physical(p), 0, p.ny + 2)
