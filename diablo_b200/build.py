@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libdiablo_gpu.so")
 SOURCES = ["diablo_gpu.cu", "transforms.cu", "column.cu"]
-HEADERS = ["fft.cuh", "kernels.cuh", "launch.h"]
+HEADERS = ["fft.cuh", "fftct.cuh", "kernels.cuh", "launch.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

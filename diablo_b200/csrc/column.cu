@@ -52,70 +52,96 @@ struct CoefParams {
     double bc_c1[MAXF][2];
 };
 
-__global__ void k_cn_coef(CoefParams c, double* mult, double* piv, double* cup, double* bcv,
-                          signed char* kind) {
-    const int f = threadIdx.x;
-    if (f >= c.d.nf) return;
-    const int ny = c.d.ny, nyp = c.d.nyp;
-    double* L = mult + (size_t)f * nyp;
-    double* D = piv + (size_t)f * nyp;
-    double* U = cup + (size_t)f * nyp;
-    double* V = bcv + (size_t)f * nyp;
-    signed char* K = kind + (size_t)f * nyp;
+// Rows are set up in shared memory (one thread per field, in the order of
+// the reference), eliminated there, then copied out by the whole block.
+__global__ void __launch_bounds__(256) k_cn_coef(CoefParams c, double* mult, double* piv, double* cup,
+                                                 double* bcv, signed char* kind) {
+    extern __shared__ double sh[];
+    const int ny = c.d.ny, nyp = c.d.nyp, nf = c.d.nf;
+    double* sL = sh;
+    double* sD = sL + nf * nyp;
+    double* sU = sD + nf * nyp;
+    double* sV = sU + nf * nyp;
+    signed char* sK = reinterpret_cast<signed char*>(sV + nf * nyp);
     const double* DY = c.dy;
     const double* DYF = c.dyf;
-    auto setrow = [&](int j, double l, double dd, double u, double v) {
-        L[j] = l; D[j] = dd; U[j] = u; V[j] = v; K[j] = 1;
-    };
-    for (int j = 0; j < nyp; ++j) setrow(j, 0.0, 1.0, 0.0, 0.0);
-    const int lo = c.bc_type[f][0], hi = c.bc_type[f][1];
-    const double clo = c.bc_c1[f][0], chi = c.bc_c1[f][1];
-    if (f >= 3) {
-        const int n = f - 3;
-        const double cc = c.temp1 / c.pr[n] * c.nu_v_scale;
-        for (int j = c.jstart_th[n]; j <= ny; ++j) {
-            L[j] = -cc / (DY[j] * DYF[j]);
-            D[j] = 1. + cc / (DY[j + 1] * DYF[j]) + cc / (DY[j] * DYF[j]);
-            U[j] = -cc / (DY[j + 1] * DYF[j]);
-            K[j] = 0;
+    for (int e = threadIdx.x; e < nf * nyp; e += blockDim.x) {
+        const int f = e / nyp, j = e % nyp;
+        double l = 0.0, dd = 1.0, u = 0.0;
+        signed char k = 1;
+        if (f >= 3) {
+            const int n = f - 3;
+            const double cc = c.temp1 / c.pr[n] * c.nu_v_scale;
+            if (j >= c.jstart_th[n] && j <= ny) {
+                l = -cc / (DY[j] * DYF[j]);
+                dd = 1. + cc / (DY[j + 1] * DYF[j]) + cc / (DY[j] * DYF[j]);
+                u = -cc / (DY[j + 1] * DYF[j]);
+                k = 0;
+            }
+        } else if (f == 1) {
+            const double t = c.temp1 * c.nu_v_scale;
+            if (j >= 2 && j <= ny) {
+                l = -t / (DYF[j - 1] * DY[j]);
+                dd = 1. + t / (DYF[j] * DY[j]) + t / (DYF[j - 1] * DY[j]);
+                u = -t / (DYF[j] * DY[j]);
+                k = 0;
+            }
+        } else {
+            const double t = c.temp1 * c.nu_v_scale;
+            if (j >= 2 && j <= ny) {
+                l = -t / (DY[j] * DYF[j]);
+                dd = 1. - t * (-1. / (DY[j + 1] * DYF[j]) - 1. / (DY[j] * DYF[j]));
+                u = -t / (DY[j + 1] * DYF[j]);
+                k = 0;
+            }
         }
-        if (lo == 0) { setrow(0, 0., 1., 0., 0.); setrow(1, 0., 1., 0., clo); }
-        else { setrow(1, 0., -1., 1., DY[2] * clo); setrow(0, 0., 1., 0., 0.); }
-        if (hi == 0) { setrow(ny + 1, 0., 1., 0., 0.); setrow(ny, 0., 1., 0., chi); }
-        else { setrow(ny, -1., 1., 0., DY[ny] * chi); setrow(ny + 1, 0., 1., 0., 0.); }
-    } else if (f == 1) {
-        const double t = c.temp1 * c.nu_v_scale;
-        for (int j = 2; j <= ny; ++j) {
-            L[j] = -t / (DYF[j - 1] * DY[j]);
-            D[j] = 1. + t / (DYF[j] * DY[j]) + t / (DYF[j - 1] * DY[j]);
-            U[j] = -t / (DYF[j] * DY[j]);
-            K[j] = 0;
-        }
-        if (lo == 0) { setrow(1, 0., 1., 0., clo); setrow(2, 0., 1., 0., clo); }
-        else { setrow(1, 0., -1., 1., DYF[1] * clo); }
-        setrow(0, 0., 1., 0., 0.);
-        if (hi == 0) { setrow(ny + 1, 0., 1., 0., chi); setrow(ny, 0., 1., 0., chi); }
-        else { setrow(ny + 1, -1., 1., 0., DYF[ny] * chi); }
-    } else {
-        const double t = c.temp1 * c.nu_v_scale;
-        for (int j = 2; j <= ny; ++j) {
-            L[j] = -t / (DY[j] * DYF[j]);
-            D[j] = 1. - t * (-1. / (DY[j + 1] * DYF[j]) - 1. / (DY[j] * DYF[j]));
-            U[j] = -t / (DY[j + 1] * DYF[j]);
-            K[j] = 0;
-        }
-        if (lo == 0) { setrow(0, 0., 1., 0., 0.); setrow(1, 0., 1., 0., clo); }
-        else { setrow(0, 0., 1., 0., 0.); setrow(1, 0., -1., 1., DY[2] * clo); }
-        if (hi == 0) { setrow(ny + 1, 0., 1., 0., 0.); setrow(ny, 0., 1., 0., chi); }
-        else { setrow(ny, -1., 1., 0., DY[ny] * chi); setrow(ny + 1, 0., 1., 0., 0.); }
+        sL[e] = l; sD[e] = dd; sU[e] = u; sV[e] = 0.0; sK[e] = k;
     }
-    // THOMAS_FORWARD_REAL_MPI with NPROCY = 1: rows 1..NY+1 eliminated
-    // (mpi.f:668-694); L becomes the multiplier, D the pivot.
-    for (int j = 1; j <= ny + 1; ++j) {
-        L[j] = -L[j] / D[j - 1];
-        D[j] = D[j] + L[j] * U[j - 1];
+    __syncthreads();
+    const int f = threadIdx.x;
+    if (f < nf) {
+        double* L = sL + f * nyp;
+        double* D = sD + f * nyp;
+        double* U = sU + f * nyp;
+        double* V = sV + f * nyp;
+        signed char* K = sK + f * nyp;
+        auto setrow = [&](int j, double l, double dd, double u, double v) {
+            L[j] = l; D[j] = dd; U[j] = u; V[j] = v; K[j] = 1;
+        };
+        const int lo = c.bc_type[f][0], hi = c.bc_type[f][1];
+        const double clo = c.bc_c1[f][0], chi = c.bc_c1[f][1];
+        if (f >= 3) {
+            if (lo == 0) { setrow(0, 0., 1., 0., 0.); setrow(1, 0., 1., 0., clo); }
+            else { setrow(1, 0., -1., 1., DY[2] * clo); setrow(0, 0., 1., 0., 0.); }
+            if (hi == 0) { setrow(ny + 1, 0., 1., 0., 0.); setrow(ny, 0., 1., 0., chi); }
+            else { setrow(ny, -1., 1., 0., DY[ny] * chi); setrow(ny + 1, 0., 1., 0., 0.); }
+        } else if (f == 1) {
+            if (lo == 0) { setrow(1, 0., 1., 0., clo); setrow(2, 0., 1., 0., clo); }
+            else { setrow(1, 0., -1., 1., DYF[1] * clo); }
+            setrow(0, 0., 1., 0., 0.);
+            if (hi == 0) { setrow(ny + 1, 0., 1., 0., chi); setrow(ny, 0., 1., 0., chi); }
+            else { setrow(ny + 1, -1., 1., 0., DYF[ny] * chi); }
+        } else {
+            if (lo == 0) { setrow(0, 0., 1., 0., 0.); setrow(1, 0., 1., 0., clo); }
+            else { setrow(0, 0., 1., 0., 0.); setrow(1, 0., -1., 1., DY[2] * clo); }
+            if (hi == 0) { setrow(ny + 1, 0., 1., 0., 0.); setrow(ny, 0., 1., 0., chi); }
+            else { setrow(ny, -1., 1., 0., DY[ny] * chi); setrow(ny + 1, 0., 1., 0., 0.); }
+        }
+        // THOMAS_FORWARD_REAL_MPI with NPROCY = 1: rows 1..NY+1 eliminated
+        // (mpi.f:668-694); L becomes the multiplier, D the pivot.
+        double dprev = D[0];
+        for (int j = 1; j <= ny + 1; ++j) {
+            const double m = -L[j] / dprev;
+            L[j] = m;
+            dprev = D[j] + m * U[j - 1];
+            D[j] = dprev;
+        }
+        L[0] = 0.0;
     }
-    L[0] = 0.0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < nf * nyp; e += blockDim.x) {
+        mult[e] = sL[e]; piv[e] = sD[e]; cup[e] = sU[e]; bcv[e] = sV[e]; kind[e] = sK[e];
+    }
 }
 
 cudaError_t launch_cn_coef(const Dims& d, const CnArgs& a, double* mult, double* piv, double* cup,
@@ -137,7 +163,9 @@ cudaError_t launch_cn_coef(const Dims& d, const CnArgs& a, double* mult, double*
         c.bc_c1[f][0] = bc_c1[2 * f];
         c.bc_c1[f][1] = bc_c1[2 * f + 1];
     }
-    k_cn_coef<<<1, 32, 0, st>>>(c, mult, piv, cup, bcv, kind);
+    const size_t smem = (sizeof(double) * 4 + 1) * (size_t)d.nf * d.nyp;
+    cudaFuncSetAttribute(k_cn_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_cn_coef<<<1, 256, smem, st>>>(c, mult, piv, cup, bcv, kind);
     return cudaGetLastError();
 }
 
@@ -146,140 +174,187 @@ cudaError_t launch_cn_coef(const Dims& d, const CnArgs& a, double* mult, double*
 // CN y terms (channel.f:606-626, 737-747), and the CN solves (forward sweep
 // ascending, back substitution descending) for every field of one column.
 // ---------------------------------------------------------------------------
-template <int NTH, typename TN>
+// Shared per-row data of all columns, staged in shared memory per block.
+struct CnShared {
+    double* mult;
+    double* piv;
+    double* cup;
+    double* bcv;
+    double* dy;
+    double* dyf;
+    signed char* kind;
+};
+
+__device__ __forceinline__ CnShared cn_stage_coefs(const CnArgs& a, unsigned char* smem) {
+    const int n = a.d.nf * a.d.nyp, nyp = a.d.nyp;
+    CnShared s;
+    double* p = reinterpret_cast<double*>(smem);
+    s.mult = p; s.piv = p + n; s.cup = p + 2 * n; s.bcv = p + 3 * n;
+    s.dy = p + 4 * n; s.dyf = p + 4 * n + nyp;
+    s.kind = reinterpret_cast<signed char*>(p + 4 * n + 2 * nyp);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    for (int e = tid; e < n; e += nt) {
+        s.mult[e] = a.mult[e]; s.piv[e] = a.piv[e]; s.cup[e] = a.cup[e]; s.bcv[e] = a.bcv[e];
+        s.kind[e] = a.kind[e];
+    }
+    for (int e = tid; e < nyp; e += nt) { s.dy[e] = a.dy[e]; s.dyf[e] = a.dyf[e]; }
+    __syncthreads();
+    return s;
+}
+
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// One lane per (column, field): a warp holds CW = 32/FS columns and FS field
+// slots (lane = field*CW + column).  Each lane sweeps its own field; the
+// couplings between fields in the explicit terms (Coriolis, buoyancy,
+// background-gradient advection) are exchanged with warp shuffles.
+template <int FS, typename TN>
 __global__ void __launch_bounds__(128) k_cn(CnArgs a, const TN* __restrict__ nl) {
-    constexpr int F = 3 + NTH;
+    constexpr int CW = 32 / FS;
+    constexpr int NTHMAX = FS - 3 < 4 ? FS - 3 : 4;
+    extern __shared__ unsigned char smem_raw[];
+    const CnShared sc = cn_stage_coefs(a, smem_raw);
     const Dims& d = a.d;
-    const int kx = blockIdx.x * 32 + threadIdx.x;
-    const int m = blockIdx.y * 4 + threadIdx.y;
-    if (kx >= d.nkxp || m >= d.nkzt) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c = lane % CW, f = lane / CW;
+    const int ncol = d.nkxp * d.nkzt;
+    const int g = (blockIdx.x * 4 + warp) * CW + c;
+    const bool active = g < ncol && f < d.nf;
+    const int gg = g < ncol ? g : ncol - 1;
+    const int fe = f < d.nf ? f : d.nf - 1;
+    const int kx = gg % d.nkxp, m = gg / d.nkxp;
     const size_t ps = (size_t)d.nkzt * d.ldx;
     const size_t fs = ps * d.nyp;
-    const size_t col = (size_t)m * d.ldx + kx;
     const int ny = d.ny, nyp = d.nyp;
     const bool zero_mode = (kx == 0 && m == 0);
     const double KX = a.kx[kx], KZ = a.kz[m];
     const double k2 = pow(KX * KX + KZ * KZ, a.beta);
-    double2* cu = a.cu + col;
-    double2* cf = a.cf + col;
-    const double2* cp = a.cp + col;
-    const TN* nlc = nl + col;
+    double2* cu = a.cu + (size_t)fe * fs + (size_t)m * d.ldx + kx;
+    double2* cf = a.cf + (size_t)fe * fs + (size_t)m * d.ldx + kx;
+    const double2* cp = a.cp + (size_t)m * d.ldx + kx;
+    const TN* nlc = nl + (size_t)fe * fs + (size_t)m * d.ldx + kx;
     const double2 zero = make_double2(0.0, 0.0);
-
-    double2 w[F][3];     // CU(j-1), CU(j), CU(j+1) of every field
+    // per-lane coefficients of the explicit terms
+    double nuf = a.nu, cU1 = 0.0, cU3 = 0.0, cn_c = a.temp1 * a.nu_v_scale, Kf = 0.0;
+    double cth[NTHMAX > 0 ? NTHMAX : 1];
 #pragma unroll
-    for (int f = 0; f < F; ++f) {
-        w[f][0] = zero;
-        w[f][1] = cu[f * fs];
-        w[f][2] = cu[f * fs + ps];
+    for (int n = 0; n < NTHMAX; ++n) cth[n] = 0.0;
+    if (f == 0) {
+        cU3 = a.i_ro; Kf = KX;
+#pragma unroll
+        for (int n = 0; n < NTHMAX; ++n) cth[n] = n < d.nth ? a.ri[n] * a.grav_x : 0.0;
+    } else if (f == 2) {
+        cU1 = -a.i_ro; Kf = KZ;
+#pragma unroll
+        for (int n = 0; n < NTHMAX; ++n) cth[n] = n < d.nth ? a.ri[n] * a.grav_z : 0.0;
+    } else if (f >= 3 && f < d.nf) {
+        const int n = f - 3;
+        nuf = a.nu / a.pr[n];
+        cU1 = -a.drhodx[n];
+        cU3 = -a.drhodz[n];
+        cn_c = (a.temp1 / a.pr[n]) * a.nu_v_scale;
     }
-    double2 cpm = zero, cpj = cp[0];
-    double2 gprev[F], g0[F];
+    const bool isu2 = (f == 1);
+    const bool buoy_y = isu2 && !zero_mode;
+    const double force = (f == 0 && zero_mode) ? a.forcing : 0.0;
+    const int cf_lo = a.cf_lo[fe], cf_hi = a.cf_hi[fe], cb_lo = a.cb_lo[fe];
+    const bool rk1 = a.rk_step > 1;
+
+    double2 w0 = zero, w1 = zero, w2 = zero, nln = zero, cfn = zero;
+    if (active) {
+        w1 = cu[0];
+        w2 = cu[ps];
+        if (0 >= cf_lo) { nln = ldn<TN>(nlc); cfn = rk1 ? cf[0] : zero; }
+    }
+    double2 cpm = zero, cpj = cp[0], cpn = cp[ps];
+    double2 gprev = zero, g0 = zero;
 
     for (int j = 0; j <= ny + 1; ++j) {
-        const double dyj = a.dy[j], dyj1 = (j + 1 < nyp) ? a.dy[j + 1] : 1.0;
-        const double dyfj = a.dyf[j], dyfjm = (j > 0) ? a.dyf[j - 1] : 0.0;
+        const double2 nlj = nln, cfj = cfn;
+        if (active && j + 1 <= cf_hi && j + 1 >= cf_lo) {
+            nln = ldn<TN>(nlc + (size_t)(j + 1) * ps);
+            cfn = rk1 ? cf[(size_t)(j + 1) * ps] : zero;
+        }
+        const double dyj = sc.dy[j], dyj1 = (j + 1 < nyp) ? sc.dy[j + 1] : 1.0;
+        const double dyfj = sc.dyf[j], dyfjm = (j > 0) ? sc.dyf[j - 1] : 0.0;
+        // couplings from the other fields of this column
+        const double2 u1j = shfl2(w1, 0 * CW + c);
+        const double2 u3j = shfl2(w1, 2 * CW + c);
+        double2 cpl = cU1 * u1j + cU3 * u3j;
 #pragma unroll
-        for (int f = 0; f < F; ++f) {
-            const int row = f * nyp + j;
-            const int knd = a.kind[row];
-            double2 G = zero;
-            if (j >= a.cf_lo[f] && j <= a.cf_hi[f]) {
-                const double2 u = w[f][1];
-                double2 CF;
-                if (f == 0) {
-                    CF = (-a.nu * k2) * u + a.i_ro * w[2][1];
-#pragma unroll
-                    for (int n = 0; n < NTH; ++n) CF = CF + (a.ri[n] * a.grav_x) * w[3 + n][1];
-                } else if (f == 2) {
-                    CF = (-a.nu * k2) * u - a.i_ro * w[0][1];
-#pragma unroll
-                    for (int n = 0; n < NTH; ++n) CF = CF + (a.ri[n] * a.grav_z) * w[3 + n][1];
-                } else if (f == 1) {
-                    CF = (-a.nu * k2) * u;
-                    if (!zero_mode) {
-#pragma unroll
-                        for (int n = 0; n < NTH; ++n)
-                            CF = CF + (a.ri[n] * a.grav_y) *
-                                          ((dyfjm * w[3 + n][1] + dyfj * w[3 + n][0]) / (2.0 * dyj));
-                    }
-                } else {
-                    const int n = f - 3;
-                    CF = (-(a.nu / a.pr[n]) * k2) * u - a.drhodx[n] * w[0][1] - a.drhodz[n] * w[2][1];
-                }
-                CF = CF + ldn<TN>(nlc + f * fs + j * ps);
-                double2 R = u;
-                if (a.rk_step > 1) R = R + a.temp3 * cf[f * fs + j * ps];
-                if (a.store_cf) cf[f * fs + j * ps] = CF;
-                if (knd == 0) {
-                    if (f == 0) {
-                        R = R - a.temp4 * ik(KX, cpj);
-                        if (zero_mode) R.x -= a.forcing;
-                    } else if (f == 2) {
-                        R = R - a.temp4 * ik(KZ, cpj);
-                    } else if (f == 1) {
-                        R = R - a.temp4 * ((cpj - cpm) / dyj);
-                    }
-                    R = R + a.temp5 * CF;
-                    double2 ex;
-                    if (f == 1)
-                        ex = ((w[f][2] - u) / dyfj - (u - w[f][0]) / dyfjm) / dyj;
-                    else
-                        ex = ((w[f][2] - u) / dyj1 - (u - w[f][0]) / dyj) / dyfj;
-                    const double c = (f >= 3) ? (a.temp1 / a.pr[f - 3]) * a.nu_v_scale : a.temp1 * a.nu_v_scale;
-                    G = R + c * ex;
-                }
+        for (int n = 0; n < NTHMAX; ++n) {
+            const double2 thj = shfl2(w1, (3 + n) * CW + c);
+            const double2 thm = shfl2(w0, (3 + n) * CW + c);
+            cpl = cpl + cth[n] * thj;
+            if (buoy_y && n < d.nth)
+                cpl = cpl + (a.ri[n] * a.grav_y) * ((dyfjm * thj + dyfj * thm) / (2.0 * dyj));
+        }
+        const int row = fe * nyp + j;
+        const int knd = sc.kind[row];
+        double2 G = zero;
+        if (j >= cf_lo && j <= cf_hi) {
+            const double2 CF = (-nuf * k2) * w1 + cpl + nlj;
+            if (active && a.store_cf) cf[(size_t)j * ps] = CF;
+            if (knd == 0) {
+                double2 R = w1;
+                if (rk1) R = R + a.temp3 * cfj;
+                R = R - a.temp4 * ik(Kf, cpj);
+                if (isu2) R = R - a.temp4 * ((cpj - cpm) / dyj);
+                R.x -= force;
+                R = R + a.temp5 * CF;
+                double2 ex;
+                if (isu2) ex = ((w2 - w1) / dyfj - (w1 - w0) / dyfjm) / dyj;
+                else ex = ((w2 - w1) / dyj1 - (w1 - w0) / dyj) / dyfj;
+                G = R + cn_c * ex;
             }
-            if (knd != 0) G = zero_mode ? make_double2(a.bcv[row], 0.0) : zero;
-            if (j == 0) {
-                g0[f] = G;
-                gprev[f] = G;
-            } else {
-                G = G + a.mult[row] * gprev[f];
-                gprev[f] = G;
-                cu[f * fs + j * ps] = G;
-            }
+        }
+        if (knd != 0) G = zero_mode ? make_double2(sc.bcv[row], 0.0) : zero;
+        if (j == 0) {
+            g0 = G;
+            gprev = G;
+        } else {
+            G = G + sc.mult[row] * gprev;
+            gprev = G;
+            if (active) cu[(size_t)j * ps] = G;
         }
         // slide the window
-#pragma unroll
-        for (int f = 0; f < F; ++f) {
-            w[f][0] = w[f][1];
-            w[f][1] = w[f][2];
-            w[f][2] = (j + 2 <= ny + 1) ? cu[f * fs + (j + 2) * ps] : zero;
-        }
+        w0 = w1;
+        w1 = w2;
+        w2 = (active && j + 2 <= ny + 1) ? cu[(size_t)(j + 2) * ps] : zero;
         cpm = cpj;
-        cpj = (j + 1 <= ny + 1) ? cp[(j + 1) * ps] : zero;
+        cpj = cpn;
+        cpn = (j + 2 <= ny + 1) ? cp[(size_t)(j + 2) * ps] : zero;
     }
     // back substitution (THOMAS_BACKWARD_REAL_MPI, mpi.f:778-800)
-    double2 xn[F];
+    if (!active) return;
+    double2 xn = zero, gn = cu[(size_t)(ny + 1) * ps];
     for (int j = ny + 1; j >= 0; --j) {
-#pragma unroll
-        for (int f = 0; f < F; ++f) {
-            const int row = f * nyp + j;
-            const double2 gj = (j == 0) ? g0[f] : cu[f * fs + j * ps];
-            const double pv = a.piv[row];
-            double2 x;
-            if (j == ny + 1) x = gj / pv;
-            else if (pv != 0.0) x = (gj - a.cup[row] * xn[f]) / pv;
-            else x = zero;
-            xn[f] = x;
-            if (j >= a.cb_lo[f]) cu[f * fs + j * ps] = x;
-        }
+        const double2 gj = gn;
+        gn = (j - 1 >= 1) ? cu[(size_t)(j - 1) * ps] : g0;
+        const int row = fe * nyp + j;
+        const double pv = sc.piv[row];
+        double2 x;
+        if (j == ny + 1) x = gj / pv;
+        else if (pv != 0.0) x = (gj - sc.cup[row] * xn) / pv;
+        else x = zero;
+        xn = x;
+        if (j >= cb_lo) cu[(size_t)j * ps] = x;
     }
 }
 
 template <typename TN>
 cudaError_t launch_cn(const CnArgs& a, const TN* nl, cudaStream_t st) {
-    dim3 block(32, 4);
-    dim3 grid((a.d.nkxp + 31) / 32, (a.d.nkzt + 3) / 4);
-    switch (a.d.nth) {
-        case 0: k_cn<0, TN><<<grid, block, 0, st>>>(a, nl); break;
-        case 1: k_cn<1, TN><<<grid, block, 0, st>>>(a, nl); break;
-        case 2: k_cn<2, TN><<<grid, block, 0, st>>>(a, nl); break;
-        case 3: k_cn<3, TN><<<grid, block, 0, st>>>(a, nl); break;
-        case 4: k_cn<4, TN><<<grid, block, 0, st>>>(a, nl); break;
-        default: return cudaErrorInvalidValue;
-    }
+    const int ncol = a.d.nkxp * a.d.nkzt;
+    const size_t smem = (sizeof(double) * 4 + 1) * (size_t)a.d.nf * a.d.nyp + 2 * sizeof(double) * a.d.nyp + 16;
+    auto go = [&](auto kern, int cw) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<(ncol + 4 * cw - 1) / (4 * cw), 128, smem, st>>>(a, nl);
+    };
+    if (a.d.nf <= 4) go(k_cn<4, TN>, 8);
+    else if (a.d.nf <= 8) go(k_cn<8, TN>, 4);
+    else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 template cudaError_t launch_cn<cpx<float>>(const CnArgs&, const cpx<float>*, cudaStream_t);
@@ -291,77 +366,108 @@ template cudaError_t launch_cn<cpx<double>>(const CnArgs&, const cpx<double>*, c
 // of mpi.f:700-865; then the velocity correction and the pressure update
 // CP += phi/h (channel.f:1059-1065).
 // ---------------------------------------------------------------------------
+// Two lanes per column: the phi systems have real coefficients, so the real
+// and the imaginary part are solved by neighbouring lanes; the products with
+// i*k that mix the parts read the partner lane's value by a shuffle.
+__device__ __forceinline__ double part_of(double2 v, int part) { return part ? v.y : v.x; }
+
 __global__ void __launch_bounds__(128) k_remdiv(RemDivArgs a) {
     const Dims& d = a.d;
-    const int kx = blockIdx.x * 32 + threadIdx.x;
-    const int m = blockIdx.y * 4 + threadIdx.y;
-    if (kx >= d.nkxp || m >= d.nkzt) return;
+    const int part = threadIdx.x & 1;
+    const int ncol = d.nkxp * d.nkzt;
+    const int g = (blockIdx.x * 128 + threadIdx.x) >> 1;
+    const bool active = g < ncol;
+    const int gg = active ? g : ncol - 1;
+    const int kx = gg % d.nkxp, m = gg / d.nkxp;
     const size_t ps = (size_t)d.nkzt * d.ldx;
     const size_t fs = ps * d.nyp;
     const size_t col = (size_t)m * d.ldx + kx;
     const int ny = d.ny;
     const bool zero_mode = (kx == 0 && m == 0);
     const double KX = a.kx[kx], KZ = a.kz[m];
-    const double K2 = KX * KX + KZ * KZ;
-    double2* u1 = a.cu + col;
-    double2* u2 = a.cu + fs + col;
-    double2* u3 = a.cu + 2 * fs + col;
+    const double sgn = part ? 1.0 : -1.0;   // (i K v) of part: re -> -K v.y, im -> +K v.x
+    const double2* u1 = a.cu + col;
+    const double2* u2 = a.cu + fs + col;
+    const double2* u3 = a.cu + 2 * fs + col;
+    double* pu1 = reinterpret_cast<double*>(a.cu + col) + part;
+    double* pu2 = reinterpret_cast<double*>(a.cu + fs + col) + part;
+    double* pu3 = reinterpret_cast<double*>(a.cu + 2 * fs + col) + part;
+    double* pcp = reinterpret_cast<double*>(a.cp + col) + part;
+    double* pphi = reinterpret_cast<double*>(a.phi + col) + part;
     double* bs = a.bsc + col;
-    double2* gs = a.gsc + col;
-    const double2 zero = make_double2(0.0, 0.0);
-    // row 1 (BC), then forward elimination over rows 2..NY
-    double bprev = 1.0, cprev = zero_mode ? 0.0 : -1.0;
-    double2 gprev = zero;
-    bs[ps] = bprev;
-    gs[ps] = gprev;
-    double2 u2j = u2[2 * ps];
+    double* gs = reinterpret_cast<double*>(a.gsc + col) + part;
+    // row 1 (BC rows of APPLY_BC_REM_DIV_MPI), then rows 2..NY
+    double bprev = 1.0, cprev = zero_mode ? 0.0 : -1.0, gprev = 0.0;
+    if (active) {
+        if (part == 0) bs[ps] = bprev;
+        gs[2 * ps] = gprev;
+    }
+    double2 u2j = active ? u2[2 * ps] : make_double2(0, 0);
+    double2 u1n = active ? u1[2 * ps] : make_double2(0, 0);
+    double2 u3n = active ? u3[2 * ps] : make_double2(0, 0);
+    double2 u2n = active ? u2[3 * ps] : make_double2(0, 0);
     for (int j = 2; j <= ny; ++j) {
-        double A, B, C;
-        double2 G;
+        const double2 u1j = u1n, u3j = u3n, u2p = u2n;
+        if (active && j + 1 <= ny) {
+            u1n = u1[(size_t)(j + 1) * ps];
+            u3n = u3[(size_t)(j + 1) * ps];
+            u2n = u2[(size_t)(j + 2) * ps];
+        }
+        double A, B, C, G;
         if (j < ny) {
             A = 1. / (a.dy[j] * a.dyf[j]);
             B = -KX * KX - KZ * KZ - 1. / (a.dy[j + 1] * a.dyf[j]) - 1. / (a.dy[j] * a.dyf[j]);
             C = 1. / (a.dy[j + 1] * a.dyf[j]);
-            const double2 u2n = u2[(j + 1) * ps];
-            G = ik(KX, u1[j * ps]) + (u2n - u2j) / a.dyf[j] + ik(KZ, u3[j * ps]);
-            u2j = u2n;
+            G = sgn * KX * part_of(u1j, part ^ 1) + (part_of(u2p, part) - part_of(u2j, part)) / a.dyf[j] +
+                sgn * KZ * part_of(u3j, part ^ 1);
+            u2j = u2p;
         } else {
-            A = 1.; B = -1.; C = 0.; G = zero;
+            A = 1.; B = -1.; C = 0.; G = 0.;
         }
-        (void)K2;
         const double Ap = (bprev != 0.0) ? -A / bprev : 0.0;
         B = B + Ap * cprev;
         G = G + Ap * gprev;
-        bs[j * ps] = B;
-        gs[j * ps] = G;
+        if (active) {
+            if (part == 0) bs[(size_t)j * ps] = B;
+            gs[2 * (size_t)j * ps] = G;
+        }
         bprev = B;
         cprev = C;
         gprev = G;
     }
     // back substitution, corrections and pressure update, descending
-    double2 xn = zero;   // phi(j+1)
+    double xn = 0.0;   // phi(j+1) of this part
+    double bn = active ? bs[(size_t)ny * ps] : 1.0, gn = active ? gs[2 * (size_t)ny * ps] : 0.0;
     for (int j = ny; j >= 1; --j) {
-        const double B = bs[j * ps];
-        const double2 G = gs[j * ps];
-        double2 x;
-        if (j == ny) x = (B != 0.0) ? G / B : zero;
+        const double B = bn, G = gn;
+        if (active && j - 1 >= 1) {
+            bn = bs[(size_t)(j - 1) * ps];
+            gn = gs[2 * (size_t)(j - 1) * ps];
+        }
+        double x;
+        if (j == ny) x = (B != 0.0) ? G / B : 0.0;
         else {
             const double C = (j == 1) ? (zero_mode ? 0.0 : -1.0) : 1. / (a.dy[j + 1] * a.dyf[j]);
-            x = (B != 0.0) ? (G - C * xn) / B : zero;
+            x = (B != 0.0) ? (G - C * xn) / B : 0.0;
         }
-        a.phi[col + j * ps] = x;
-        u1[j * ps] = u1[j * ps] - ik(KX, x);
-        u3[j * ps] = u3[j * ps] - ik(KZ, x);
-        if (j + 1 <= ny) u2[(j + 1) * ps] = u2[(j + 1) * ps] - (xn - x) / a.dy[j + 1];
-        if (a.update_cp && j + 1 <= ny) a.cp[col + (j + 1) * ps] = a.cp[col + (j + 1) * ps] + a.inv_h * xn;
+        const double xo = __shfl_xor_sync(0xffffffffu, x, 1);   // the other part of phi(j)
+        if (active) {
+            pphi[2 * (size_t)j * ps] = x;
+            // CU1 -= i KX phi, CU3 -= i KZ phi  (part re: +K phi.im, part im: -K phi.re)
+            pu1[2 * (size_t)j * ps] -= sgn * KX * xo;
+            pu3[2 * (size_t)j * ps] -= sgn * KZ * xo;
+            if (j + 1 <= ny) {
+                pu2[2 * (size_t)(j + 1) * ps] -= (xn - x) / a.dy[j + 1];
+                if (a.update_cp) pcp[2 * (size_t)(j + 1) * ps] += a.inv_h * xn;
+            }
+        }
         xn = x;
     }
 }
 
 cudaError_t launch_remdiv(const RemDivArgs& a, cudaStream_t st) {
-    dim3 block(32, 4);
-    dim3 grid((a.d.nkxp + 31) / 32, (a.d.nkzt + 3) / 4);
-    k_remdiv<<<grid, block, 0, st>>>(a);
+    const int ncol = a.d.nkxp * a.d.nkzt;
+    k_remdiv<<<(2 * ncol + 127) / 128, 128, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -55,8 +55,9 @@ struct Handle {
     double *mult = nullptr, *piv = nullptr, *cup = nullptr, *bcv = nullptr;
     signed char* kind = nullptr;
     double* dtmin = nullptr;
-    FftPlan px, pz;
-    void *twx_d = nullptr, *twz_d = nullptr, *twx_f = nullptr, *twz_f = nullptr;
+    FftPlan pm, pz;   // NX/2-point complex plan (real x transforms), NZ-point plan
+    void *twn_d = nullptr, *twm_d = nullptr, *twz_d = nullptr;   // exp(-2 pi i k/n), n = NX, NX/2, NZ
+    void *twn_f = nullptr, *twm_f = nullptr, *twz_f = nullptr;
     int bc_type[2 * MAXF];
     double bc_c1[2 * MAXF];
     long long launches = 0;
@@ -89,7 +90,8 @@ void free_handle(Handle* h) {
     if (!h) return;
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
                     h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->mult, h->piv, h->cup,
-                    h->bcv, h->kind, h->dtmin, h->twx_d, h->twz_d, h->twx_f, h->twz_f};
+                    h->bcv, h->kind, h->dtmin, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
+                    h->twz_f};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (h->st) cudaStreamDestroy(h->st);
@@ -238,22 +240,27 @@ int validate(const diablo_params* p) {
     return DIABLO_OK;
 }
 
-int fp32_limits(const Handle* h) {
-    // shared memory and register budgets of the transform kernels
-    const int npair_in = (h->d.nf + 1) / 2;
-    int group = (12 * 256) / h->d.nx;
-    if (group > 6) group = 6;
-    if (npair_in > group) return fail(DIABLO_EINVAL, "too many fields for NX");
+int smem_limits(const Handle* h) {
+    // shared-memory budget of the products kernel (FP64 is the larger case)
+    const Dims& d = h->d;
+    const int group = products_group(d.nx);
+    const int m = d.nx / 2;
+    const size_t smem = sizeof(double) * (size_t)3 * d.nf * d.nx + 16 * (size_t)group * (m + m / 16 + 1);
+    if (group < 1 || smem > 227 * 1024) return fail(DIABLO_EINVAL, "NX too large for the number of fields");
+    // column kernels stage the per-row coefficients of every field
+    if ((33 * (size_t)d.nf + 16) * d.nyp > 200 * 1024) return fail(DIABLO_EINVAL, "NY too large");
     return DIABLO_OK;
 }
 
 template <typename T>
 int run_transforms(Handle* h) {
     const Dims& d = h->d;
-    const void* twx = std::is_same<T, float>::value ? h->twx_f : h->twx_d;
-    const void* twz = std::is_same<T, float>::value ? h->twz_f : h->twz_d;
+    const bool f = std::is_same<T, float>::value;
+    const void* twn = f ? h->twn_f : h->twn_d;
+    const void* twm = f ? h->twm_f : h->twm_d;
+    const void* twz = f ? h->twz_f : h->twz_d;
     CK(launch_zinv<T>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, twz, h->st));
-    CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, 32, h->d_dy, h->d_dyf, h->px, twx, h->st));
+    CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, 32, h->d_dy, h->d_dyf, h->pm, twm, twn, h->st));
     CK(launch_zfwd_nl<T>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->d_kx, h->d_kz, h->pz, twz, h->st));
     h->launches += 3;
     return DIABLO_OK;
@@ -299,8 +306,8 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
         h->jstart_th[n] = p->th_bc_ymin[n] == 1 ? 1 : 2;
         if (h->jstart_th[n] < h->jlo_prod) h->jlo_prod = h->jstart_th[n];
     }
-    if ((rc = fp32_limits(h))) { delete h; return rc; }
-    if (!make_plan(d.nx, &h->px) || !make_plan(d.nz, &h->pz)) { delete h; return fail(DIABLO_ERADIX, "bad radix"); }
+    if ((rc = smem_limits(h))) { delete h; return rc; }
+    if (!make_plan(d.nx / 2, &h->pm) || !make_plan(d.nz, &h->pz)) { delete h; return fail(DIABLO_ERADIX, "bad radix"); }
     // BC table: [field][lower, upper]
     for (int f = 0; f < 2 * MAXF; ++f) { h->bc_type[f] = 0; h->bc_c1[f] = 0.0; }
     h->bc_type[0] = p->u_bc_ymin; h->bc_type[1] = p->u_bc_ymax;
@@ -360,9 +367,11 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = cudaMemcpy(h->d_kz, kz.data(), sizeof(double) * d.nkzt, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(h->d_dy, dy, sizeof(double) * nyp, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(h->d_dyf, dyf, sizeof(double) * nyp, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) h->twx_d = make_twiddles<double>(d.nx, &e);
+    if (e == cudaSuccess) h->twn_d = make_twiddles<double>(d.nx, &e);
+    if (e == cudaSuccess) h->twm_d = make_twiddles<double>(d.nx / 2, &e);
     if (e == cudaSuccess) h->twz_d = make_twiddles<double>(d.nz, &e);
-    if (e == cudaSuccess) h->twx_f = make_twiddles<float>(d.nx, &e);
+    if (e == cudaSuccess) h->twn_f = make_twiddles<float>(d.nx, &e);
+    if (e == cudaSuccess) h->twm_f = make_twiddles<float>(d.nx / 2, &e);
     if (e == cudaSuccess) h->twz_f = make_twiddles<float>(d.nz, &e);
     if (e != cudaSuccess) {
         free_handle(h);
@@ -471,7 +480,7 @@ static int courant(Handle* h, double* delta_t, double* h_bar) {
     const double inf = HUGE_VAL;
     CK(cudaMemcpyAsync(h->dtmin, &inf, sizeof(double), cudaMemcpyHostToDevice, h->st));
     CK(launch_zinv<double>(d, h->cu, h->s_field, h->xb, h->x_field, 3, 0, d.nyp, h->pz, h->twz_d, h->st));
-    CK(launch_cfl(d, h->xb, h->x_field, h->px, h->twx_d, h->d_dy, p.cfl, h->dx, h->dz, h->dtmin, h->st));
+    CK(launch_cfl(d, h->xb, h->x_field, h->pm, h->twm_d, h->twn_d, h->d_dy, p.cfl, h->dx, h->dz, h->dtmin, h->st));
     h->launches += 2;
     double vmin = inf;
     CK(cudaMemcpyAsync(&vmin, h->dtmin, sizeof(double), cudaMemcpyDeviceToHost, h->st));
@@ -598,7 +607,7 @@ int diablo_gpu_fft_xz_to_fourier(void* handle, const double* v, double* vv, int 
     if (rc) return rc;
     const int np = jmax - jmin + 1;
     CK(copy_physical(h, h->phys, v, nullptr, jmin, np));
-    CK(launch_xfwd(d, h->phys, h->xb, jmin, np, h->px, h->twx_d, h->st));
+    CK(launch_xfwd(d, h->phys, h->xb, jmin, np, h->pm, h->twm_d, h->twn_d, h->st));
     CK(launch_zfwd_pack(d, h->xb, h->api_s, jmin, np, h->pz, h->twz_d, h->st));
     h->launches += 2;
     CK(copy_fourier(h, h->api_s, nullptr, vv, jmin, np));
@@ -623,7 +632,7 @@ int diablo_gpu_fft_xz_to_physical(void* handle, const double* vv, double* v, int
     const int np = jmax - jmin + 1;
     CK(copy_fourier(h, h->api_s, vv, nullptr, jmin, np));
     CK(launch_zinv<double>(d, h->api_s, h->s_field, h->xb, h->x_field, 1, jmin, np, h->pz, h->twz_d, h->st));
-    CK(launch_xinv(d, h->xb, h->phys, jmin, np, h->px, h->twx_d, h->st));
+    CK(launch_xinv(d, h->xb, h->phys, jmin, np, h->pm, h->twm_d, h->twn_d, h->st));
     h->launches += 2;
     CK(copy_physical(h, h->phys, nullptr, v, jmin, np));
     CK(cudaStreamSynchronize(h->st));

@@ -136,14 +136,39 @@ __device__ __forceinline__ cpx<T> twid(const cpx<T>* __restrict__ tw, int m, int
     return s > 0 ? conjg(w) : w;
 }
 
-// One Stockham stage over a batch of transforms held in shared memory.
-// Element p of transform b is at buf[p*ps + b*bs].  POS_FAST selects the
-// thread mapping: consecutive threads take consecutive butterflies of one
-// transform (contiguous transforms) or the same butterfly of consecutive
-// transforms (interleaved transforms).  VMAX bounds the complex values a
-// thread holds: n*nbatch <= VMAX*blockDim.x.
-template <typename T, int R, int VMAX, bool POS_FAST>
-__device__ __forceinline__ void stockham_stage(cpx<T>* buf, int n, int nbatch, int ps, int bs, int Ns,
+// Shared-memory layouts of a batch of transforms: element p of transform b.
+//  ColLayout<TX>  at p*TX + b: TX transforms interleaved (consecutive
+//                 threads take consecutive transforms: conflict-free).
+//  RowLayoutCT<M> / RowLayoutRT  at b*pitch + p + p/16: one transform per
+//                 row, with a pad word every 16 elements so that the strided
+//                 Stockham writes of the early stages hit distinct banks.
+template <int TX>
+struct ColLayout {
+    static constexpr bool kRowMajor = false;
+    static constexpr int kBatch = TX;
+    __device__ __forceinline__ int at(int p, int b) const { return p * TX + b; }
+};
+
+template <int M>
+struct RowLayoutCT {
+    static constexpr bool kRowMajor = true;
+    static constexpr int PITCH = M + M / 16 + 1;
+    __device__ __forceinline__ int at(int p, int b) const { return b * PITCH + p + (p >> 4); }
+};
+
+struct RowLayoutRT {
+    static constexpr bool kRowMajor = true;
+    int pitch;
+    __device__ __forceinline__ int at(int p, int b) const { return b * pitch + p + (p >> 4); }
+};
+
+__host__ __device__ constexpr int row_pitch(int m) { return m + m / 16 + 1; }
+
+// One Stockham stage over a batch of transforms held in shared memory, for
+// a length known only at run time.  VMAX bounds the complex values a thread
+// holds: n*nbatch <= VMAX*blockDim.x.
+template <typename T, int R, int VMAX, class L>
+__device__ __forceinline__ void stockham_stage(cpx<T>* buf, int n, int nbatch, const L& lay, int Ns,
                                                const cpx<T>* __restrict__ tw, int s) {
     constexpr int QMAX = (VMAX + R - 1) / R;
     const int nR = n / R;
@@ -155,12 +180,11 @@ __device__ __forceinline__ void stockham_stage(cpx<T>* buf, int n, int nbatch, i
         const int b = threadIdx.x + q * blockDim.x;
         if (b < nb) {
             int j, col;
-            if (POS_FAST) { j = b % nR; col = b / nR; }
+            if (L::kRowMajor) { j = b % nR; col = b / nR; }
             else { col = b % nbatch; j = b / nbatch; }
             const int k = j % Ns;
-            const cpx<T>* src = buf + (size_t)col * bs + (size_t)j * ps;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[q][r] = src[(size_t)r * nR * ps];
+            for (int r = 0; r < R; ++r) v[q][r] = buf[lay.at(j + r * nR, col)];
             if (Ns > 1) {
                 const int m = k * tstep;
 #pragma unroll
@@ -175,13 +199,12 @@ __device__ __forceinline__ void stockham_stage(cpx<T>* buf, int n, int nbatch, i
         const int b = threadIdx.x + q * blockDim.x;
         if (b < nb) {
             int j, col;
-            if (POS_FAST) { j = b % nR; col = b / nR; }
+            if (L::kRowMajor) { j = b % nR; col = b / nR; }
             else { col = b % nbatch; j = b / nbatch; }
             const int k = j % Ns;
             const int idxD = (j / Ns) * Ns * R + k;
-            cpx<T>* dst = buf + (size_t)col * bs;
 #pragma unroll
-            for (int r = 0; r < R; ++r) dst[(size_t)(idxD + r * Ns) * ps] = v[q][r];
+            for (int r = 0; r < R; ++r) buf[lay.at(idxD + r * Ns, col)] = v[q][r];
         }
     }
     __syncthreads();
@@ -189,18 +212,18 @@ __device__ __forceinline__ void stockham_stage(cpx<T>* buf, int n, int nbatch, i
 
 // Full transform of every batch member; callers synchronise before (data
 // in place) and the routine ends synchronised.
-template <typename T, int VMAX, bool POS_FAST>
-__device__ void smem_fft(cpx<T>* buf, int nbatch, int ps, int bs, const FftPlan& P,
+template <typename T, int VMAX, class L>
+__device__ void smem_fft(cpx<T>* buf, int nbatch, const L& lay, const FftPlan& P,
                          const cpx<T>* __restrict__ tw, int s) {
     int Ns = 1;
     for (int st = 0; st < P.nst; ++st) {
         const int R = P.rad[st];
         switch (R) {
-            case 8: stockham_stage<T, 8, VMAX, POS_FAST>(buf, P.n, nbatch, ps, bs, Ns, tw, s); break;
-            case 4: stockham_stage<T, 4, VMAX, POS_FAST>(buf, P.n, nbatch, ps, bs, Ns, tw, s); break;
-            case 2: stockham_stage<T, 2, VMAX, POS_FAST>(buf, P.n, nbatch, ps, bs, Ns, tw, s); break;
-            case 3: stockham_stage<T, 3, VMAX, POS_FAST>(buf, P.n, nbatch, ps, bs, Ns, tw, s); break;
-            default: stockham_stage<T, 5, VMAX, POS_FAST>(buf, P.n, nbatch, ps, bs, Ns, tw, s); break;
+            case 8: stockham_stage<T, 8, VMAX>(buf, P.n, nbatch, lay, Ns, tw, s); break;
+            case 4: stockham_stage<T, 4, VMAX>(buf, P.n, nbatch, lay, Ns, tw, s); break;
+            case 2: stockham_stage<T, 2, VMAX>(buf, P.n, nbatch, lay, Ns, tw, s); break;
+            case 3: stockham_stage<T, 3, VMAX>(buf, P.n, nbatch, lay, Ns, tw, s); break;
+            default: stockham_stage<T, 5, VMAX>(buf, P.n, nbatch, lay, Ns, tw, s); break;
         }
         Ns *= R;
     }

@@ -18,10 +18,11 @@ cudaError_t launch_zinv(const Dims& d, const double2* S, size_t s_fstride, void*
 // the 8 + 3*N_TH physical products of RK_CHAN_1 (channel.f:410-571,
 // 670-720) at planes jlo..jhi, forward x transform with 1/NX and truncation
 // to kx <= NKX (mpi.f:1493-1508) -> Y.
+// pm/twm: plan and table of the NX/2-point complex FFT; twn: table of NX.
 template <typename T>
 cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int jhi, int chunk,
-                            const double* dy, const double* dyf, const FftPlan& px, const void* twx,
-                            cudaStream_t st);
+                            const double* dy, const double* dyf, const FftPlan& pm, const void* twm,
+                            const void* twn, cudaStream_t st);
 
 // Per plane: forward z transform of every product, kz packing and 1/NZ
 // (mpi.f:1526-1540), then the derivative combination into the nonlinear
@@ -34,10 +35,10 @@ cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int 
 // Transform-API helpers (one field at a time, FP64):
 // X -> physical rows P (c2r, unnormalised, Nyquist and kx > NKX zero).
 cudaError_t launch_xinv(const Dims& d, const void* X, double* P, int j0, int nplanes,
-                        const FftPlan& px, const void* twx, cudaStream_t st);
+                        const FftPlan& pm, const void* twm, const void* twn, cudaStream_t st);
 // physical rows P -> X (r2c, 1/NX, truncation).
 cudaError_t launch_xfwd(const Dims& d, const double* P, void* X, int j0, int nplanes,
-                        const FftPlan& px, const void* twx, cudaStream_t st);
+                        const FftPlan& pm, const void* twm, const void* twn, cudaStream_t st);
 // X -> S (forward z transform, 1/NZ, kz packing) for one field.
 cudaError_t launch_zfwd_pack(const Dims& d, const void* X, double2* S, int j0, int nplanes,
                              const FftPlan& pz, const void* twz, cudaStream_t st);
@@ -52,9 +53,9 @@ cudaError_t launch_remdiv(const RemDivArgs& a, cudaStream_t st);
 
 // CFL minimum (courant.f:35-47) over planes 1..NY of the physical velocity
 // obtained from X (3 fields, FP64).  Result: atomically min-ed into *dtmin.
-cudaError_t launch_cfl(const Dims& d, const void* X, size_t x_fstride, const FftPlan& px,
-                       const void* twx, const double* dy, double cfl, double dx, double dz,
-                       double* dtmin, cudaStream_t st);
-
-// Fortran-layout helpers for the physical arrays of the transform API.
+cudaError_t launch_cfl(const Dims& d, const void* X, size_t x_fstride, const FftPlan& pm,
+                       const void* twm, const void* twn, const double* dy, double cfl, double dx,
+                       double dz, double* dtmin, cudaStream_t st);
+// rows transformed together by the products kernel for a given NX
+int products_group(int nx);
 }  // namespace dgpu
