@@ -21,8 +21,8 @@ from .params import DiabloParams, validate
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdiablo_gpu.so")
 
-DIABLO_OK, DIABLO_EINVAL, DIABLO_ERADIX, DIABLO_ECUDA, DIABLO_ENOTSUP, DIABLO_ENAN, DIABLO_ENOMEM = (
-    0, -1, -2, -3, -4, -5, -6)
+DIABLO_OK, DIABLO_EINVAL, DIABLO_ERADIX, DIABLO_ECUDA, DIABLO_ENOTSUP, DIABLO_ENAN, DIABLO_ENOMEM, DIABLO_ETIMEOUT = (
+    0, -1, -2, -3, -4, -5, -6, -7)
 NSTATS = 17
 
 # C entry points declared in include/diablo_gpu.h

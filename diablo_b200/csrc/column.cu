@@ -139,8 +139,11 @@ __global__ void __launch_bounds__(256) k_cn_coef(CoefParams c, double* mult, dou
         L[0] = 0.0;
     }
     __syncthreads();
+    // pivots are stored as reciprocals; a zero pivot maps to 0, which gives
+    // the x = 0 of the guarded back substitution (mpi.f:790-794)
     for (int e = threadIdx.x; e < nf * nyp; e += blockDim.x) {
-        mult[e] = sL[e]; piv[e] = sD[e]; cup[e] = sU[e]; bcv[e] = sV[e]; kind[e] = sK[e];
+        mult[e] = sL[e]; piv[e] = sD[e] != 0.0 ? 1.0 / sD[e] : 0.0; cup[e] = sU[e]; bcv[e] = sV[e];
+        kind[e] = sK[e];
     }
 }
 
@@ -170,197 +173,6 @@ cudaError_t launch_cn_coef(const Dims& d, const CnArgs& a, double* mult, double*
 }
 
 // ---------------------------------------------------------------------------
-// K4: Fourier RHS assembly (channel.f:77-293, 581-595), explicit half of the
-// CN y terms (channel.f:606-626, 737-747), and the CN solves (forward sweep
-// ascending, back substitution descending) for every field of one column.
-// ---------------------------------------------------------------------------
-// Shared per-row data of all columns, staged in shared memory per block.
-struct CnShared {
-    double* mult;
-    double* piv;
-    double* cup;
-    double* bcv;
-    double* dy;
-    double* dyf;
-    signed char* kind;
-};
-
-__device__ __forceinline__ CnShared cn_stage_coefs(const CnArgs& a, unsigned char* smem) {
-    const int n = a.d.nf * a.d.nyp, nyp = a.d.nyp;
-    CnShared s;
-    double* p = reinterpret_cast<double*>(smem);
-    s.mult = p; s.piv = p + n; s.cup = p + 2 * n; s.bcv = p + 3 * n;
-    s.dy = p + 4 * n; s.dyf = p + 4 * n + nyp;
-    s.kind = reinterpret_cast<signed char*>(p + 4 * n + 2 * nyp);
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
-    for (int e = tid; e < n; e += nt) {
-        s.mult[e] = a.mult[e]; s.piv[e] = a.piv[e]; s.cup[e] = a.cup[e]; s.bcv[e] = a.bcv[e];
-        s.kind[e] = a.kind[e];
-    }
-    for (int e = tid; e < nyp; e += nt) { s.dy[e] = a.dy[e]; s.dyf[e] = a.dyf[e]; }
-    __syncthreads();
-    return s;
-}
-
-__device__ __forceinline__ double2 shfl2(double2 v, int src) {
-    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
-}
-
-// One lane per (column, field): a warp holds CW = 32/FS columns and FS field
-// slots (lane = field*CW + column).  Each lane sweeps its own field; the
-// couplings between fields in the explicit terms (Coriolis, buoyancy,
-// background-gradient advection) are exchanged with warp shuffles.
-template <int FS, typename TN>
-__global__ void __launch_bounds__(128) k_cn(CnArgs a, const TN* __restrict__ nl) {
-    constexpr int CW = 32 / FS;
-    constexpr int NTHMAX = FS - 3 < 4 ? FS - 3 : 4;
-    extern __shared__ unsigned char smem_raw[];
-    const CnShared sc = cn_stage_coefs(a, smem_raw);
-    const Dims& d = a.d;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int c = lane % CW, f = lane / CW;
-    const int ncol = d.nkxp * d.nkzt;
-    const int g = (blockIdx.x * 4 + warp) * CW + c;
-    const bool active = g < ncol && f < d.nf;
-    const int gg = g < ncol ? g : ncol - 1;
-    const int fe = f < d.nf ? f : d.nf - 1;
-    const int kx = gg % d.nkxp, m = gg / d.nkxp;
-    const size_t ps = (size_t)d.nkzt * d.ldx;
-    const size_t fs = ps * d.nyp;
-    const int ny = d.ny, nyp = d.nyp;
-    const bool zero_mode = (kx == 0 && m == 0);
-    const double KX = a.kx[kx], KZ = a.kz[m];
-    const double k2 = pow(KX * KX + KZ * KZ, a.beta);
-    double2* cu = a.cu + (size_t)fe * fs + (size_t)m * d.ldx + kx;
-    double2* cf = a.cf + (size_t)fe * fs + (size_t)m * d.ldx + kx;
-    const double2* cp = a.cp + (size_t)m * d.ldx + kx;
-    const TN* nlc = nl + (size_t)fe * fs + (size_t)m * d.ldx + kx;
-    const double2 zero = make_double2(0.0, 0.0);
-    // per-lane coefficients of the explicit terms
-    double nuf = a.nu, cU1 = 0.0, cU3 = 0.0, cn_c = a.temp1 * a.nu_v_scale, Kf = 0.0;
-    double cth[NTHMAX > 0 ? NTHMAX : 1];
-#pragma unroll
-    for (int n = 0; n < NTHMAX; ++n) cth[n] = 0.0;
-    if (f == 0) {
-        cU3 = a.i_ro; Kf = KX;
-#pragma unroll
-        for (int n = 0; n < NTHMAX; ++n) cth[n] = n < d.nth ? a.ri[n] * a.grav_x : 0.0;
-    } else if (f == 2) {
-        cU1 = -a.i_ro; Kf = KZ;
-#pragma unroll
-        for (int n = 0; n < NTHMAX; ++n) cth[n] = n < d.nth ? a.ri[n] * a.grav_z : 0.0;
-    } else if (f >= 3 && f < d.nf) {
-        const int n = f - 3;
-        nuf = a.nu / a.pr[n];
-        cU1 = -a.drhodx[n];
-        cU3 = -a.drhodz[n];
-        cn_c = (a.temp1 / a.pr[n]) * a.nu_v_scale;
-    }
-    const bool isu2 = (f == 1);
-    const bool buoy_y = isu2 && !zero_mode;
-    const double force = (f == 0 && zero_mode) ? a.forcing : 0.0;
-    const int cf_lo = a.cf_lo[fe], cf_hi = a.cf_hi[fe], cb_lo = a.cb_lo[fe];
-    const bool rk1 = a.rk_step > 1;
-
-    double2 w0 = zero, w1 = zero, w2 = zero, nln = zero, cfn = zero;
-    if (active) {
-        w1 = cu[0];
-        w2 = cu[ps];
-        if (0 >= cf_lo) { nln = ldn<TN>(nlc); cfn = rk1 ? cf[0] : zero; }
-    }
-    double2 cpm = zero, cpj = cp[0], cpn = cp[ps];
-    double2 gprev = zero, g0 = zero;
-
-    for (int j = 0; j <= ny + 1; ++j) {
-        const double2 nlj = nln, cfj = cfn;
-        if (active && j + 1 <= cf_hi && j + 1 >= cf_lo) {
-            nln = ldn<TN>(nlc + (size_t)(j + 1) * ps);
-            cfn = rk1 ? cf[(size_t)(j + 1) * ps] : zero;
-        }
-        const double dyj = sc.dy[j], dyj1 = (j + 1 < nyp) ? sc.dy[j + 1] : 1.0;
-        const double dyfj = sc.dyf[j], dyfjm = (j > 0) ? sc.dyf[j - 1] : 0.0;
-        // couplings from the other fields of this column
-        const double2 u1j = shfl2(w1, 0 * CW + c);
-        const double2 u3j = shfl2(w1, 2 * CW + c);
-        double2 cpl = cU1 * u1j + cU3 * u3j;
-#pragma unroll
-        for (int n = 0; n < NTHMAX; ++n) {
-            const double2 thj = shfl2(w1, (3 + n) * CW + c);
-            const double2 thm = shfl2(w0, (3 + n) * CW + c);
-            cpl = cpl + cth[n] * thj;
-            if (buoy_y && n < d.nth)
-                cpl = cpl + (a.ri[n] * a.grav_y) * ((dyfjm * thj + dyfj * thm) / (2.0 * dyj));
-        }
-        const int row = fe * nyp + j;
-        const int knd = sc.kind[row];
-        double2 G = zero;
-        if (j >= cf_lo && j <= cf_hi) {
-            const double2 CF = (-nuf * k2) * w1 + cpl + nlj;
-            if (active && a.store_cf) cf[(size_t)j * ps] = CF;
-            if (knd == 0) {
-                double2 R = w1;
-                if (rk1) R = R + a.temp3 * cfj;
-                R = R - a.temp4 * ik(Kf, cpj);
-                if (isu2) R = R - a.temp4 * ((cpj - cpm) / dyj);
-                R.x -= force;
-                R = R + a.temp5 * CF;
-                double2 ex;
-                if (isu2) ex = ((w2 - w1) / dyfj - (w1 - w0) / dyfjm) / dyj;
-                else ex = ((w2 - w1) / dyj1 - (w1 - w0) / dyj) / dyfj;
-                G = R + cn_c * ex;
-            }
-        }
-        if (knd != 0) G = zero_mode ? make_double2(sc.bcv[row], 0.0) : zero;
-        if (j == 0) {
-            g0 = G;
-            gprev = G;
-        } else {
-            G = G + sc.mult[row] * gprev;
-            gprev = G;
-            if (active) cu[(size_t)j * ps] = G;
-        }
-        // slide the window
-        w0 = w1;
-        w1 = w2;
-        w2 = (active && j + 2 <= ny + 1) ? cu[(size_t)(j + 2) * ps] : zero;
-        cpm = cpj;
-        cpj = cpn;
-        cpn = (j + 2 <= ny + 1) ? cp[(size_t)(j + 2) * ps] : zero;
-    }
-    // back substitution (THOMAS_BACKWARD_REAL_MPI, mpi.f:778-800)
-    if (!active) return;
-    double2 xn = zero, gn = cu[(size_t)(ny + 1) * ps];
-    for (int j = ny + 1; j >= 0; --j) {
-        const double2 gj = gn;
-        gn = (j - 1 >= 1) ? cu[(size_t)(j - 1) * ps] : g0;
-        const int row = fe * nyp + j;
-        const double pv = sc.piv[row];
-        double2 x;
-        if (j == ny + 1) x = gj / pv;
-        else if (pv != 0.0) x = (gj - sc.cup[row] * xn) / pv;
-        else x = zero;
-        xn = x;
-        if (j >= cb_lo) cu[(size_t)j * ps] = x;
-    }
-}
-
-template <typename TN>
-cudaError_t launch_cn(const CnArgs& a, const TN* nl, cudaStream_t st) {
-    const int ncol = a.d.nkxp * a.d.nkzt;
-    const size_t smem = (sizeof(double) * 4 + 1) * (size_t)a.d.nf * a.d.nyp + 2 * sizeof(double) * a.d.nyp + 16;
-    auto go = [&](auto kern, int cw) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<(ncol + 4 * cw - 1) / (4 * cw), 128, smem, st>>>(a, nl);
-    };
-    if (a.d.nf <= 4) go(k_cn<4, TN>, 8);
-    else if (a.d.nf <= 8) go(k_cn<8, TN>, 4);
-    else return cudaErrorInvalidValue;
-    return cudaGetLastError();
-}
-template cudaError_t launch_cn<cpx<float>>(const CnArgs&, const cpx<float>*, cudaStream_t);
-template cudaError_t launch_cn<cpx<double>>(const CnArgs&, const cpx<double>*, cudaStream_t);
-
-// ---------------------------------------------------------------------------
 // K5: REM_DIV_CHAN (channel.f:1103-1214) per column with the boundary rows
 // of APPLY_BC_REM_DIV_MPI (mpi.f:1239-1278) and the guarded complex Thomas
 // of mpi.f:700-865; then the velocity correction and the pressure update
@@ -379,7 +191,7 @@ __global__ void __launch_bounds__(128) k_remdiv(RemDivArgs a) {
     const bool active = g < ncol;
     const int gg = active ? g : ncol - 1;
     const int kx = gg % d.nkxp, m = gg / d.nkxp;
-    const size_t ps = (size_t)d.nkzt * d.ldx;
+    const size_t ps = d.splane();
     const size_t fs = ps * d.nyp;
     const size_t col = (size_t)m * d.ldx + kx;
     const int ny = d.ny;

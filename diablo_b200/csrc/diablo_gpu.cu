@@ -55,6 +55,9 @@ struct Handle {
     double *mult = nullptr, *piv = nullptr, *cup = nullptr, *bcv = nullptr;
     signed char* kind = nullptr;
     double* dtmin = nullptr;
+    double* d_k2 = nullptr;       // (KX^2+KZ^2)**BETA per padded column
+    double* d_rows = nullptr;     // [RT_COUNT][nyp] reciprocal grid metrics
+    int* d_err = nullptr;         // kernel error flag (KERR_*)
     FftPlan pm, pz;   // NX/2-point complex plan (real x transforms), NZ-point plan
     void *twn_d = nullptr, *twm_d = nullptr, *twz_d = nullptr;   // exp(-2 pi i k/n), n = NX, NX/2, NZ
     void *twn_f = nullptr, *twm_f = nullptr, *twz_f = nullptr;
@@ -90,7 +93,7 @@ void free_handle(Handle* h) {
     if (!h) return;
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
                     h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->mult, h->piv, h->cup,
-                    h->bcv, h->kind, h->dtmin, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
+                    h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->d_err, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
                     h->twz_f};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -107,7 +110,7 @@ cudaError_t copy_fourier(Handle* h, double2* dev, const double* host_in, double*
     const size_t dpitch = sizeof(double2) * (size_t)d.ldx;
     cudaPitchedPtr hp = make_cudaPitchedPtr((void*)(host_in ? host_in : host_out), hpitch,
                                             (size_t)(h->nxp + 1), (size_t)(d.nz + 2));
-    cudaPitchedPtr dp = make_cudaPitchedPtr((void*)dev, dpitch, (size_t)d.ldx, (size_t)d.nkzt);
+    cudaPitchedPtr dp = make_cudaPitchedPtr((void*)dev, dpitch, (size_t)d.ldx, (size_t)d.nkzp);
     c.extent = make_cudaExtent(sizeof(double2) * (size_t)d.nkxp, (size_t)d.nkzt, (size_t)nplanes);
     if (host_in) {
         c.srcPtr = hp; c.dstPtr = dp;
@@ -144,7 +147,7 @@ __global__ void k_apply_bc_vel(Dims d, double2* cu, const double* dy, const doub
     const int kx = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     if (kx >= d.nkxp || m >= d.nkzt) return;
-    const size_t ps = (size_t)d.nkzt * d.ldx, fs = ps * d.nyp, col = (size_t)m * d.ldx + kx;
+    const size_t ps = d.splane(), fs = ps * d.nyp, col = (size_t)m * d.ldx + kx;
     const bool z0 = (kx == 0 && m == 0);
     const int ny = d.ny;
     double2* u1 = cu + col;
@@ -266,6 +269,20 @@ int run_transforms(Handle* h) {
     return DIABLO_OK;
 }
 
+
+// Read and clear the kernels' error flag (after a stream synchronisation).
+int check_device_flag(Handle* h) {
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (flag) {
+        CK(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->st));
+        CK(cudaStreamSynchronize(h->st));
+        return fail(DIABLO_ETIMEOUT, "a device pipeline wait timed out; results of the last calls are invalid");
+    }
+    return DIABLO_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -286,6 +303,7 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     d.np = 8 + 3 * p->n_th;
     d.nkx = p->nx / 3; d.nkz = p->nz / 3; d.tnkz = 2 * d.nkz;
     d.nkxp = d.nkx + 1; d.nkzt = d.tnkz + 1;
+    d.nkzp = (d.nkzt + 1) / 2 * 2;
     d.ldx = (d.nkxp + 15) / 16 * 16;
     d.nyp = p->ny + 2;
     h->nxp = p->nx / 2;
@@ -321,7 +339,7 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
         h->bc_c1[2 * (3 + n)] = p->th_bc_ymin_c1[n]; h->bc_c1[2 * (3 + n) + 1] = p->th_bc_ymax_c1[n];
     }
 
-    h->s_plane = (size_t)d.nkzt * d.ldx;
+    h->s_plane = d.splane();
     h->s_field = h->s_plane * d.nyp;
     h->x_plane = (size_t)d.nz * d.ldx;
     h->x_field = h->x_plane * d.nyp;
@@ -336,7 +354,7 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_dy, sizeof(double) * nyp);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_dyf, sizeof(double) * nyp);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_kx, sizeof(double) * d.ldx);
-    if (e == cudaSuccess) e = dmalloc((void**)&h->d_kz, sizeof(double) * d.nkzt);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_kz, sizeof(double) * d.nkzp);
     if (e == cudaSuccess) e = dmalloc((void**)&h->cu, sb * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->cf, sb * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->cp, sb);
@@ -353,18 +371,45 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = dmalloc((void**)&h->bcv, sizeof(double) * nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->kind, nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->dtmin, sizeof(double));
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_k2, sizeof(double) * d.splane());
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_rows, sizeof(double) * RT_COUNT * nyp);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_err, sizeof(int));
     if (e != cudaSuccess) {
         free_handle(h);
         return fail(e == cudaErrorMemoryAllocation ? DIABLO_ENOMEM : DIABLO_ECUDA,
                     std::string("device set-up: ") + cudaGetErrorString(e));
     }
     // wavenumbers (fft.f:77-100)
-    std::vector<double> kx(d.ldx, 0.0), kz(d.nkzt, 0.0);
+    std::vector<double> kx(d.ldx, 0.0), kz(d.nkzp, 0.0);
     for (int i = 0; i <= d.nkx; ++i) kx[i] = (double)i * (2.0 * h->pi) / p->lx;
     for (int k = 0; k <= d.nkz; ++k) kz[k] = (double)k * (2.0 * h->pi) / p->lz;
     for (int k = 1; k <= d.nkz; ++k) kz[d.tnkz + 1 - k] = -(double)k * (2.0 * h->pi) / p->lz;
-    e = cudaMemcpy(h->d_kx, kx.data(), sizeof(double) * d.ldx, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(h->d_kz, kz.data(), sizeof(double) * d.nkzt, cudaMemcpyHostToDevice);
+    // (KX2+KZ2)**BETA of the horizontal viscous term (channel.f:178)
+    std::vector<double> k2(d.splane(), 0.0);
+    for (int m = 0; m < d.nkzp; ++m)
+        for (int i = 0; i < d.ldx; ++i) k2[(size_t)m * d.ldx + i] = std::pow(kx[i] * kx[i] + kz[m] * kz[m], p->beta);
+    e = cudaMemcpy(h->d_k2, k2.data(), sizeof(double) * k2.size(), cudaMemcpyHostToDevice);
+    {
+        std::vector<double> rows((size_t)RT_COUNT * nyp, 0.0);
+        auto R = [&](int t, int j) -> double& { return rows[(size_t)t * nyp + j]; };
+        for (int j = 0; j < (int)nyp; ++j) {
+            const double DYj = dy[j], DYFj = dyf[j];
+            const double DYj1 = j + 1 < (int)nyp ? dy[j + 1] : 0.0, DYFjm = j > 0 ? dyf[j - 1] : 0.0;
+            auto inv = [](double v) { return v != 0.0 ? 1.0 / v : 0.0; };
+            R(RT_RDY, j) = inv(DYj);
+            R(RT_RDYF, j) = inv(DYFj);
+            R(RT_E1P, j) = inv(DYj1 * DYFj);
+            R(RT_E1M, j) = inv(DYj * DYFj);
+            R(RT_E2P, j) = inv(DYFj * DYj);
+            R(RT_E2M, j) = inv(DYFjm * DYj);
+            R(RT_BY0, j) = DYj != 0.0 ? DYFjm / (2.0 * DYj) : 0.0;
+            R(RT_BY1, j) = DYj != 0.0 ? DYFj / (2.0 * DYj) : 0.0;
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpy(h->d_rows, rows.data(), sizeof(double) * rows.size(), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_kx, kx.data(), sizeof(double) * d.ldx, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_kz, kz.data(), sizeof(double) * d.nkzp, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(h->d_dy, dy, sizeof(double) * nyp, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(h->d_dyf, dyf, sizeof(double) * nyp, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) h->twn_d = make_twiddles<double>(d.nx, &e);
@@ -433,7 +478,7 @@ int diablo_gpu_download_state(void* handle, double* cu1, double* cu2, double* cu
     }
     if (cp) CK(copy_fourier(h, h->cp, nullptr, cp, 0, d.nyp));
     CK(cudaStreamSynchronize(h->st));
-    return DIABLO_OK;
+    return check_device_flag(h);
 }
 
 int diablo_gpu_download_phi(void* handle, double* phi) {
@@ -549,12 +594,26 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     a.rk_step = rk_step;
     a.store_cf = 1;
     CK(launch_cn_coef(d, a, h->mult, h->piv, h->cup, h->bcv, h->kind, h->bc_type, h->bc_c1, h->st));
-    if (h->fp32) CK(launch_cn<cpx<float>>(a, (const cpx<float>*)h->nl, h->st));
-    else CK(launch_cn<cpx<double>>(a, (const cpx<double>*)h->nl, h->st));
+    const bool cfl = p.variable_dt && rk_step == 3 && (time_step % p.update_dt) == 0;
+    ColArgs ca;
+    ca.cn = a;
+    ca.k2 = h->d_k2;
+    ca.rows = h->d_rows;
+    ca.phi = h->phi;
+    ca.bsc = h->bsc;
+    ca.gsc = h->gsc;
+    ca.inv_h = 1.0 / TEMP4;
+    ca.project = cfl ? 0 : 1;     // COURANT sees the velocity before the projection
+    ca.update_cp = 1;
+    ca.store_phi = 1;
+    ca.err = h->d_err;
+    if (h->fp32) CK(launch_column<cpx<float>>(ca, (const cpx<float>*)h->nl, h->st));
+    else CK(launch_column<cpx<double>>(ca, (const cpx<double>*)h->nl, h->st));
     h->launches += 2;
-    if (p.variable_dt && rk_step == 3 && (time_step % p.update_dt) == 0) {
-        if ((rc = courant(h, delta_t, h_bar))) return rc;
-    }
+    if (!cfl) return DIABLO_OK;
+    // COURANT at the last substage (channel.f:1037-1040), then REM_DIV and the
+    // pressure update with the h of this substage
+    if ((rc = courant(h, delta_t, h_bar))) return rc;
     return rem_div(h, 1, 1.0 / TEMP4);
 }
 
@@ -654,7 +713,7 @@ int diablo_gpu_synchronize(void* handle) {
     Handle* h = (Handle*)handle;
     if (!h) return fail(DIABLO_EINVAL, "null handle");
     CK(cudaStreamSynchronize(h->st));
-    return DIABLO_OK;
+    return check_device_flag(h);
 }
 
 long long diablo_gpu_kernel_launches(void* handle) {

@@ -3,7 +3,8 @@
 // Device layouts (all row-major, fastest index last):
 //   spectral  S[f][J][m][kx]   complex, J in [0,NY+1], m in [0,TNKZ] (the
 //             packed kz of FFT_XZ_TO_FOURIER, mpi.f:1530-1539), kx in
-//             [0,NKX]; rows padded to ldx (a multiple of 16) with zeros.
+//             [0,NKX]; rows padded to ldx (a multiple of 16) and the kz rows
+//             of a plane padded to an even count nkzp, all padding zero.
 //             State (CU, CP, CF) is FP64; the nonlinear term NL is the
 //             transform type T.
 //   x-spectrum X[f][J][z][kx]  complex<T>: after the inverse z transform,
@@ -21,6 +22,9 @@ constexpr int MAXF = 3 + 4;   // fields: U1, U2, U3, TH(1..N_TH)
 struct Dims {
     int nx, ny, nz, nth, nf, np;
     int nkx, nkz, tnkz, nkxp, nkzt, ldx, nyp;
+    int nkzp;   // kz rows per plane in the S layout: nkzt padded to even, so
+                // that a plane (nkzp*ldx elements) is a multiple of 32 columns
+    __host__ __device__ size_t splane() const { return (size_t)nkzp * ldx; }
 };
 
 // Everything K4 (the column kernel) needs besides the arrays.
@@ -34,7 +38,7 @@ struct CnArgs {
     const double* dy;     // DY(0..NY+1)
     const double* dyf;    // DYF(0..NY+1)
     const double* mult;   // [nf][nyp] forward multipliers -A(j)/B'(j-1)
-    const double* piv;    // [nf][nyp] pivots B'(j)
+    const double* piv;    // [nf][nyp] reciprocal pivots 1/B'(j) (0 where B'(j) = 0)
     const double* cup;    // [nf][nyp] upper diagonal C(j)
     const double* bcv;    // [nf][nyp] RHS of BC rows for the (0,0) mode
     const signed char* kind;  // [nf][nyp] 0: interior row, 1: BC row
@@ -46,6 +50,37 @@ struct CnArgs {
     double forcing;       // value subtracted from CR1(0,0,j) (F_TYPE 1/2), already * TEMP4
     int rk_step;
     int store_cf;
+};
+
+// Per-row grid metrics shared by all columns (reciprocals computed once, so
+// the column sweeps multiply instead of divide):
+enum RowTab {
+    RT_RDY = 0,    // 1/DY(j)
+    RT_RDYF,       // 1/DYF(j)                          (0 where DYF(j) = 0)
+    RT_E1P,        // 1/(DY(j+1) DYF(j))   U1/U3/TH stencil, phi rows C(j)
+    RT_E1M,        // 1/(DY(j) DYF(j))     U1/U3/TH stencil, phi rows A(j)
+    RT_E2P,        // 1/(DYF(j) DY(j))     U2 stencil
+    RT_E2M,        // 1/(DYF(j-1) DY(j))   U2 stencil
+    RT_BY0,        // DYF(j-1)/(2 DY(j))   weight of TH(j) at GY(j)
+    RT_BY1,        // DYF(j)/(2 DY(j))     weight of TH(j-1) at GY(j)
+    RT_COUNT
+};
+
+// The fused column kernel (colfused.cu): CnArgs plus the projection.
+constexpr int COL_STAGES = 8;   // rows of every operand in flight per block
+
+struct ColArgs {
+    CnArgs cn;
+    const double* k2;     // (KX^2+KZ^2)**BETA per padded column [m][kx]
+    const double* rows;   // [RT_COUNT][nyp] row tables
+    double2* phi;         // S, phi (J = 1..NY), written when store_phi
+    double* bsc;          // scratch: pivots of the bottom-up phi elimination
+    double2* gsc;         // scratch: right-hand sides of that elimination
+    double inv_h;         // 1/TEMP4
+    int project;          // run REM_DIV (sweeps 2b and 3)
+    int update_cp;        // CP += phi/h on J = 2..NY
+    int store_phi;
+    int* err;             // device error flag (KERR_*)
 };
 
 struct RemDivArgs {

@@ -47,8 +47,11 @@ cudaError_t launch_zfwd_pack(const Dims& d, const void* X, double2* S, int j0, i
 cudaError_t launch_cn_coef(const Dims& d, const CnArgs& a, double* mult, double* piv, double* cup,
                            double* bcv, signed char* kind, const int* bc_type, const double* bc_c1,
                            cudaStream_t st);
+// Fused column kernel: RHS, CN solves, projection and pressure update.
 template <typename TN>
-cudaError_t launch_cn(const CnArgs& a, const TN* nl, cudaStream_t st);
+cudaError_t launch_column(const ColArgs& a, const TN* nl, cudaStream_t st);
+template <typename TN>
+size_t column_smem(const Dims& d);
 cudaError_t launch_remdiv(const RemDivArgs& a, cudaStream_t st);
 
 // CFL minimum (courant.f:35-47) over planes 1..NY of the physical velocity

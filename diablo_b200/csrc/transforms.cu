@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, const double2* __restrict_
     const int kx0 = blockIdx.x * TX;
     const int J = j0 + blockIdx.y;
     const int f = blockIdx.z;
-    const double2* src = S + (size_t)f * s_fstride + (size_t)J * nkzt * d.ldx;
+    const double2* src = S + (size_t)f * s_fstride + (size_t)J * d.splane();
     for (int e = threadIdx.x; e < nz * TX; e += 256) {
         const int z = e / TX, c = e % TX;
         const int kx = kx0 + c;
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __rest
         }
         __syncthreads();
     }
-    const size_t sp = (size_t)nkzt * d.ldx;     // plane stride of S
+    const size_t sp = d.splane();               // plane stride of S
     const size_t sf = (size_t)d.nyp * sp;       // field stride of S
     cpx<T>* dst = NL + (size_t)f * sf + (size_t)J * sp + kx0;
     for (int e = threadIdx.x; e < nkzt * TX; e += 256) dst[(size_t)(e / TX) * d.ldx + e % TX] = acc[e];
@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(256) k_zfwd_pack(Dims d, const cpx<double>* __
     __syncthreads();
     col_fft<double, 0, TX, -1>(buf, pz, twz);
     const double inv_nz = 1.0 / (double)nz;
-    double2* dst = S + (size_t)J * d.nkzt * d.ldx + kx0;
+    double2* dst = S + (size_t)J * d.splane() + kx0;
     for (int e = threadIdx.x; e < d.nkzt * TX; e += blockDim.x) {
         const int m = e / TX, c = e % TX;
         const cpx<double> v = buf[(size_t)m_to_z(m, d.nkz, nz, d.nkzt) * TX + c];

@@ -42,6 +42,7 @@ extern "C" {
 #define DIABLO_ENOTSUP      -4   /* feature not supported (RK_CHAN_2, LES) */
 #define DIABLO_ENAN         -5   /* a non-finite value was found in the state */
 #define DIABLO_ENOMEM       -6   /* device allocation failed */
+#define DIABLO_ETIMEOUT     -7   /* a bounded wait inside a kernel gave up */
 
 #define DIABLO_MAX_TH        4   /* largest N_TH the library accepts */
 
