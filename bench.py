@@ -1,0 +1,400 @@
+#!/usr/bin/env python3
+"""RK3 steps/s of DIABLO's channel timestep at 512x257x384 on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (diablo_b200.workloads.precision): channel 512x257x384 (NX x NY x
+NZ), tanh-stretched y (CS=1.75) on [-1,1], seeded shear-layer fields, one
+scalar, fixed dt; the headline number is the FP32-split path (transforms and
+products in FP32, solves, state and the projection in FP64).  Besides the
+device-timed value the line carries: the all-FP64 path's steps/s and its
+difference from the FP32-split state after the same steps, the end-to-end
+rate through the C ABI with host buffers, the roofline of the dominant
+kernel, a CPU baseline and the SM clocks seen during the timed region.
+
+Multi-GPU: independent replicas, one process per GPU (torchrun); no data-path
+collective (the single-instance path does not shard).  The reference arm
+times the CPU restatement of the reference (oracle/) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "RK3 steps/s at 512×257×384: FP32-split vs FP64 on 1 B200, err vs FP64 oracle"
+FALLBACK_HBM_GBS = 6650.0
+
+# DRAM traffic per launch of the column kernel, per plane of the S layout,
+# from the ncu capture summarised in profiles/column_kernel_512x65x384.md
+# (dram__bytes_read.sum + dram__bytes_write.sum / 67 planes); scaled to the
+# full grid by the number of planes (the kernel streams planes).
+COLUMN_TRAFFIC_PER_PLANE = {"fp32split": (829.99e6 + 728.24e6) / 67.0}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--grid", default="512,257,384", help="NX,NY,NZ")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "100"]
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 10:
+                continue
+            if self.uuid and self.uuid not in parts[1]:
+                continue
+            rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        smax = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i].lower() == "active"})
+        loaded = [s for s in sm if smax and s > 0.5 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------
+# algorithmic bytes per launch (per RK substage), the roofline numerators
+# --------------------------------------------------------------------------
+def algorithmic_bytes(p, prec: str) -> dict:
+    nkxp, nkzt, nyp, nz = p.nx // 3 + 1, 2 * (p.nz // 3) + 1, p.ny + 2, p.nz
+    nf, npr = 3 + p.n_th, 8 + 3 * p.n_th
+    tb = 8 if prec == "fp32split" else 16          # complex element of the transform path
+    A = nkxp * nkzt                                  # dealiased modes per plane
+    X = nz * nkxp                                    # x-spectrum entries per plane
+    planes_p = p.ny - 1                              # product planes 2..NY
+    col = (nf * 16 + (2.0 / 3.0) * nf * 16 + nf * tb + 16    # read CU, CF (rk>1), NL, CP
+           + nf * 16 + nf * 16 + 16)                          # write CU, CF, CP
+    return {
+        "zinv": nf * nyp * (A * 16 + X * tb),
+        "products": nf * nyp * X * tb + npr * planes_p * X * tb,
+        "zfwd_nl": npr * planes_p * X * tb + nf * planes_p * A * tb,
+        "column": col * A * nyp,
+    }
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def make_channel(w, prec, u=None, th=None):
+    from diablo_b200.channel import Channel
+    p = w.p.copy()
+    p.precision = prec
+    c = Channel(p, w.grid, w.dt)
+    if u is None:
+        u, th = w.initial_fields()
+    c.init_from_physical(u, th)
+    return c, u, th
+
+
+def timed_steps(c, steps, torch):
+    """Device time of `steps` time steps on the library's stream (ms)."""
+    stream = torch.cuda.ExternalStream(c.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    c.synchronize()
+    e0.record(stream)
+    c.step(steps)
+    e1.record(stream)
+    c.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def rel_errors(p, a, b):
+    from diablo_b200.layout import dealiased
+    out = {}
+    refs = [dealiased(p, b["cu"][k]) for k in range(3)]
+    uscale = float(np.sqrt(sum(np.linalg.norm(r) ** 2 for r in refs)))
+    for k in range(3):
+        d = np.linalg.norm(dealiased(p, a["cu"][k]) - refs[k])
+        out[f"cu{k + 1}"] = float(d / max(np.linalg.norm(refs[k]), 1e-300))
+        out[f"cu{k + 1}_vs_velocity_scale"] = float(d / uscale)
+    for n in range(p.n_th):
+        r = dealiased(p, b["cth"][n])
+        out[f"cth{n + 1}"] = float(np.linalg.norm(dealiased(p, a["cth"][n]) - r) / np.linalg.norm(r))
+    r = dealiased(p, b["cp"])
+    d = np.linalg.norm(dealiased(p, a["cp"]) - r)
+    out["cp"] = float(d / max(np.linalg.norm(r), 1e-300))
+    out["cp_vs_pressure_scale"] = float(d / (uscale ** 2 / math.sqrt(refs[0].size)))
+    return out
+
+
+def e2e_rate(c, steps, torch):
+    """Steps/s through the C ABI with pinned host buffers in the Fortran
+    layout: every step uploads CU1..3, CP, CTH, runs the three substages and
+    downloads the same arrays."""
+    from diablo_b200.layout import fourier_shape
+    p = c.p
+    shape = fourier_shape(p)
+    n = int(np.prod(shape)) * 2
+
+    def pinned():
+        t = torch.empty(n, dtype=torch.float64).pin_memory()
+        return t, t.numpy().view(np.complex128).reshape(shape)
+
+    bufs = [pinned() for _ in range(4 + max(p.n_th, 1))]
+    host = [b[1] for b in bufs]
+    c.download_into(host[0:3], host[3], host[4:4 + p.n_th])
+    per_field = (p.nx // 3 + 1) * (2 * (p.nz // 3) + 1) * (p.ny + 2) * 16
+    nfields = 4 + p.n_th
+    c.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        c.upload(host[0:3], host[3], np.stack(host[4:4 + p.n_th]) if p.n_th > 1 else host[4][None])
+        c.step(1)
+        c.download_into(host[0:3], host[3], host[4:4 + p.n_th])
+    el = time.perf_counter() - t0
+    return steps / el, nfields * per_field, nfields * per_field
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from diablo_b200 import build, workloads
+    from diablo_b200.params import PREC_FP32SPLIT, PREC_FP64
+
+    build.build()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    nx, ny, nz = (int(v) for v in args.grid.split(","))
+    w = workloads.precision(nx, ny, nz)
+    try:
+        uuid = str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        uuid = None
+
+    c32, u, th = make_channel(w, PREC_FP32SPLIT)
+    c32.step(args.warmup)
+    c32.synchronize()
+    if dist:
+        dist.barrier()
+    n0 = c32.kernel_launches()
+    with ClockSampler(uuid) as clk:
+        ms = timed_steps(c32, args.steps, torch)
+    launches = c32.kernel_launches() - n0
+    t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1e3)
+
+    # per-kernel device time of one step (events on the launching stream)
+    c32.set_profiling(True)
+    c32.step(1)
+    ktimes = c32.kernel_times()
+    c32.set_profiling(False)
+
+    # all-FP64 path from the same initial fields: rate and state difference
+    fp64 = None
+    if not args.no_fp64:
+        c64, _, _ = make_channel(w, PREC_FP64, u, th)
+        c64.step(args.warmup)
+        ms64 = timed_steps(c64, args.steps, torch)
+        s32 = c32.download()
+        # re-run FP32-split from the same start for exactly the same steps
+        c32b, _, _ = make_channel(w, PREC_FP32SPLIT, u, th)
+        c32b.step(args.warmup + args.steps)
+        errs = rel_errors(w.p, c32b.download(), c64.download())
+        fp64 = {"steps_per_s": args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
+                "err_fp32split_vs_fp64_after_steps": args.warmup + args.steps, "err": errs}
+        del s32
+        c64.close()
+        c32b.close()
+
+    e2e = None
+    if not args.no_e2e:
+        rate, bi, bo = e2e_rate(c32, max(3, min(args.steps, 20)), torch)
+        e2e = {"value": world * rate, "unit": "steps/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo}
+
+    peak, peak_kind = hbm_peak()
+    alg = algorithmic_bytes(w.p, "fp32split")
+    dom = max(ktimes, key=lambda k: ktimes[k][1])
+    dom_launches, dom_ms = ktimes[dom]
+    avg_s = dom_ms / dom_launches / 1e3
+    achieved = alg.get(dom, 0.0) / avg_s / 1e9 if dom in alg else None
+    traffic = None
+    if dom == "column":
+        traffic = COLUMN_TRAFFIC_PER_PLANE["fp32split"] * (w.p.ny + 2)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": traffic, "algorithmic_bytes_per_launch": alg.get(dom),
+                "avg_launch_ms": avg_s * 1e3}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(w, nx, ny, nz)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    kernel_ms = {k: round(v[1] / max(v[0], 1) * 3, 4) for k, v in ktimes.items()}
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 transforms/products + f64 solves/state",
+        "data": "synthetic (seeded shear layer, splitmix64/Box-Muller)",
+        "config": {"workload": f"channel {nx}x{ny}x{nz}, tanh y CS=1.75, shear layer delta=0.1, FP32-split",
+                   "grid": [nx, ny, nz], "n_th": w.p.n_th, "dt": w.dt, "nu": w.p.nu, "ri": w.p.ri[0],
+                   "lx": w.p.lx, "lz": w.p.lz, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (each state field 187 MB)"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk.summary(), "fp64": fp64,
+        "fp32_split_speedup_vs_fp64": (value / world) / fp64["steps_per_s"] if fp64 else None,
+        "kernel_ms_per_step": kernel_ms,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# CPU: the oracle (a restatement of the reference, OpenMP) on the host cores
+# --------------------------------------------------------------------------
+SAMPLE_NY = 33
+
+
+def cpu_sample(w, nx, ny, nz, steps: int = 2):
+    """One bounded sample: full NX x NZ planes, a y-subset of SAMPLE_NY
+    planes, `steps` RK steps after one untimed step; per-step time scaled by
+    (NY+2)/(SAMPLE_NY+2), the work of the path being proportional to the
+    number of planes."""
+    from diablo_b200 import workloads
+    from oracle.oracle import Oracle
+
+    nys = min(SAMPLE_NY, ny)
+    ws = workloads.precision(nx, nys, nz)
+    o = Oracle(ws.p, ws.grid, ws.dt)
+    u, th = ws.initial_fields()
+    o.init_from_physical(u, th)
+    o.step(1)
+    t0 = time.perf_counter()
+    o.step(steps)
+    el = (time.perf_counter() - t0) / steps
+    scale = (ny + 2) / (nys + 2)
+    cores = os.cpu_count() or 1
+    return {"value": 1.0 / (el * scale), "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} RK3 steps of {nx}x{nys}x{nz} (full x-z planes, {nys + 2} of {ny + 2} y-planes), "
+                      f"{el:.3f} s/step scaled x{scale:.2f} to {ny + 2} planes; OpenMP on {cores} threads"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from diablo_b200 import workloads
+    from oracle.oracle import Oracle, build as build_oracle
+
+    build_oracle()
+    nx, ny, nz = (int(v) for v in args.grid.split(","))
+    nys = min(SAMPLE_NY, ny)
+    ws = workloads.precision(nx, nys, nz)
+    o = Oracle(ws.p, ws.grid, ws.dt)
+    u, th = ws.initial_fields()
+    o.init_from_physical(u, th)
+    o.step(max(1, min(args.warmup, 2)))
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    el = (time.perf_counter() - t0) / args.steps
+    scale = (ny + 2) / (nys + 2)
+    value = 1.0 / (el * scale)
+    cores = os.cpu_count() or 1
+    sample = (f"each step: one RK3 step of {nx}x{nys}x{nz} ({nys + 2} of {ny + 2} y-planes) timed and scaled "
+              f"x{scale:.2f}; OpenMP on {cores} threads")
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded shear layer)", "impl": "reference",
+        "config": {"workload": f"channel {nx}x{ny}x{nz}, tanh y CS=1.75, shear layer delta=0.1",
+                   "grid": [nx, ny, nz], "parallelism": "cpu"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

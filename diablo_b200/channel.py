@@ -32,7 +32,9 @@ EXPORTS = [
     "diablo_gpu_fft_xz_to_physical", "diablo_gpu_rem_div_chan", "diablo_gpu_download_phi",
     "diablo_gpu_poisson_p_chan", "diablo_gpu_apply_bc_vel", "diablo_gpu_courant", "diablo_gpu_stats",
     "diablo_gpu_synchronize", "diablo_gpu_kernel_launches", "diablo_gpu_last_error",
+    "diablo_gpu_get_stream", "diablo_gpu_set_profiling", "diablo_gpu_kernel_times",
 ]
+KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
 
 
 class DiabloError(RuntimeError):
@@ -70,6 +72,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_kernel_launches.argtypes = [vp]
     L.diablo_gpu_kernel_launches.restype = ctypes.c_longlong
     L.diablo_gpu_last_error.restype = ctypes.c_char_p
+    L.diablo_gpu_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.diablo_gpu_set_profiling.argtypes = [vp, ip]
+    L.diablo_gpu_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), dp]
     _lib = L
     return L
 
@@ -159,6 +164,21 @@ class Channel:
         out["cfth"] = out["cfth"][: p.n_th]
         return out
 
+    def download_into(self, cu: list[np.ndarray], cp: np.ndarray, cth: list[np.ndarray]) -> None:
+        """Download CU1..3, CP and CTH into caller-owned Fortran-layout arrays."""
+        v = lambda a: _dp(a.view(np.float64)) if a is not None else None
+        if self.p.n_th > 1:
+            tmp = np.empty((self.p.n_th,) + fourier_shape(self.p), dtype=np.complex128)
+            th_ptr = v(tmp)
+        else:
+            tmp = None
+            th_ptr = v(cth[0]) if self.p.n_th else None
+        _check(self.L.diablo_gpu_download_state(self._h, v(cu[0]), v(cu[1]), v(cu[2]), v(cp), th_ptr,
+                                                None, None, None, None), "diablo_gpu_download_state")
+        if tmp is not None:
+            for n in range(self.p.n_th):
+                cth[n][...] = tmp[n]
+
     def download_phi(self) -> np.ndarray:
         phi = new_fourier(self.p)
         _check(self.L.diablo_gpu_download_phi(self._h, _dp(phi.view(np.float64))), "diablo_gpu_download_phi")
@@ -222,6 +242,22 @@ class Channel:
 
     def kernel_launches(self) -> int:
         return int(self.L.diablo_gpu_kernel_launches(self._h))
+
+    def stream(self) -> int:
+        """The handle's cudaStream_t as an integer (for timing events)."""
+        s = ctypes.c_void_p()
+        _check(self.L.diablo_gpu_get_stream(self._h, ctypes.byref(s)), "diablo_gpu_get_stream")
+        return int(s.value or 0)
+
+    def set_profiling(self, on: bool) -> None:
+        _check(self.L.diablo_gpu_set_profiling(self._h, int(on)), "diablo_gpu_set_profiling")
+
+    def kernel_times(self) -> dict:
+        """{kernel kind: (launches, total ms)} since profiling was switched on."""
+        n = (ctypes.c_longlong * len(KERNEL_NAMES))()
+        ms = np.zeros(len(KERNEL_NAMES))
+        _check(self.L.diablo_gpu_kernel_times(self._h, n, _dp(ms)), "diablo_gpu_kernel_times")
+        return {KERNEL_NAMES[k]: (int(n[k]), float(ms[k])) for k in range(len(KERNEL_NAMES)) if n[k]}
 
     # --- initial condition (CREATE_TH_CHAN then CREATE_FLOW_CHAN) ------------
     def init_from_physical(self, u: np.ndarray, th: np.ndarray) -> None:

@@ -64,6 +64,31 @@ struct Handle {
     int bc_type[2 * MAXF];
     double bc_c1[2 * MAXF];
     long long launches = 0;
+    // optional per-kernel event timing
+    bool profiling = false;
+    struct Rec { int kind; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+};
+
+// Bracket a launch with events when profiling (kinds: DIABLO_KERNEL_*).
+struct ProfScope {
+    Handle* h;
+    int kind;
+    cudaEvent_t a = nullptr;
+    ProfScope(Handle* hh, int k) : h(hh), kind(k) {
+        if (h->profiling && cudaEventCreate(&a) == cudaSuccess) cudaEventRecord(a, h->st);
+        else a = nullptr;
+    }
+    ~ProfScope() {
+        if (!a) return;
+        cudaEvent_t b;
+        if (cudaEventCreate(&b) == cudaSuccess) {
+            cudaEventRecord(b, h->st);
+            h->recs.push_back({kind, a, b});
+        } else {
+            cudaEventDestroy(a);
+        }
+    }
 };
 
 bool is_235(int n) {
@@ -91,6 +116,7 @@ void* make_twiddles(int n, cudaError_t* err) {
 
 void free_handle(Handle* h) {
     if (!h) return;
+    for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
                     h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->mult, h->piv, h->cup,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->d_err, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
@@ -248,7 +274,8 @@ int smem_limits(const Handle* h) {
     const Dims& d = h->d;
     const int group = products_group(d.nx);
     const int m = d.nx / 2;
-    const size_t smem = sizeof(double) * (size_t)3 * d.nf * d.nx + 16 * (size_t)group * (m + m / 16 + 1);
+    const int rows = group < d.nf + d.np ? group : d.nf + d.np;
+    const size_t smem = sizeof(double) * (size_t)4 * d.nf * d.nx + 16 * (size_t)rows * (m + m / 16 + 1);
     if (group < 1 || smem > 227 * 1024) return fail(DIABLO_EINVAL, "NX too large for the number of fields");
     // column kernels stage the per-row coefficients of every field
     if ((33 * (size_t)d.nf + 16) * d.nyp > 200 * 1024) return fail(DIABLO_EINVAL, "NY too large");
@@ -262,9 +289,12 @@ int run_transforms(Handle* h) {
     const void* twn = f ? h->twn_f : h->twn_d;
     const void* twm = f ? h->twm_f : h->twm_d;
     const void* twz = f ? h->twz_f : h->twz_d;
-    CK(launch_zinv<T>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, twz, h->st));
-    CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, 32, h->d_dy, h->d_dyf, h->pm, twm, twn, h->st));
-    CK(launch_zfwd_nl<T>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->d_kx, h->d_kz, h->pz, twz, h->st));
+    { ProfScope ps(h, DIABLO_KERNEL_ZINV);
+      CK(launch_zinv<T>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, twz, h->st)); }
+    { ProfScope ps(h, DIABLO_KERNEL_PRODUCTS);
+      CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, 32, h->d_dy, h->d_dyf, h->pm, twm, twn, h->st)); }
+    { ProfScope ps(h, DIABLO_KERNEL_ZFWD_NL);
+      CK(launch_zfwd_nl<T>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->d_kx, h->d_kz, h->pz, twz, h->st)); }
     h->launches += 3;
     return DIABLO_OK;
 }
@@ -503,7 +533,7 @@ static int rem_div(Handle* h, int update_cp, double inv_h) {
     a.dyf = h->d_dyf;
     a.inv_h = inv_h;
     a.update_cp = update_cp;
-    CK(launch_remdiv(a, h->st));
+    { ProfScope ps(h, DIABLO_KERNEL_REMDIV); CK(launch_remdiv(a, h->st)); }
     h->launches += 1;
     return DIABLO_OK;
 }
@@ -524,8 +554,9 @@ static int courant(Handle* h, double* delta_t, double* h_bar) {
         }
     const double inf = HUGE_VAL;
     CK(cudaMemcpyAsync(h->dtmin, &inf, sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(launch_zinv<double>(d, h->cu, h->s_field, h->xb, h->x_field, 3, 0, d.nyp, h->pz, h->twz_d, h->st));
-    CK(launch_cfl(d, h->xb, h->x_field, h->pm, h->twm_d, h->twn_d, h->d_dy, p.cfl, h->dx, h->dz, h->dtmin, h->st));
+    { ProfScope ps(h, DIABLO_KERNEL_CFL);
+      CK(launch_zinv<double>(d, h->cu, h->s_field, h->xb, h->x_field, 3, 0, d.nyp, h->pz, h->twz_d, h->st));
+      CK(launch_cfl(d, h->xb, h->x_field, h->pm, h->twm_d, h->twn_d, h->d_dy, p.cfl, h->dx, h->dz, h->dtmin, h->st)); }
     h->launches += 2;
     double vmin = inf;
     CK(cudaMemcpyAsync(&vmin, h->dtmin, sizeof(double), cudaMemcpyDeviceToHost, h->st));
@@ -593,7 +624,8 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     else if (p.f_type == 2) a.forcing = TEMP4 * (p.px0 + p.amp_omega0 * std::cos(p.omega0 * time));
     a.rk_step = rk_step;
     a.store_cf = 1;
-    CK(launch_cn_coef(d, a, h->mult, h->piv, h->cup, h->bcv, h->kind, h->bc_type, h->bc_c1, h->st));
+    { ProfScope ps(h, DIABLO_KERNEL_CN_COEF);
+      CK(launch_cn_coef(d, a, h->mult, h->piv, h->cup, h->bcv, h->kind, h->bc_type, h->bc_c1, h->st)); }
     const bool cfl = p.variable_dt && rk_step == 3 && (time_step % p.update_dt) == 0;
     ColArgs ca;
     ca.cn = a;
@@ -605,10 +637,13 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     ca.inv_h = 1.0 / TEMP4;
     ca.project = cfl ? 0 : 1;     // COURANT sees the velocity before the projection
     ca.update_cp = 1;
-    ca.store_phi = 1;
+    ca.store_phi = 0;             // phi stays where REM_DIV_CHAN alone puts it
     ca.err = h->d_err;
-    if (h->fp32) CK(launch_column<cpx<float>>(ca, (const cpx<float>*)h->nl, h->st));
-    else CK(launch_column<cpx<double>>(ca, (const cpx<double>*)h->nl, h->st));
+    {
+        ProfScope ps(h, DIABLO_KERNEL_COLUMN);
+        if (h->fp32) CK(launch_column<cpx<float>>(ca, (const cpx<float>*)h->nl, h->st));
+        else CK(launch_column<cpx<double>>(ca, (const cpx<double>*)h->nl, h->st));
+    }
     h->launches += 2;
     if (!cfl) return DIABLO_OK;
     // COURANT at the last substage (channel.f:1037-1040), then REM_DIV and the
@@ -635,7 +670,8 @@ int diablo_gpu_apply_bc_vel(void* handle) {
     Handle* h = (Handle*)handle;
     if (!h) return fail(DIABLO_EINVAL, "null handle");
     dim3 grid((h->d.nkxp + 127) / 128, h->d.nkzt);
-    k_apply_bc_vel<<<grid, 128, 0, h->st>>>(h->d, h->cu, h->d_dy, h->d_dyf, h->p);
+    { ProfScope ps(h, DIABLO_KERNEL_OTHER);
+      k_apply_bc_vel<<<grid, 128, 0, h->st>>>(h->d, h->cu, h->d_dy, h->d_dyf, h->p); }
     CK(cudaGetLastError());
     h->launches += 1;
     CK(cudaStreamSynchronize(h->st));
@@ -666,8 +702,9 @@ int diablo_gpu_fft_xz_to_fourier(void* handle, const double* v, double* vv, int 
     if (rc) return rc;
     const int np = jmax - jmin + 1;
     CK(copy_physical(h, h->phys, v, nullptr, jmin, np));
-    CK(launch_xfwd(d, h->phys, h->xb, jmin, np, h->pm, h->twm_d, h->twn_d, h->st));
-    CK(launch_zfwd_pack(d, h->xb, h->api_s, jmin, np, h->pz, h->twz_d, h->st));
+    { ProfScope ps(h, DIABLO_KERNEL_OTHER);
+      CK(launch_xfwd(d, h->phys, h->xb, jmin, np, h->pm, h->twm_d, h->twn_d, h->st));
+      CK(launch_zfwd_pack(d, h->xb, h->api_s, jmin, np, h->pz, h->twz_d, h->st)); }
     h->launches += 2;
     CK(copy_fourier(h, h->api_s, nullptr, vv, jmin, np));
     CK(cudaStreamSynchronize(h->st));
@@ -690,8 +727,9 @@ int diablo_gpu_fft_xz_to_physical(void* handle, const double* vv, double* v, int
     if (rc) return rc;
     const int np = jmax - jmin + 1;
     CK(copy_fourier(h, h->api_s, vv, nullptr, jmin, np));
-    CK(launch_zinv<double>(d, h->api_s, h->s_field, h->xb, h->x_field, 1, jmin, np, h->pz, h->twz_d, h->st));
-    CK(launch_xinv(d, h->xb, h->phys, jmin, np, h->pm, h->twm_d, h->twn_d, h->st));
+    { ProfScope ps(h, DIABLO_KERNEL_OTHER);
+      CK(launch_zinv<double>(d, h->api_s, h->s_field, h->xb, h->x_field, 1, jmin, np, h->pz, h->twz_d, h->st));
+      CK(launch_xinv(d, h->xb, h->phys, jmin, np, h->pm, h->twm_d, h->twn_d, h->st)); }
     h->launches += 2;
     CK(copy_physical(h, h->phys, nullptr, v, jmin, np));
     CK(cudaStreamSynchronize(h->st));
@@ -714,6 +752,43 @@ int diablo_gpu_synchronize(void* handle) {
     if (!h) return fail(DIABLO_EINVAL, "null handle");
     CK(cudaStreamSynchronize(h->st));
     return check_device_flag(h);
+}
+
+int diablo_gpu_get_stream(void* handle, void** stream) {
+    Handle* h = (Handle*)handle;
+    if (!h || !stream) return fail(DIABLO_EINVAL, "null pointer argument");
+    *stream = (void*)h->st;
+    return DIABLO_OK;
+}
+
+static void drop_records(Handle* h) {
+    for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    h->recs.clear();
+}
+
+int diablo_gpu_set_profiling(void* handle, int on) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    CK(cudaStreamSynchronize(h->st));
+    drop_records(h);
+    h->profiling = on != 0;
+    return DIABLO_OK;
+}
+
+int diablo_gpu_kernel_times(void* handle, long long* launches, double* ms) {
+    Handle* h = (Handle*)handle;
+    if (!h || !launches || !ms) return fail(DIABLO_EINVAL, "null pointer argument");
+    CK(cudaStreamSynchronize(h->st));
+    for (int k = 0; k < DIABLO_NKERNELS; ++k) { launches[k] = 0; ms[k] = 0.0; }
+    for (auto& r : h->recs) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess && r.kind >= 0 && r.kind < DIABLO_NKERNELS) {
+            launches[r.kind] += 1;
+            ms[r.kind] += t;
+        }
+    }
+    drop_records(h);
+    return DIABLO_OK;
 }
 
 long long diablo_gpu_kernel_launches(void* handle) {

@@ -129,7 +129,7 @@ __device__ __forceinline__ cpx<T> extract_real_forward(const cpx<T>* buf, const 
     return X * scale;
 }
 
-constexpr int PROD_G = 11;          // product rows transformed together
+constexpr int PROD_G = 16;          // rows transformed together by the products kernel
 constexpr int RT_VMAX = 12;         // run-time path: values per thread
 
 template <typename T, int MC, int S, class L>
@@ -140,25 +140,31 @@ __device__ __forceinline__ void row_fft(cpx<T>* buf, int nrows, const L& lay, co
 }
 
 // ---------------------------------------------------------------------------
-// K2: per z-row, marching over planes: x-inverse of the fields, the
-// physical products, x-forward of the products.
+// K2: per z-row, marching over planes.  Iteration J transforms, in one
+// batch of forward M-point FFTs, the fields of plane J back to physical
+// space (the backward FFT taken as conj(FFT(conj(.))) so that both halves of
+// the batch share one transform) and the products of plane J-2, whose
+// neighbours J-3..J-1 are already in the ring of physical planes; then
+// unpacks the fields into the ring and writes the products' x spectra.
 // ---------------------------------------------------------------------------
+constexpr int RING = 4;
+
 template <typename T, int MC>
 __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __restrict__ X,
-                                                  cpx<T>* __restrict__ Y, int jlo, int jhi, int chunk,
-                                                  int group, const double* __restrict__ dy,
-                                                  const double* __restrict__ dyf, FftPlan pm,
-                                                  const cpx<T>* __restrict__ twm,
-                                                  const cpx<T>* __restrict__ twn) {
+                                                     cpx<T>* __restrict__ Y, int jlo, int jhi, int chunk,
+                                                     int group, const double* __restrict__ dy,
+                                                     const double* __restrict__ dyf, FftPlan pm,
+                                                     const cpx<T>* __restrict__ twm,
+                                                     const cpx<T>* __restrict__ twn) {
     extern __shared__ unsigned char smem_raw[];
     const int M = MC > 0 ? MC : d.nx / 2;
     const int nx = 2 * M;
-    const int nf = d.nf, np = d.np;
+    const int nf = d.nf, np = d.np, nrow = nf + np;
     using Lay = typename std::conditional<(MC > 0), RowLayoutCT<MC>, RowLayoutRT>::type;
     Lay lay;
     if constexpr (MC == 0) lay.pitch = row_pitch(M);
-    T* ring = reinterpret_cast<T*>(smem_raw);                              // [3][nf][nx]
-    cpx<T>* buf = reinterpret_cast<cpx<T>*>(ring + (size_t)3 * nf * nx);  // [group][pitch]
+    T* ring = reinterpret_cast<T*>(smem_raw);                                 // [RING][nf][nx]
+    cpx<T>* buf = reinterpret_cast<cpx<T>*>(ring + (size_t)RING * nf * nx);  // [group][pitch]
     T* tbuf = reinterpret_cast<T*>(buf);
     const int z = blockIdx.x;
     const int jb = jlo + blockIdx.y * chunk;
@@ -166,79 +172,88 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
     const size_t xrow = (size_t)d.nz * d.ldx;            // plane stride of X / Y
     const size_t xf = (size_t)d.nyp * xrow;              // field stride of X / Y
     const T inv_nx = T(1.0 / (double)nx);
-    for (int J = jb - 1; J <= je + 1; ++J) {
-        const int slot = (J - (jb - 1)) % 3;
-        // --- backward x transform of the fields at plane J, row z ---------
-        for (int f0 = 0; f0 < nf; f0 += group) {
-            const int nr = min(group, nf - f0);
-            for (int e = threadIdx.x; e < nr * M; e += 256) {
-                const int r = e / M, k = e % M;
-                const cpx<T>* xr = X + (size_t)(f0 + r) * xf + (size_t)J * xrow + (size_t)z * d.ldx;
-                fill_real_inverse(buf, lay, r, xr, M, d.nkx, twn, k);
-            }
-            __syncthreads();
-            row_fft<T, MC, +1>(buf, nr, lay, pm, twm);
-            for (int e = threadIdx.x; e < nr * M; e += 256) {
-                const int r = e / M, m = e % M;
-                const cpx<T> v = buf[lay.at(m, r)];
-                T* dst = ring + ((size_t)slot * nf + f0 + r) * nx + 2 * m;
-                dst[0] = v.x;
-                dst[1] = v.y;
-            }
-            __syncthreads();
+    auto slot = [&](int j) { return (j - (jb - 1)) % RING; };
+    for (int J = jb - 1; J <= je + 2; ++J) {
+        const bool do_inv = (J <= je + 1);
+        const int jp = J - 2;                            // plane whose products are formed
+        const bool do_prod = (jp >= jb);
+        const int r0 = do_inv ? 0 : nf, r1 = do_prod ? nrow : nf;
+        T a1 = 0, a0 = 0, i2dyf = 0, idy = 0;
+        if (do_prod) {
+            a1 = (T)(dyf[jp] / (2.0 * dy[jp]));
+            a0 = (T)(dyf[jp - 1] / (2.0 * dy[jp]));
+            i2dyf = (T)(1.0 / (2.0 * dyf[jp]));
+            idy = (T)(1.0 / dy[jp]);
         }
-        const int jp = J - 1;    // plane whose products are now computable
-        if (jp < jb) continue;
-        const int sm = (jp - 1 - (jb - 1)) % 3, s0 = (jp - (jb - 1)) % 3, sp = (J - (jb - 1)) % 3;
-        const T a1 = (T)(dyf[jp] / (2.0 * dy[jp]));
-        const T a0 = (T)(dyf[jp - 1] / (2.0 * dy[jp]));
-        const T i2dyf = (T)(1.0 / (2.0 * dyf[jp]));
-        const T idy = (T)(1.0 / dy[jp]);
-        const T* U1m = ring + ((size_t)sm * nf + 0) * nx;
-        const T* U1c = ring + ((size_t)s0 * nf + 0) * nx;
-        const T* U1p = ring + ((size_t)sp * nf + 0) * nx;
-        const T* U2m = ring + ((size_t)sm * nf + 1) * nx;
-        const T* U2c = ring + ((size_t)s0 * nf + 1) * nx;
-        const T* U2p = ring + ((size_t)sp * nf + 1) * nx;
-        const T* U3m = ring + ((size_t)sm * nf + 2) * nx;
-        const T* U3c = ring + ((size_t)s0 * nf + 2) * nx;
-        const T* U3p = ring + ((size_t)sp * nf + 2) * nx;
-        for (int g0 = 0; g0 < np; g0 += group) {
-            const int ng = min(group, np - g0);
-            for (int e = threadIdx.x; e < ng * nx; e += 256) {
-                const int q = e / nx, x = e % nx;
-                const int p = g0 + q;
-                const T u1 = U1c[x], u2 = U2c[x], u3 = U3c[x];
-                T v;
-                if (p == 0) v = u3 * u1;
-                else if (p == 1) v = u1 * u1;
-                else if (p == 2) v = u3 * u3;
-                else if (p == 3) v = (a1 * u1 + a0 * U1m[x]) * u2;
-                else if (p == 4) v = (a1 * u3 + a0 * U3m[x]) * u2;
-                else if (p == 5) v = (U1p[x] * U2p[x] + u1 * U2p[x] - u1 * u2 - U1m[x] * u2) * i2dyf;
-                else if (p == 6) v = (U3p[x] * U2p[x] + u3 * U2p[x] - u3 * u2 - U3m[x] * u2) * i2dyf;
-                else if (p == 7) {
-                    const T s1 = u2 + U2p[x], s2 = u2 + U2m[x];
-                    v = (T(0.25) * s1 * s1 - T(0.25) * s2 * s2) * idy;
-                } else {
-                    const int n = (p - 8) / 3, r = (p - 8) % 3;
-                    const T* THc = ring + ((size_t)s0 * nf + 3 + n) * nx;
-                    if (r == 0) v = THc[x] * u1;
-                    else if (r == 1) v = THc[x] * u3;
-                    else {
-                        const T* THm = ring + ((size_t)sm * nf + 3 + n) * nx;
-                        const T* THp = ring + ((size_t)sp * nf + 3 + n) * nx;
-                        v = (THp[x] * U2p[x] + THc[x] * U2p[x] - THc[x] * u2 - THm[x] * u2) * i2dyf;
+        for (int c0 = r0; c0 < r1; c0 += group) {
+            const int nr = min(group, r1 - c0);
+            // ---- fill: conjugated half spectra of the fields, products ----
+            const int nfill = max(0, min(nf, c0 + nr) - c0);        // inverse rows in this chunk
+            for (int e = threadIdx.x; e < nfill * M; e += 256) {
+                const int r = e / M, k = e % M;
+                const cpx<T>* xr = X + (size_t)(c0 + r) * xf + (size_t)J * xrow + (size_t)z * d.ldx;
+                fill_real_inverse(buf, lay, r, xr, M, d.nkx, twn, k);
+                buf[lay.at(k, r)].y = -buf[lay.at(k, r)].y;
+            }
+            const int p0 = max(c0, nf) - nf, p1 = c0 + nr - nf;       // products p0..p1-1 here
+            if (p1 > p0) {
+                const int sm = slot(jp - 1), s0 = slot(jp), sp = slot(jp + 1);
+                for (int x = threadIdx.x; x < nx; x += 256) {
+                    const T* r_m = ring + (size_t)sm * nf * nx + x;
+                    const T* r_c = ring + (size_t)s0 * nf * nx + x;
+                    const T* r_p = ring + (size_t)sp * nf * nx + x;
+                    const T u1m = r_m[0], u1 = r_c[0], u1p = r_p[0];
+                    const T u2m = r_m[nx], u2 = r_c[nx], u2p = r_p[nx];
+                    const T u3m = r_m[2 * nx], u3 = r_c[2 * nx], u3p = r_p[2 * nx];
+                    T v[8];
+                    v[0] = u3 * u1;
+                    v[1] = u1 * u1;
+                    v[2] = u3 * u3;
+                    v[3] = (a1 * u1 + a0 * u1m) * u2;
+                    v[4] = (a1 * u3 + a0 * u3m) * u2;
+                    v[5] = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) * i2dyf;
+                    v[6] = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) * i2dyf;
+                    const T s1 = u2 + u2p, s2 = u2 + u2m;
+                    v[7] = (T(0.25) * s1 * s1 - T(0.25) * s2 * s2) * idy;
+                    const int eoff = 2 * lay.at(x >> 1, 0) + (x & 1);
+                    const int rstride = 2 * (lay.at(0, 1) - lay.at(0, 0));
+#pragma unroll
+                    for (int p = 0; p < 8; ++p)
+                        if (p >= p0 && p < p1) tbuf[eoff + (nf + p - c0) * rstride] = v[p];
+                    for (int n = 0; n < d.nth; ++n) {
+                        const T thm = r_m[(3 + n) * nx], th = r_c[(3 + n) * nx], thp = r_p[(3 + n) * nx];
+                        T w[3];
+                        w[0] = th * u1;
+                        w[1] = th * u3;
+                        w[2] = (thp * u2p + th * u2p - th * u2 - thm * u2) * i2dyf;
+#pragma unroll
+                        for (int r = 0; r < 3; ++r) {
+                            const int p = 8 + 3 * n + r;
+                            if (p >= p0 && p < p1) tbuf[eoff + (nf + p - c0) * rstride] = w[r];
+                        }
                     }
                 }
-                tbuf[2 * lay.at(x >> 1, q) + (x & 1)] = v;
             }
             __syncthreads();
-            row_fft<T, MC, -1>(buf, ng, lay, pm, twm);
-            for (int e = threadIdx.x; e < ng * d.ldx; e += 256) {
-                const int q = e / d.ldx, k = e % d.ldx;
-                Y[(size_t)(g0 + q) * xf + (size_t)jp * xrow + (size_t)z * d.ldx + k] =
-                    extract_real_forward(buf, lay, q, M, d.nkx, twn, k, inv_nx);
+            row_fft<T, MC, -1>(buf, nr, lay, pm, twm);
+            // ---- unpack the fields of plane J, write the products of jp --------
+            if (nfill > 0) {
+                const int sl = slot(J);
+                for (int e = threadIdx.x; e < nfill * M; e += 256) {
+                    const int r = e / M, m = e % M;
+                    const cpx<T> v = buf[lay.at(m, r)];
+                    T* dst = ring + ((size_t)sl * nf + c0 + r) * nx + 2 * m;
+                    dst[0] = v.x;
+                    dst[1] = -v.y;
+                }
+            }
+            if (p1 > p0) {
+                for (int e = threadIdx.x; e < (p1 - p0) * d.ldx; e += 256) {
+                    const int q = e / d.ldx, k = e % d.ldx;
+                    const int p = p0 + q;
+                    Y[(size_t)p * xf + (size_t)jp * xrow + (size_t)z * d.ldx + k] =
+                        extract_real_forward(buf, lay, nf + p - c0, M, d.nkx, twn, k, inv_nx);
+                }
             }
             __syncthreads();
         }
@@ -354,7 +369,8 @@ cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int 
     const int group = products_group(d.nx);
     if (group < 1) return cudaErrorInvalidValue;
     const int M = d.nx / 2;
-    const size_t smem = sizeof(T) * (size_t)3 * d.nf * d.nx + sizeof(cpx<T>) * (size_t)group * row_pitch(M);
+    const int rows = group < d.nf + d.np ? group : d.nf + d.np;
+    const size_t smem = sizeof(T) * (size_t)RING * d.nf * d.nx + sizeof(cpx<T>) * (size_t)rows * row_pitch(M);
     const int nchunks = (jhi - jlo + chunk) / chunk;
     dim3 grid(d.nz, nchunks);
     auto go = [&](auto kern) {

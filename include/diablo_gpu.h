@@ -155,6 +155,26 @@ int diablo_gpu_courant(void* handle, double* delta_t, double* h_bar);
 #define DIABLO_NSTATS      17
 int diablo_gpu_stats(void* handle, double* profiles);
 
+/* The CUDA stream (a cudaStream_t) all work of the handle is queued on, as
+ * an opaque pointer: callers may record timing events on it. */
+int diablo_gpu_get_stream(void* handle, void** stream);
+/* Kernel timing: with profiling on, every library launch is bracketed by
+ * CUDA events on the handle's stream.  diablo_gpu_kernel_times waits for the
+ * stream, then returns per kernel kind the number of launches and the summed
+ * device time in ms since profiling was switched on (and restarts the
+ * count).  Kinds: DIABLO_KERNEL_*; arrays hold DIABLO_NKERNELS entries. */
+#define DIABLO_KERNEL_ZINV      0   /* inverse z transform of the state */
+#define DIABLO_KERNEL_PRODUCTS  1   /* x transforms + nonlinear products */
+#define DIABLO_KERNEL_ZFWD_NL   2   /* forward z transform + derivative combination */
+#define DIABLO_KERNEL_CN_COEF   3   /* CN tridiagonal factors */
+#define DIABLO_KERNEL_COLUMN    4   /* CN solves + projection + pressure update */
+#define DIABLO_KERNEL_REMDIV    5   /* stand-alone projection */
+#define DIABLO_KERNEL_CFL       6   /* CFL minimum */
+#define DIABLO_KERNEL_OTHER     7   /* transform API, BCs, statistics */
+#define DIABLO_NKERNELS         8
+int diablo_gpu_set_profiling(void* handle, int on);
+int diablo_gpu_kernel_times(void* handle, long long* launches, double* ms);
+
 /* Wait for all work queued on the handle's stream. */
 int diablo_gpu_synchronize(void* handle);
 /* Sum over the last launches of the handle: number of kernels launched by
