@@ -33,6 +33,7 @@ EXPORTS = [
     "diablo_gpu_poisson_p_chan", "diablo_gpu_apply_bc_vel", "diablo_gpu_courant", "diablo_gpu_stats",
     "diablo_gpu_synchronize", "diablo_gpu_kernel_launches", "diablo_gpu_last_error",
     "diablo_gpu_get_stream", "diablo_gpu_set_profiling", "diablo_gpu_kernel_times",
+    "diablo_gpu_rem_div_chan_noalloc",
 ]
 KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
 
@@ -75,6 +76,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.diablo_gpu_set_profiling.argtypes = [vp, ip]
     L.diablo_gpu_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), dp]
+    L.diablo_gpu_rem_div_chan_noalloc.argtypes = [ctypes.POINTER(DiabloParams), dp, dp, vp, vp, vp, vp, vp]
     _lib = L
     return L
 

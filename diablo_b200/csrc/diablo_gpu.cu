@@ -315,6 +315,8 @@ int check_device_flag(Handle* h) {
 
 }  // namespace
 
+int dgpu::set_error(int code, const std::string& msg) { return fail(code, msg); }
+
 extern "C" {
 
 const char* diablo_gpu_last_error(void) { return g_err.c_str(); }

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "kernels.cuh"
 
 namespace dgpu {
@@ -61,4 +63,6 @@ cudaError_t launch_cfl(const Dims& d, const void* X, size_t x_fstride, const Fft
                        double dz, double* dtmin, cudaStream_t st);
 // rows transformed together by the products kernel for a given NX
 int products_group(int nx);
+// Record the one-line message returned by diablo_gpu_last_error; returns code.
+int set_error(int code, const std::string& msg);
 }  // namespace dgpu

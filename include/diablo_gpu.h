@@ -175,6 +175,28 @@ int diablo_gpu_get_stream(void* handle, void** stream);
 int diablo_gpu_set_profiling(void* handle, int on);
 int diablo_gpu_kernel_times(void* handle, long long* launches, double* ms);
 
+/* REM_DIV_CHAN for callers that cannot allocate device memory.  This entry
+ * point has no counterpart in the reference: it exists for hosts that keep
+ * CU1, CU2, CU3 in device memory they obtained themselves (OpenACC or CUDA
+ * Fortran device arrays, a framework's memory pool, code running during
+ * stream capture) and cannot let a library call cudaMalloc.  It allocates
+ * nothing: it launches one kernel on `stream` (a cudaStream_t, NULL for the
+ * default stream) and keeps its working storage in an 8 MiB array of static
+ * device memory that every GPU loading this library holds until exit.
+ *   p        sizes and LX, LZ (other fields unused)
+ *   dy, dyf  HOST pointers to DY(0:NY+1), DYF(0:NY+1)
+ *   cu1..3   DEVICE pointers, Fortran layout (0:NXP,0:NZ+1,0:NY+1) complex;
+ *            projected in place (dealiased block, J = 1..NY)
+ *   phi      DEVICE pointer, same layout; receives phi on J = 1..NY
+ * Limit: (NX/3+1)*(2*(NZ/3)+1)*(NY+2) + 2*(NY+2) <= 2^20, else
+ * DIABLO_EINVAL.  The first call on a device looks up the static array's
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls that may overlap on the GPU
+ * race and must be serialised by the caller. */
+int diablo_gpu_rem_div_chan_noalloc(const diablo_params* p, const double* dy, const double* dyf,
+                                    double* cu1, double* cu2, double* cu3, double* phi,
+                                    void* stream);
+
 /* Wait for all work queued on the handle's stream. */
 int diablo_gpu_synchronize(void* handle);
 /* Sum over the last launches of the handle: number of kernels launched by
