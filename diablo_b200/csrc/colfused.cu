@@ -101,29 +101,38 @@ __global__ void __launch_bounds__(128, 4) k_column(ColArgs A, const TN* __restri
     }
     __syncthreads();
 
-    // ---- producer (thread 0): one stage = one row of every operand --------
+    // ---- producer (warp 0): one stage = one row of every operand -----------
+    // lane 0 posts the byte count, then lane i issues the i-th bulk copy.
     auto issue = [&](int q, int sweep, int j) {
         uint64_t* bar = &bars[q % D];
         unsigned char* base = smem + (size_t)(q % D) * sg.bytes;
         const size_t off = (size_t)j * ps + gblk;
-        if (sweep == 1) {
-            const uint32_t bytes = nf * sg.szC * (rk1 ? 2 : 1) + nf * sg.szN + sg.szC;
-            mbar_arrive_expect_tx(bar, bytes);
-            for (int q2 = 0; q2 < nf; ++q2) {
-                bulk_g2s(base + q2 * sg.szC, a.cu + q2 * fs + off, sg.szC, bar);
-                if (rk1) bulk_g2s(base + sg.oCF + q2 * sg.szC, a.cf + q2 * fs + off, sg.szC, bar);
-                bulk_g2s(base + sg.oNL + q2 * sg.szN, nl + q2 * fs + off, sg.szN, bar);
+        uint32_t bytes;
+        int ncopy;
+        if (sweep == 1) { bytes = nf * sg.szC * (rk1 ? 2 : 1) + nf * sg.szN + sg.szC; ncopy = 3 * nf + 1; }
+        else if (sweep == 2) { bytes = nf * sg.szC; ncopy = nf; }
+        else { bytes = 5 * sg.szC + CB * 8; ncopy = 6; }
+        if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
+        __syncwarp();
+        const int l = lane;
+        if (l < ncopy) {
+            if (sweep == 1) {
+                if (l < nf) bulk_g2s(base + l * sg.szC, a.cu + l * fs + off, sg.szC, bar);
+                else if (l < 2 * nf) {
+                    if (rk1) bulk_g2s(base + sg.oCF + (l - nf) * sg.szC, a.cf + (l - nf) * fs + off, sg.szC, bar);
+                } else if (l < 3 * nf) {
+                    bulk_g2s(base + sg.oNL + (l - 2 * nf) * sg.szN, nl + (l - 2 * nf) * fs + off, sg.szN, bar);
+                } else {
+                    bulk_g2s(base + sg.oCP, a.cp + off, sg.szC, bar);
+                }
+            } else if (sweep == 2) {
+                bulk_g2s(base + l * sg.szC, a.cu + l * fs + off, sg.szC, bar);
+            } else {
+                if (l < 3) bulk_g2s(base + l * sg.szC, a.cu + l * fs + off, sg.szC, bar);
+                else if (l == 3) bulk_g2s(base + sg.oB, A.bsc + off, CB * 8, bar);
+                else if (l == 4) bulk_g2s(base + sg.oG, A.gsc + off, sg.szC, bar);
+                else bulk_g2s(base + sg.oCP3, a.cp + off, sg.szC, bar);
             }
-            bulk_g2s(base + sg.oCP, a.cp + off, sg.szC, bar);
-        } else if (sweep == 2) {
-            mbar_arrive_expect_tx(bar, nf * sg.szC);
-            for (int q2 = 0; q2 < nf; ++q2) bulk_g2s(base + q2 * sg.szC, a.cu + q2 * fs + off, sg.szC, bar);
-        } else {
-            mbar_arrive_expect_tx(bar, 5 * sg.szC + CB * 8);
-            for (int q2 = 0; q2 < 3; ++q2) bulk_g2s(base + q2 * sg.szC, a.cu + q2 * fs + off, sg.szC, bar);
-            bulk_g2s(base + sg.oB, A.bsc + off, CB * 8, bar);
-            bulk_g2s(base + sg.oG, A.gsc + off, sg.szC, bar);
-            bulk_g2s(base + sg.oCP3, a.cp + off, sg.szC, bar);
         }
     };
     auto stage = [&](int q) -> unsigned char* { return smem + (size_t)(q % D) * sg.bytes; };
@@ -170,7 +179,7 @@ __global__ void __launch_bounds__(128, 4) k_column(ColArgs A, const TN* __restri
 
     // ======================= sweep 1 (ascending) ==============================
     const int n1 = ny + 2;
-    if (tid == 0)
+    if (warp == 0)
         for (int q = 0; q < D && q < n1; ++q) issue(q, 1, q);
     wait(0);
     wait(1);
@@ -220,7 +229,7 @@ __global__ void __launch_bounds__(128, 4) k_column(ColArgs A, const TN* __restri
             if (fvalid) cuo[(size_t)j * ps] = G;
         }
         __syncthreads();                         // stage j consumed by all lanes
-        if (tid == 0 && j + D < n1) issue(j + D, 1, j + D);
+        if (warp == 0 && j + D < n1) issue(j + D, 1, j + D);
         w0 = w1;
         w1 = w2;
         cpm = cpj;
@@ -240,7 +249,7 @@ __global__ void __launch_bounds__(128, 4) k_column(ColArgs A, const TN* __restri
     __syncthreads();
     const int q2base = n1;                       // rows ny+1 .. 1
     const int n2 = ny + 1;
-    if (tid == 0)
+    if (warp == 0)
         for (int i = 0; i < D && i < n2; ++i) issue(q2base + i, 2, ny + 1 - i);
     double2 xn = zero;                           // own field's x(j+1)
     double rbt_n = 0.0, a_n = 0.0;               // phi system: reverse-eliminated row j+1
@@ -296,7 +305,7 @@ __global__ void __launch_bounds__(128, 4) k_column(ColArgs A, const TN* __restri
         }
         xn = x;
         __syncthreads();
-        if (tid == 0 && j >= 1 && i + D < n2) issue(q2base + i + D, 2, ny + 1 - (i + D));
+        if (warp == 0 && j >= 1 && i + D < n2) issue(q2base + i + D, 2, ny + 1 - (i + D));
     }
     if (!proj) return;
 
@@ -305,7 +314,7 @@ __global__ void __launch_bounds__(128, 4) k_column(ColArgs A, const TN* __restri
     __syncthreads();
     const int q3base = q2base + n2;              // rows 1 .. ny
     const int n3 = ny;
-    if (tid == 0)
+    if (warp == 0)
         for (int i = 0; i < D && i < n3; ++i) issue(q3base + i, 3, 1 + i);
     const int f3 = f < 3 ? f : 0;
     double2 phip = zero;                          // phi(j-1)
@@ -331,7 +340,7 @@ __global__ void __launch_bounds__(128, 4) k_column(ColArgs A, const TN* __restri
         }
         phip = phi;
         __syncthreads();
-        if (tid == 0 && j - 1 + D < n3) issue(q + D, 3, j + D);
+        if (warp == 0 && j - 1 + D < n3) issue(q + D, 3, j + D);
     }
 }
 

@@ -15,6 +15,8 @@
 // any other product of 2, 3 and 5 runs with the run-time plan (fft.cuh).
 #include <cuda_runtime.h>
 
+#include <stdint.h>
+
 #include <type_traits>
 
 #include "fft.cuh"
@@ -279,52 +281,120 @@ __device__ __forceinline__ void field_products(int f, int* p, int* mlt) {
     }
 }
 
+// 16-byte asynchronous global -> shared copies (sm_80+ cp.async).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Block: kx tile of TX columns, field f, planes J0 .. J0+ZF_PLANES-1.  The
+// 3*ZF_PLANES product tiles it consumes stream through two shared buffers
+// (cp.async), the next tile in flight while the current one is transformed.
+constexpr int ZF_PLANES = 8;
+constexpr int ZF_TX = 8;
+
 template <typename T, int NC, int TX>
 __global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __restrict__ Y,
-                                                    cpx<T>* __restrict__ NL, int jlo,
+                                                    cpx<T>* __restrict__ NL, int jlo, int jhi,
                                                     const double* __restrict__ kxw,
                                                     const double* __restrict__ kzw, FftPlan pz,
                                                     const cpx<T>* __restrict__ twz) {
-    extern __shared__ unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nz = NC > 0 ? NC : d.nz;
     const int nkz = nz / 3, nkzt = 2 * nkz + 1;
-    cpx<T>* buf = reinterpret_cast<cpx<T>*>(smem_raw);          // [nz][TX]
-    cpx<T>* acc = buf + (size_t)nz * TX;                         // [nkzt][TX]
+    constexpr int QA = NC > 0 ? ((2 * (NC / 3) + 1) * TX + 255) / 256 : 1;
+    cpx<T>* bufs = reinterpret_cast<cpx<T>*>(smem_raw);          // [2][nz][TX]
+    cpx<T>* sacc = bufs + 2 * (size_t)nz * TX;                    // run-time path: [nkzt][TX]
     const int kx0 = blockIdx.x * TX;
-    const int J = jlo + blockIdx.y;
     const int f = blockIdx.z;
+    const int J0 = jlo + blockIdx.y * ZF_PLANES;
+    const int nplanes = min(ZF_PLANES, jhi - J0 + 1);
     const size_t xrow = (size_t)nz * d.ldx;
     const size_t xf = (size_t)d.nyp * xrow;
     const T inv_nz = T(1.0 / (double)nz);
     int prod[3], mlt[3];
     field_products(f, prod, mlt);
-    for (int e = threadIdx.x; e < nkzt * TX; e += 256) acc[e] = mk<T>(0, 0);
-    for (int t = 0; t < 3; ++t) {
-        const cpx<T>* src = Y + (size_t)prod[t] * xf + (size_t)J * xrow + kx0;
-        for (int e = threadIdx.x; e < nz * TX; e += 256) {
-            const int z = e / TX, c = e % TX;
-            buf[e] = src[(size_t)z * d.ldx + c];
+    const size_t sp = d.splane();
+    const size_t sf = (size_t)d.nyp * sp;
+    constexpr int CH = (int)(TX * sizeof(cpx<T>) / 16);           // 16-byte chunks per z row
+    auto load = [&](int t, int buf) {                             // tile t = 3*plane + product
+        const int J = J0 + t / 3;
+        const cpx<T>* src = Y + (size_t)prod[t % 3] * xf + (size_t)J * xrow + kx0;
+        unsigned char* dst = reinterpret_cast<unsigned char*>(bufs + (size_t)buf * nz * TX);
+        for (int e = threadIdx.x; e < nz * CH; e += 256) {
+            const int z = e / CH, q = e % CH;
+            cp_async16(dst + (size_t)z * TX * sizeof(cpx<T>) + q * 16,
+                       reinterpret_cast<const unsigned char*>(src + (size_t)z * d.ldx) + q * 16);
+        }
+        cp_async_commit();
+    };
+    const int ntiles = 3 * nplanes;
+    load(0, 0);
+    cpx<T> acc[QA];
+    for (int t = 0; t < ntiles; ++t) {
+        const int pl = t / 3, r = t % 3;
+        if (t + 1 < ntiles) {
+            load(t + 1, (t + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
+        cpx<T>* buf = bufs + (size_t)(t & 1) * nz * TX;
         col_fft<T, NC, TX, -1>(buf, pz, twz);
-        const int mt = mlt[t];
-        for (int e = threadIdx.x; e < nkzt * TX; e += 256) {
-            const int m = e / TX, c = e % TX;
-            const cpx<T> v = buf[(size_t)m_to_z(m, nkz, nz, nkzt) * TX + c] * inv_nz;
-            cpx<T> a = acc[e];
-            if (mt == 0) a = a - v;
-            else {
-                const T K = mt == 1 ? (T)kxw[kx0 + c] : (T)kzw[m];
-                a = mk<T>(a.x + K * v.y, a.y - K * v.x);
-            }
-            acc[e] = a;
+        const int mt = mlt[r];
+        if (r == 0) {
+#pragma unroll
+            for (int q = 0; q < QA; ++q) acc[q] = mk<T>(0, 0);
+            if constexpr (NC == 0)
+                for (int e = threadIdx.x; e < nkzt * TX; e += 256) sacc[e] = mk<T>(0, 0);
         }
-        __syncthreads();
+        if constexpr (NC > 0) {
+#pragma unroll
+            for (int q = 0; q < QA; ++q) {
+                const int e = threadIdx.x + q * 256;
+                if (e < nkzt * TX) {
+                    const int m = e / TX, c = e % TX;
+                    const cpx<T> v = buf[(size_t)m_to_z(m, nkz, nz, nkzt) * TX + c] * inv_nz;
+                    if (mt == 0) acc[q] = acc[q] - v;
+                    else {
+                        const T K = mt == 1 ? (T)kxw[kx0 + c] : (T)kzw[m];
+                        acc[q] = mk<T>(acc[q].x + K * v.y, acc[q].y - K * v.x);
+                    }
+                }
+            }
+        } else {
+            for (int e = threadIdx.x; e < nkzt * TX; e += 256) {
+                const int m = e / TX, c = e % TX;
+                const cpx<T> v = buf[(size_t)m_to_z(m, nkz, nz, nkzt) * TX + c] * inv_nz;
+                cpx<T> a = sacc[e];
+                if (mt == 0) a = a - v;
+                else {
+                    const T K = mt == 1 ? (T)kxw[kx0 + c] : (T)kzw[m];
+                    a = mk<T>(a.x + K * v.y, a.y - K * v.x);
+                }
+                sacc[e] = a;
+            }
+        }
+        if (r == 2) {
+            cpx<T>* dst = NL + (size_t)f * sf + (size_t)(J0 + pl) * sp + kx0;
+            if constexpr (NC > 0) {
+#pragma unroll
+                for (int q = 0; q < QA; ++q) {
+                    const int e = threadIdx.x + q * 256;
+                    if (e < nkzt * TX) dst[(size_t)(e / TX) * d.ldx + e % TX] = acc[q];
+                }
+            } else {
+                __syncthreads();
+                for (int e = threadIdx.x; e < nkzt * TX; e += 256) dst[(size_t)(e / TX) * d.ldx + e % TX] = sacc[e];
+            }
+        }
+        __syncthreads();   // buffer t&1 is refilled by the load issued next iteration
     }
-    const size_t sp = d.splane();               // plane stride of S
-    const size_t sf = (size_t)d.nyp * sp;       // field stride of S
-    cpx<T>* dst = NL + (size_t)f * sf + (size_t)J * sp + kx0;
-    for (int e = threadIdx.x; e < nkzt * TX; e += 256) dst[(size_t)(e / TX) * d.ldx + e % TX] = acc[e];
 }
 
 // ---------------------------------------------------------------------------
@@ -391,13 +461,13 @@ template <typename T>
 cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int jhi,
                            const double* kx, const double* kz, const FftPlan& pz, const void* twz,
                            cudaStream_t st) {
-    constexpr int TX = ZTile<T>::TX;
+    constexpr int TX = ZF_TX;
     if (jhi < jlo) return cudaSuccess;
-    dim3 grid(d.ldx / TX, jhi - jlo + 1, d.nf);
-    auto go = [&](auto kern, bool) {
-        const size_t smem = sizeof(cpx<T>) * ((size_t)d.nz * TX + (size_t)d.nkzt * TX);
+    dim3 grid(d.ldx / TX, (jhi - jlo + ZF_PLANES) / ZF_PLANES, d.nf);
+    auto go = [&](auto kern, bool ct) {
+        const size_t smem = sizeof(cpx<T>) * (2 * (size_t)d.nz * TX + (ct ? 0 : (size_t)d.nkzt * TX));
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, 256, smem, st>>>(d, (const cpx<T>*)Y, (cpx<T>*)NL, jlo, kx, kz, pz, (const cpx<T>*)twz);
+        kern<<<grid, 256, smem, st>>>(d, (const cpx<T>*)Y, (cpx<T>*)NL, jlo, jhi, kx, kz, pz, (const cpx<T>*)twz);
     };
     switch (d.nz) {
 #define CASE(N) case N: go(k_zfwd_nl<T, N, TX>, true); break;
