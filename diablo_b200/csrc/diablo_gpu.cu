@@ -52,6 +52,10 @@ struct Handle {
     double* bsc = nullptr;
     double2* gsc = nullptr;
     double* phys = nullptr;
+    double* d_gyf = nullptr;
+    double* pw = nullptr;         // 4 physical fields (POISSON_P_CHAN, statistics), allocated on first use
+    double* d_me = nullptr;       // [4][nyp] mean profiles for the statistics
+    double* d_sums = nullptr;     // [9][nyp] plane sums of the statistics
     double *mult = nullptr, *piv = nullptr, *cup = nullptr, *bcv = nullptr;
     signed char* kind = nullptr;
     double* dtmin = nullptr;
@@ -118,7 +122,7 @@ void free_handle(Handle* h) {
     if (!h) return;
     for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
-                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->mult, h->piv, h->cup,
+                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->mult, h->piv, h->cup,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->d_err, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
                     h->twz_f};
     for (void* q : ptrs)
@@ -385,6 +389,7 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     const size_t nyp = (size_t)d.nyp;
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_dy, sizeof(double) * nyp);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_dyf, sizeof(double) * nyp);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_gyf, sizeof(double) * nyp);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_kx, sizeof(double) * d.ldx);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_kz, sizeof(double) * d.nkzp);
     if (e == cudaSuccess) e = dmalloc((void**)&h->cu, sb * d.nf);
@@ -444,6 +449,7 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = cudaMemcpy(h->d_kz, kz.data(), sizeof(double) * d.nkzp, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(h->d_dy, dy, sizeof(double) * nyp, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(h->d_dyf, dyf, sizeof(double) * nyp, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_gyf, gyf, sizeof(double) * nyp, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) h->twn_d = make_twiddles<double>(d.nx, &e);
     if (e == cudaSuccess) h->twm_d = make_twiddles<double>(d.nx / 2, &e);
     if (e == cudaSuccess) h->twz_d = make_twiddles<double>(d.nz, &e);
@@ -738,15 +744,157 @@ int diablo_gpu_fft_xz_to_physical(void* handle, const double* vv, double* v, int
     return DIABLO_OK;
 }
 
-int diablo_gpu_poisson_p_chan(void* handle) {
-    (void)handle;
-    return fail(DIABLO_ENOTSUP, "POISSON_P_CHAN is not built yet");
+static int ensure_work(Handle* h) {
+    if (h->pw) return DIABLO_OK;
+    const size_t pf = (size_t)h->d.nyp * h->d.nz * h->d.nx;
+    cudaError_t e = cudaMalloc((void**)&h->pw, sizeof(double) * 4 * pf);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->d_me, sizeof(double) * 4 * h->d.nyp);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->d_sums, sizeof(double) * 9 * h->d.nyp);
+    if (e != cudaSuccess) {
+        cudaFree(h->pw); cudaFree(h->d_me); cudaFree(h->d_sums);
+        h->pw = h->d_me = h->d_sums = nullptr;
+        return fail(DIABLO_ENOMEM, std::string("work buffers: ") + cudaGetErrorString(e));
+    }
+    return DIABLO_OK;
 }
 
+// POISSON_P_CHAN (channel.f:1217-1453): CP from the current velocity and
+// scalars.  The nine gradient fields go to physical space one at a time; the
+// products are summed there and transformed forward once.  CF is left as it
+// was (the reference uses CF1..CF3 as scratch here, so their values after
+// this call are not part of its result).
+int diablo_gpu_poisson_p_chan(void* handle) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    int rc = ensure_work(h);
+    if (rc) return rc;
+    const Dims& d = h->d;
+    const size_t pf = (size_t)d.nyp * d.nz * d.nx;
+    double* acc = h->pw;
+    double* pa = h->pw + pf;
+    double* pb = h->pw + 2 * pf;
+    const int j0 = 2, np = d.ny - 1;
+    ProfScope ps(h, DIABLO_KERNEL_OTHER);
+    auto to_phys = [&](int kind, double* dst) -> cudaError_t {
+        cudaError_t e = launch_grad_field(d, kind, h->cu, h->api_s, h->d_kx, h->d_kz, h->d_dyf, h->st);
+        if (e == cudaSuccess)
+            e = launch_zinv<double>(d, h->api_s, h->s_field, h->xb, h->x_field, 1, j0, np, h->pz, h->twz_d, h->st);
+        if (e == cudaSuccess) e = launch_xinv(d, h->xb, dst, j0, np, h->pm, h->twm_d, h->twn_d, h->st);
+        h->launches += 3;
+        return e;
+    };
+    // (du/dx)^2 + (dv/dy)^2 + (dw/dz)^2
+    for (int k = 0; k < 3; ++k) {
+        CK(to_phys(k, pa));
+        CK(launch_phys_fma(d, acc, pa, pa, 1.0, k == 0, h->st));
+    }
+    // 2 (du/dy)(dv/dx), 2 (dw/dy)(dv/dz), 2 (du/dz)(dw/dx)
+    for (int k = 3; k < 9; k += 2) {
+        CK(to_phys(k, pa));
+        CK(to_phys(k + 1, pb));
+        CK(launch_phys_fma(d, acc, pa, pb, 2.0, 0, h->st));
+    }
+    h->launches += 6;
+    CK(launch_xfwd(d, acc, h->xb, j0, np, h->pm, h->twm_d, h->twn_d, h->st));
+    CK(launch_zfwd_pack(d, h->xb, h->api_s, j0, np, h->pz, h->twz_d, h->st));
+    PoissonArgs a;
+    a.d = d;
+    a.rhs = h->api_s;
+    a.cth = h->cu + 3 * h->s_field;
+    a.cp = h->cp;
+    a.bsc = h->bsc;
+    a.gsc = h->gsc;
+    a.kx = h->d_kx;
+    a.kz = h->d_kz;
+    a.dy = h->d_dy;
+    a.dyf = h->d_dyf;
+    a.gyf = h->d_gyf;
+    for (int n = 0; n < 4; ++n) a.ri[n] = n < d.nth ? h->p.ri[n] : 0.0;
+    CK(launch_poisson_column(a, h->st));
+    h->launches += 3;
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
+}
+
+// SAVE_STATS_CHAN plane statistics (save_stats.f:104-347, 452-536) after
+// APPLY_BC_VEL (save_stats.f:28-36), in FP64.  Means are the (0,0) modes;
+// fluctuation sums run on the device over the physical fields.
 int diablo_gpu_stats(void* handle, double* profiles) {
-    (void)handle;
-    (void)profiles;
-    return fail(DIABLO_ENOTSUP, "statistics are not built yet");
+    Handle* h = (Handle*)handle;
+    if (!h || !profiles) return fail(DIABLO_EINVAL, "null pointer argument");
+    int rc = ensure_work(h);
+    if (rc) return rc;
+    const Dims& d = h->d;
+    const size_t nyp = (size_t)d.nyp, pf = nyp * d.nz * d.nx;
+    const int nstat_f = 3 + (d.nth > 0 ? 1 : 0);
+    ProfScope ps(h, DIABLO_KERNEL_OTHER);
+    {
+        dim3 grid((d.nkxp + 127) / 128, d.nkzt);
+        k_apply_bc_vel<<<grid, 128, 0, h->st>>>(d, h->cu, h->d_dy, h->d_dyf, h->p);
+        CK(cudaGetLastError());
+    }
+    // (0,0) modes of U1, U2, U3, TH1 and CP
+    std::vector<double2> m00((size_t)5 * nyp, make_double2(0.0, 0.0));
+    for (int f = 0; f < 5; ++f) {
+        const double2* src = f < 3 ? h->cu + (size_t)f * h->s_field
+                           : f == 3 ? (d.nth > 0 ? h->cu + 3 * h->s_field : nullptr) : h->cp;
+        if (!src) continue;
+        CK(cudaMemcpy2DAsync(m00.data() + (size_t)f * nyp, sizeof(double2), src, sizeof(double2) * h->s_plane,
+                             sizeof(double2), nyp, cudaMemcpyDeviceToHost, h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    std::vector<double> me(4 * nyp);
+    for (size_t j = 0; j < nyp; ++j)
+        for (int f = 0; f < 4; ++f) me[f * nyp + j] = m00[f * nyp + j].x;
+    CK(cudaMemcpyAsync(h->d_me, me.data(), sizeof(double) * me.size(), cudaMemcpyHostToDevice, h->st));
+    CK(launch_zinv<double>(d, h->cu, h->s_field, h->xb, h->x_field, nstat_f, 0, d.nyp, h->pz, h->twz_d, h->st));
+    for (int f = 0; f < nstat_f; ++f)
+        CK(launch_xinv(d, (const double2*)h->xb + (size_t)f * h->x_field, h->pw + (size_t)f * pf, 0, d.nyp, h->pm,
+                       h->twm_d, h->twn_d, h->st));
+    CK(launch_stats_planes(d, h->pw, h->pw + pf, h->pw + 2 * pf, d.nth > 0 ? h->pw + 3 * pf : nullptr, h->d_me,
+                           h->d_dy, h->d_dyf, h->d_sums, h->st));
+    h->launches += 3 + nstat_f;
+    std::vector<double> sums(9 * nyp);
+    CK(cudaMemcpyAsync(sums.data(), h->d_sums, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    double* out = profiles;
+    for (size_t q = 0; q < (size_t)DIABLO_NSTATS * nyp; ++q) out[q] = 0.0;
+    auto O = [&](int s, size_t j) -> double& { return out[(size_t)s * nyp + j]; };
+    auto S = [&](int k, size_t j) { return sums[(size_t)k * nyp + j]; };
+    const double* ume = me.data();
+    const double* wme = me.data() + 2 * nyp;
+    const double* thme = me.data() + 3 * nyp;
+    for (size_t j = 0; j < nyp; ++j) {
+        O(DIABLO_STAT_UME, j) = me[j];
+        O(DIABLO_STAT_VME, j) = me[nyp + j];
+        O(DIABLO_STAT_WME, j) = me[2 * nyp + j];
+        O(DIABLO_STAT_CP, j) = m00[4 * nyp + j].x;
+    }
+    // NX*NZ formed in single precision as in save_stats.f (FLOAT(NZ*NX))
+    const double nn = (double)((float)d.nz * (float)d.nx);
+    for (int j = 1; j <= d.ny; ++j) {
+        const double dg = h->gyf[j] - h->gyf[j - 1];
+        O(DIABLO_STAT_URMS, j) = std::sqrt(S(0, j) / nn);
+        O(DIABLO_STAT_VRMS, j) = std::sqrt(S(1, j) / nn);
+        O(DIABLO_STAT_WRMS, j) = std::sqrt(S(2, j) / nn);
+        O(DIABLO_STAT_UV, j) = S(3, j) / nn;
+        O(DIABLO_STAT_UW, j) = S(4, j) / nn;
+        O(DIABLO_STAT_WV, j) = S(5, j) / nn;
+        O(DIABLO_STAT_DUDY, j) = (ume[j] - ume[j - 1]) / dg;
+        O(DIABLO_STAT_DWDY, j) = (wme[j] - wme[j - 1]) / dg;
+        O(DIABLO_STAT_SHEAR, j) = S(6, j) / (double)(d.nx * d.nz);
+        if (d.nth > 0) {
+            O(DIABLO_STAT_THME, j) = thme[j];
+            O(DIABLO_STAT_THRMS, j) = std::sqrt(S(7, j) / nn);
+            O(DIABLO_STAT_THV, j) = S(8, j) / nn;
+            O(DIABLO_STAT_DTHDY, j) = (thme[j] - thme[j - 1]) / dg;
+        }
+    }
+    if (d.nth > 0) {
+        O(DIABLO_STAT_THME, 0) = thme[0];
+        O(DIABLO_STAT_THME, nyp - 1) = thme[nyp - 1];
+    }
+    return DIABLO_OK;
 }
 
 int diablo_gpu_synchronize(void* handle) {

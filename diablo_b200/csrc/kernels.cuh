@@ -98,4 +98,20 @@ struct RemDivArgs {
     int update_cp;        // CP += phi/h on J = 2..NY
 };
 
+// POISSON_P_CHAN column solve (poisson_stats.cu).
+struct PoissonArgs {
+    Dims d;
+    const double2* rhs;   // S, sum_ij (du_i/dx_j)(du_j/dx_i) on J = 2..NY-1
+    const double2* cth;   // S, N_TH scalar fields
+    double2* cp;          // S, receives CP on J = 1..NY
+    double* bsc;          // scratch pivots  [J][m][kx]
+    double2* gsc;         // scratch RHS     [J][m][kx]
+    const double* kx;
+    const double* kz;
+    const double* dy;
+    const double* dyf;
+    const double* gyf;
+    double ri[4];
+};
+
 }  // namespace dgpu

@@ -61,6 +61,18 @@ cudaError_t launch_remdiv(const RemDivArgs& a, cudaStream_t st);
 cudaError_t launch_cfl(const Dims& d, const void* X, size_t x_fstride, const FftPlan& pm,
                        const void* twm, const void* twn, const double* dy, double cfl, double dx,
                        double dz, double* dtmin, cudaStream_t st);
+// POISSON_P_CHAN and SAVE_STATS_CHAN pieces (poisson_stats.cu, FP64).
+// One velocity-gradient field of the pressure source into S (kinds 0..8).
+cudaError_t launch_grad_field(const Dims& d, int kind, const double2* cu, double2* out, const double* kx,
+                              const double* kz, const double* dyf, cudaStream_t st);
+// acc (+)= alpha*a*b on physical planes 2..NY.
+cudaError_t launch_phys_fma(const Dims& d, double* acc, const double* a, const double* b, double alpha, int init,
+                            cudaStream_t st);
+cudaError_t launch_poisson_column(const PoissonArgs& a, cudaStream_t st);
+// Plane sums of the second-order statistics, planes 1..NY (th may be null).
+cudaError_t launch_stats_planes(const Dims& d, const double* u1, const double* u2, const double* u3,
+                                const double* th, const double* me, const double* dy, const double* dyf, double* out,
+                                cudaStream_t st);
 // rows transformed together by the products kernel for a given NX
 int products_group(int nx);
 // Record the one-line message returned by diablo_gpu_last_error; returns code.
