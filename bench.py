@@ -37,11 +37,16 @@ import numpy as np  # noqa: E402
 METRIC = "RK3 steps/s at 512×257×384: FP32-split vs FP64 on 1 B200, err vs FP64 oracle"
 FALLBACK_HBM_GBS = 6650.0
 
-# DRAM traffic per launch of the column kernel, per plane of the S layout,
-# from the ncu capture summarised in profiles/column_kernel_512x65x384.md
-# (dram__bytes_read.sum + dram__bytes_write.sum / 67 planes); scaled to the
-# full grid by the number of planes (the kernel streams planes).
-COLUMN_TRAFFIC_PER_PLANE = {"fp32split": (829.99e6 + 728.24e6) / 67.0}
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) per
+# y-plane of the grid, from one ncu capture of each kernel at 512x65x384
+# (67 planes); scaled to a grid by its number of planes, the kernels
+# streaming planes.  FP32-split build.
+TRAFFIC_PER_PLANE = {
+    "zinv": (193.98e6 + 98.83e6) / 67.0,
+    "products": (146.79e6 + 330.22e6) / 67.0,
+    "zfwd_nl": (423.00e6 + 85.44e6) / 67.0,
+    "column": (735.09e6 + 629.72e6) / 67.0,
+}
 
 
 def parse_args():
@@ -286,9 +291,7 @@ def run_ours(args, rank, world, local_rank):
     dom_launches, dom_ms = ktimes[dom]
     avg_s = dom_ms / dom_launches / 1e3
     achieved = alg.get(dom, 0.0) / avg_s / 1e9 if dom in alg else None
-    traffic = None
-    if dom == "column":
-        traffic = COLUMN_TRAFFIC_PER_PLANE["fp32split"] * (w.p.ny + 2)
+    traffic = TRAFFIC_PER_PLANE[dom] * (w.p.ny + 2) if dom in TRAFFIC_PER_PLANE else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": alg.get(dom),
