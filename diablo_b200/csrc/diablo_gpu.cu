@@ -56,12 +56,12 @@ struct Handle {
     double* pw = nullptr;         // 4 physical fields (POISSON_P_CHAN, statistics), allocated on first use
     double* d_me = nullptr;       // [4][nyp] mean profiles for the statistics
     double* d_sums = nullptr;     // [9][nyp] plane sums of the statistics
-    double *mult = nullptr, *piv = nullptr, *cup = nullptr, *bcv = nullptr;
+    double* bcv = nullptr;        // [nf][nyp] BC-row values of the (0,0) mode
+    double* d_tabs = nullptr;     // [nf][part_table_doubles] CN partition factors
     signed char* kind = nullptr;
     double* dtmin = nullptr;
     double* d_k2 = nullptr;       // (KX^2+KZ^2)**BETA per padded column
     double* d_rows = nullptr;     // [RT_COUNT][nyp] reciprocal grid metrics
-    int* d_err = nullptr;         // kernel error flag (KERR_*)
     FftPlan pm, pz;   // NX/2-point complex plan (real x transforms), NZ-point plan
     void *twn_d = nullptr, *twm_d = nullptr, *twz_d = nullptr;   // exp(-2 pi i k/n), n = NX, NX/2, NZ
     void *twn_f = nullptr, *twm_f = nullptr, *twz_f = nullptr;
@@ -122,8 +122,8 @@ void free_handle(Handle* h) {
     if (!h) return;
     for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
-                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->mult, h->piv, h->cup,
-                    h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->d_err, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
+                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_tabs,
+                    h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
                     h->twz_f};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -281,8 +281,9 @@ int smem_limits(const Handle* h) {
     const int rows = group < d.nf + d.np ? group : d.nf + d.np;
     const size_t smem = sizeof(double) * (size_t)4 * d.nf * d.nx + 16 * (size_t)rows * (m + m / 16 + 1);
     if (group < 1 || smem > 227 * 1024) return fail(DIABLO_EINVAL, "NX too large for the number of fields");
-    // column kernels stage the per-row coefficients of every field
-    if ((33 * (size_t)d.nf + 16) * d.nyp > 200 * 1024) return fail(DIABLO_EINVAL, "NY too large");
+    // the column kernel holds whole columns: NY+2 <= 528 rows
+    if (part_rows(d.nyp) == 0) return fail(DIABLO_EINVAL, "NY too large (at most 526)");
+    if (colpart_smem<cpx<double>>(d) > 227 * 1024) return fail(DIABLO_EINVAL, "NY too large for the number of fields");
     return DIABLO_OK;
 }
 
@@ -303,19 +304,6 @@ int run_transforms(Handle* h) {
     return DIABLO_OK;
 }
 
-
-// Read and clear the kernels' error flag (after a stream synchronisation).
-int check_device_flag(Handle* h) {
-    int flag = 0;
-    CK(cudaMemcpyAsync(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    if (flag) {
-        CK(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->st));
-        CK(cudaStreamSynchronize(h->st));
-        return fail(DIABLO_ETIMEOUT, "a device pipeline wait timed out; results of the last calls are invalid");
-    }
-    return DIABLO_OK;
-}
 
 }  // namespace
 
@@ -402,15 +390,12 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = dmalloc((void**)&h->gsc, sb);
     if (e == cudaSuccess) e = dmalloc(&h->xb, sizeof(double2) * h->x_field * d.nf);
     if (e == cudaSuccess) e = dmalloc(&h->yb, sizeof(double2) * h->x_field * d.np);
-    if (e == cudaSuccess) e = dmalloc((void**)&h->mult, sizeof(double) * nyp * d.nf);
-    if (e == cudaSuccess) e = dmalloc((void**)&h->piv, sizeof(double) * nyp * d.nf);
-    if (e == cudaSuccess) e = dmalloc((void**)&h->cup, sizeof(double) * nyp * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_tabs, sizeof(double) * part_table_doubles(d.nyp) * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->bcv, sizeof(double) * nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->kind, nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->dtmin, sizeof(double));
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_k2, sizeof(double) * d.splane());
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_rows, sizeof(double) * RT_COUNT * nyp);
-    if (e == cudaSuccess) e = dmalloc((void**)&h->d_err, sizeof(int));
     if (e != cudaSuccess) {
         free_handle(h);
         return fail(e == cudaErrorMemoryAllocation ? DIABLO_ENOMEM : DIABLO_ECUDA,
@@ -516,7 +501,7 @@ int diablo_gpu_download_state(void* handle, double* cu1, double* cu2, double* cu
     }
     if (cp) CK(copy_fourier(h, h->cp, nullptr, cp, 0, d.nyp));
     CK(cudaStreamSynchronize(h->st));
-    return check_device_flag(h);
+    return DIABLO_OK;
 }
 
 int diablo_gpu_download_phi(void* handle, double* phi) {
@@ -607,9 +592,6 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     a.kz = h->d_kz;
     a.dy = h->d_dy;
     a.dyf = h->d_dyf;
-    a.mult = h->mult;
-    a.piv = h->piv;
-    a.cup = h->cup;
     a.bcv = h->bcv;
     a.kind = h->kind;
     for (int f = 0; f < MAXF; ++f) { a.cf_lo[f] = 2; a.cf_hi[f] = d.ny; a.cb_lo[f] = 1; }
@@ -633,24 +615,21 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     a.rk_step = rk_step;
     a.store_cf = 1;
     { ProfScope ps(h, DIABLO_KERNEL_CN_COEF);
-      CK(launch_cn_coef(d, a, h->mult, h->piv, h->cup, h->bcv, h->kind, h->bc_type, h->bc_c1, h->st)); }
+      CK(launch_cn_part(d, a, h->d_tabs, h->bcv, h->kind, h->bc_type, h->bc_c1, h->st)); }
     const bool cfl = p.variable_dt && rk_step == 3 && (time_step % p.update_dt) == 0;
     ColArgs ca;
     ca.cn = a;
     ca.k2 = h->d_k2;
     ca.rows = h->d_rows;
     ca.phi = h->phi;
-    ca.bsc = h->bsc;
-    ca.gsc = h->gsc;
     ca.inv_h = 1.0 / TEMP4;
     ca.project = cfl ? 0 : 1;     // COURANT sees the velocity before the projection
     ca.update_cp = 1;
     ca.store_phi = 0;             // phi stays where REM_DIV_CHAN alone puts it
-    ca.err = h->d_err;
     {
         ProfScope ps(h, DIABLO_KERNEL_COLUMN);
-        if (h->fp32) CK(launch_column<cpx<float>>(ca, (const cpx<float>*)h->nl, h->st));
-        else CK(launch_column<cpx<double>>(ca, (const cpx<double>*)h->nl, h->st));
+        if (h->fp32) CK(launch_colpart<cpx<float>>(ca, (const cpx<float>*)h->nl, h->d_tabs, h->st));
+        else CK(launch_colpart<cpx<double>>(ca, (const cpx<double>*)h->nl, h->d_tabs, h->st));
     }
     h->launches += 2;
     if (!cfl) return DIABLO_OK;
@@ -901,7 +880,7 @@ int diablo_gpu_synchronize(void* handle) {
     Handle* h = (Handle*)handle;
     if (!h) return fail(DIABLO_EINVAL, "null handle");
     CK(cudaStreamSynchronize(h->st));
-    return check_device_flag(h);
+    return DIABLO_OK;
 }
 
 int diablo_gpu_get_stream(void* handle, void** stream) {

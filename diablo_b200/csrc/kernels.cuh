@@ -37,9 +37,6 @@ struct CnArgs {
     const double* kz;     // KZ(0..TNKZ)
     const double* dy;     // DY(0..NY+1)
     const double* dyf;    // DYF(0..NY+1)
-    const double* mult;   // [nf][nyp] forward multipliers -A(j)/B'(j-1)
-    const double* piv;    // [nf][nyp] reciprocal pivots 1/B'(j) (0 where B'(j) = 0)
-    const double* cup;    // [nf][nyp] upper diagonal C(j)
     const double* bcv;    // [nf][nyp] RHS of BC rows for the (0,0) mode
     const signed char* kind;  // [nf][nyp] 0: interior row, 1: BC row
     int cf_lo[MAXF], cf_hi[MAXF];   // rows where CF is formed
@@ -50,6 +47,18 @@ struct CnArgs {
     double forcing;       // value subtracted from CR1(0,0,j) (F_TYPE 1/2), already * TEMP4
     int rk_step;
     int store_cf;
+};
+
+// Everything the CN row set-up needs (k_cn_part).
+struct CoefParams {
+    Dims d;
+    const double* dy;
+    const double* dyf;
+    double temp1, nu_v_scale;
+    double pr[4];
+    int jstart_th[4];
+    int bc_type[MAXF][2];
+    double bc_c1[MAXF][2];
 };
 
 // Per-row grid metrics shared by all columns (reciprocals computed once, so
@@ -66,21 +75,16 @@ enum RowTab {
     RT_COUNT
 };
 
-// The fused column kernel (colfused.cu): CnArgs plus the projection.
-constexpr int COL_STAGES = 8;   // rows of every operand in flight per block
-
+// The column kernel (colpart.cu): CnArgs plus the projection.
 struct ColArgs {
     CnArgs cn;
     const double* k2;     // (KX^2+KZ^2)**BETA per padded column [m][kx]
     const double* rows;   // [RT_COUNT][nyp] row tables
     double2* phi;         // S, phi (J = 1..NY), written when store_phi
-    double* bsc;          // scratch: pivots of the bottom-up phi elimination
-    double2* gsc;         // scratch: right-hand sides of that elimination
     double inv_h;         // 1/TEMP4
-    int project;          // run REM_DIV (sweeps 2b and 3)
+    int project;          // run the REM_DIV projection
     int update_cp;        // CP += phi/h on J = 2..NY
     int store_phi;
-    int* err;             // device error flag (KERR_*)
 };
 
 struct RemDivArgs {

@@ -46,14 +46,19 @@ cudaError_t launch_zfwd_pack(const Dims& d, const void* X, double2* S, int j0, i
                              const FftPlan& pz, const void* twz, cudaStream_t st);
 
 // Column kernels (FP64).
-cudaError_t launch_cn_coef(const Dims& d, const CnArgs& a, double* mult, double* piv, double* cup,
-                           double* bcv, signed char* kind, const int* bc_type, const double* bc_c1,
-                           cudaStream_t st);
-// Fused column kernel: RHS, CN solves, projection and pressure update.
+// CN rows of every field and their partition factors (column-independent),
+// the BC-row values of the (0,0) mode and the row kinds.
+cudaError_t launch_cn_part(const Dims& d, const CnArgs& a, double* tabs, double* bcv, signed char* kind,
+                           const int* bc_type, const double* bc_c1, cudaStream_t st);
+// doubles of the partition tables per field
+size_t part_table_doubles(int nyp);
+// rows per CN block of the partition solve (0 when NY+2 > 528)
+int part_rows(int nyp);
+// One pass per column pair: RHS, CN solves, projection and pressure update.
 template <typename TN>
-cudaError_t launch_column(const ColArgs& a, const TN* nl, cudaStream_t st);
+cudaError_t launch_colpart(const ColArgs& a, const TN* nl, const double* tabs, cudaStream_t st);
 template <typename TN>
-size_t column_smem(const Dims& d);
+size_t colpart_smem(const Dims& d);
 cudaError_t launch_remdiv(const RemDivArgs& a, cudaStream_t st);
 
 // CFL minimum (courant.f:35-47) over planes 1..NY of the physical velocity
