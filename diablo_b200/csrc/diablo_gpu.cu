@@ -58,6 +58,7 @@ struct Handle {
     double* d_sums = nullptr;     // [9][nyp] plane sums of the statistics
     double* bcv = nullptr;        // [nf][nyp] BC-row values of the (0,0) mode
     double* d_tabs = nullptr;     // [nf][part_table_doubles] CN partition factors
+    double* d_phitab = nullptr;   // [column][phi_table_doubles/column] phi partition factors
     signed char* kind = nullptr;
     double* dtmin = nullptr;
     double* d_k2 = nullptr;       // (KX^2+KZ^2)**BETA per padded column
@@ -122,7 +123,7 @@ void free_handle(Handle* h) {
     if (!h) return;
     for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
-                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_tabs,
+                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_tabs, h->d_phitab,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
                     h->twz_f};
     for (void* q : ptrs)
@@ -391,6 +392,7 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = dmalloc(&h->xb, sizeof(double2) * h->x_field * d.nf);
     if (e == cudaSuccess) e = dmalloc(&h->yb, sizeof(double2) * h->x_field * d.np);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_tabs, sizeof(double) * part_table_doubles(d.nyp) * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_phitab, sizeof(double) * phi_table_doubles(d));
     if (e == cudaSuccess) e = dmalloc((void**)&h->bcv, sizeof(double) * nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->kind, nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->dtmin, sizeof(double));
@@ -441,6 +443,8 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) h->twn_f = make_twiddles<float>(d.nx, &e);
     if (e == cudaSuccess) h->twm_f = make_twiddles<float>(d.nx / 2, &e);
     if (e == cudaSuccess) h->twz_f = make_twiddles<float>(d.nz, &e);
+    if (e == cudaSuccess) e = launch_phi_part(d, h->d_rows, h->d_kx, h->d_kz, h->d_phitab, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
     if (e != cudaSuccess) {
         free_handle(h);
         return fail(DIABLO_ECUDA, std::string("device set-up: ") + cudaGetErrorString(e));
@@ -621,6 +625,7 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     ca.cn = a;
     ca.k2 = h->d_k2;
     ca.rows = h->d_rows;
+    ca.phitab = h->d_phitab;
     ca.phi = h->phi;
     ca.inv_h = 1.0 / TEMP4;
     ca.project = cfl ? 0 : 1;     // COURANT sees the velocity before the projection

@@ -80,6 +80,7 @@ struct ColArgs {
     CnArgs cn;
     const double* k2;     // (KX^2+KZ^2)**BETA per padded column [m][kx]
     const double* rows;   // [RT_COUNT][nyp] row tables
+    const double* phitab; // per column: partition factors of the phi system
     double2* phi;         // S, phi (J = 1..NY), written when store_phi
     double inv_h;         // 1/TEMP4
     int project;          // run the REM_DIV projection

@@ -52,8 +52,12 @@ cudaError_t launch_cn_part(const Dims& d, const CnArgs& a, double* tabs, double*
                            const int* bc_type, const double* bc_c1, cudaStream_t st);
 // doubles of the partition tables per field
 size_t part_table_doubles(int nyp);
-// rows per CN block of the partition solve (0 when NY+2 > 528)
+// rows per CN block of the partition solve (0 when NY+2 > 544)
 int part_rows(int nyp);
+// Per-column partition factors of the phi system (built once per instance).
+size_t phi_table_doubles(const Dims& d);
+cudaError_t launch_phi_part(const Dims& d, const double* rows, const double* kx, const double* kz, double* tab,
+                            cudaStream_t st);
 // One pass per column pair: RHS, CN solves, projection and pressure update.
 template <typename TN>
 cudaError_t launch_colpart(const ColArgs& a, const TN* nl, const double* tabs, cudaStream_t st);
