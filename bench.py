@@ -132,17 +132,18 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 def algorithmic_bytes(p, prec: str) -> dict:
     nkxp, nkzt, nyp, nz = p.nx // 3 + 1, 2 * (p.nz // 3) + 1, p.ny + 2, p.nz
-    nf, npr = 3 + p.n_th, 8 + 3 * p.n_th
+    nf = 3 + p.n_th
     tb = 8 if prec == "fp32split" else 16          # complex element of the transform path
     A = nkxp * nkzt                                  # dealiased modes per plane
     X = nz * nkxp                                    # x-spectrum entries per plane
     planes_p = p.ny - 1                              # product planes 2..NY
     col = (nf * 16 + (2.0 / 3.0) * nf * 16 + nf * tb + 16    # read CU, CF (rk>1), NL, CP
            + nf * 16 + nf * 16 + 16)                          # write CU, CF, CP
+    nq = 2 * nf                                      # product outputs (ikx*Pa + Pflux, Pz per field)
     return {
         "zinv": nf * nyp * (A * 16 + X * tb),
-        "products": nf * nyp * X * tb + npr * planes_p * X * tb,
-        "zfwd_nl": npr * planes_p * X * tb + nf * planes_p * A * tb,
+        "products": nf * nyp * X * tb + nq * planes_p * X * tb,
+        "zfwd_nl": nq * planes_p * X * tb + nf * planes_p * A * tb,
         "column": col * A * nyp,
     }
 

@@ -280,7 +280,7 @@ int smem_limits(const Handle* h) {
     const int group = products_group(d.nx);
     const int m = d.nx / 2;
     const int rows = group < d.nf + d.np ? group : d.nf + d.np;
-    const size_t smem = sizeof(double) * (size_t)4 * d.nf * d.nx + 16 * (size_t)rows * (m + m / 16 + 1);
+    const size_t smem = sizeof(double) * (size_t)4 * d.nf * d.nx + 16 * (size_t)rows * (m + m / 16 + 1) + 16 * 3 * (size_t)m;
     if (group < 1 || smem > 227 * 1024) return fail(DIABLO_EINVAL, "NX too large for the number of fields");
     // the column kernel holds whole columns: NY+2 <= 528 rows
     if (part_rows(d.nyp) == 0) return fail(DIABLO_EINVAL, "NY too large (at most 526)");
@@ -298,7 +298,8 @@ int run_transforms(Handle* h) {
     { ProfScope ps(h, DIABLO_KERNEL_ZINV);
       CK(launch_zinv<T>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, twz, h->st)); }
     { ProfScope ps(h, DIABLO_KERNEL_PRODUCTS);
-      CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, 32, h->d_dy, h->d_dyf, h->pm, twm, twn, h->st)); }
+      CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, 32, h->d_dy, h->d_dyf, h->d_kx, h->pm, twm, twn,
+                            h->st)); }
     { ProfScope ps(h, DIABLO_KERNEL_ZFWD_NL);
       CK(launch_zfwd_nl<T>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->d_kx, h->d_kz, h->pz, twz, h->st)); }
     h->launches += 3;

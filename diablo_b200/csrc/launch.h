@@ -19,16 +19,17 @@ cudaError_t launch_zinv(const Dims& d, const double2* S, size_t s_fstride, void*
 // Fused per z-row: backward x transform of the fields at planes jlo-1..jhi+1,
 // the 8 + 3*N_TH physical products of RK_CHAN_1 (channel.f:410-571,
 // 670-720) at planes jlo..jhi, forward x transform with 1/NX and truncation
-// to kx <= NKX (mpi.f:1493-1508) -> Y.
+// to kx <= NKX (mpi.f:1493-1508), combined into 2 outputs per field
+// (ikx*Pa + Pflux, Pz) -> Y.
 // pm/twm: plan and table of the NX/2-point complex FFT; twn: table of NX.
 template <typename T>
 cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int jhi, int chunk,
-                            const double* dy, const double* dyf, const FftPlan& pm, const void* twm,
-                            const void* twn, cudaStream_t st);
+                            const double* dy, const double* dyf, const double* kx, const FftPlan& pm,
+                            const void* twm, const void* twn, cudaStream_t st);
 
-// Per plane: forward z transform of every product, kz packing and 1/NZ
-// (mpi.f:1526-1540), then the derivative combination into the nonlinear
-// term of each field (CF -= ik*(.) or -(.)) -> NL (type T, S layout).
+// Per plane: forward z transform of the 2 product outputs of every field,
+// kz packing and 1/NZ (mpi.f:1526-1540), then NL = -(first) - ikz (second)
+// -> NL (type T, S layout).
 template <typename T>
 cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int jhi,
                            const double* kx, const double* kz, const FftPlan& pz, const void* twz,

@@ -151,11 +151,32 @@ __device__ __forceinline__ void row_fft(cpx<T>* buf, int nrows, const L& lay, co
 // ---------------------------------------------------------------------------
 constexpr int RING = 4;
 
+// Sources of product output q (x spectra, S layout of the nonlinear terms of
+// channel.f:410-571, 670-720): field f = q/2 has
+//   q = 2f:   ikx*Pa + Pflux   (the x-derivative and y-flux terms)
+//   q = 2f+1: Pz               (the z-derivative term, ikz applied after the z transform)
+//   U1: Pa=P1 (U1U1), Pflux=P5, Pz=P0 (U1U3)   U2: Pa=P3, Pflux=P7, Pz=P4
+//   U3: Pa=P0 (U1U3), Pflux=P6, Pz=P2          TH_n: Pa=P(8+3n), Pflux=P(10+3n), Pz=P(9+3n)
+__device__ __forceinline__ int field_pz(int f) { return f == 0 ? 0 : f == 1 ? 4 : f == 2 ? 2 : 9 + 3 * (f - 3); }
+__device__ __forceinline__ int field_sources(int q, int* sp, bool* sx) {
+    const int f = q >> 1;
+    int pa, pf, pz;
+    if (f == 0) { pa = 1; pf = 5; pz = 0; }
+    else if (f == 1) { pa = 3; pf = 7; pz = 4; }
+    else if (f == 2) { pa = 0; pf = 6; pz = 2; }
+    else { const int n = f - 3; pa = 8 + 3 * n; pf = 10 + 3 * n; pz = 9 + 3 * n; }
+    if (q & 1) { sp[0] = pz; sx[0] = false; return 1; }
+    sp[0] = pa; sx[0] = true;
+    sp[1] = pf; sx[1] = false;
+    return 2;
+}
+
 template <typename T, int MC>
 __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __restrict__ X,
                                                      cpx<T>* __restrict__ Y, int jlo, int jhi, int chunk,
                                                      int group, const double* __restrict__ dy,
-                                                     const double* __restrict__ dyf, FftPlan pm,
+                                                     const double* __restrict__ dyf,
+                                                     const double* __restrict__ kxw, FftPlan pm,
                                                      const cpx<T>* __restrict__ twm,
                                                      const cpx<T>* __restrict__ twn) {
     extern __shared__ unsigned char smem_raw[];
@@ -166,8 +187,13 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
     Lay lay;
     if constexpr (MC == 0) lay.pitch = row_pitch(M);
     T* ring = reinterpret_cast<T*>(smem_raw);                                 // [RING][nf][nx]
-    cpx<T>* buf = reinterpret_cast<cpx<T>*>(ring + (size_t)RING * nf * nx);  // [group][pitch]
+    cpx<T>* stw = reinterpret_cast<cpx<T>*>(ring + (size_t)RING * nf * nx);  // twiddles: M then NX
+    cpx<T>* buf = stw + 3 * M;                                                // [group][pitch]
     T* tbuf = reinterpret_cast<T*>(buf);
+    for (int e = threadIdx.x; e < 3 * M; e += 256) stw[e] = e < M ? twm[e] : twn[e - M];
+    twm = stw;
+    twn = stw + M;
+    __syncthreads();
     const int z = blockIdx.x;
     const int jb = jlo + blockIdx.y * chunk;
     const int je = min(jb + chunk - 1, jhi);
@@ -250,11 +276,30 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
                 }
             }
             if (p1 > p0) {
-                for (int e = threadIdx.x; e < (p1 - p0) * d.ldx; e += 256) {
-                    const int q = e / d.ldx, k = e % d.ldx;
-                    const int p = p0 + q;
-                    Y[(size_t)p * xf + (size_t)jp * xrow + (size_t)z * d.ldx + k] =
-                        extract_real_forward(buf, lay, nf + p - c0, M, d.nkx, twn, k, inv_nx);
+                // outputs of field f: 2f = ikx*Pa + Pflux, 2f+1 = Pz (field_sources);
+                // an output whose sources span two batches is completed by adding to
+                // what the earlier batch stored
+                for (int e = threadIdx.x; e < nf * d.ldx; e += 256) {
+                    const int f = e / d.ldx, k = e % d.ldx;
+                    int sp[2];
+                    bool sx[2];
+                    field_sources(2 * f, sp, sx);
+                    const int pz = field_pz(f);
+                    cpx<T>* ya = Y + (size_t)(2 * f) * xf + (size_t)jp * xrow + (size_t)z * d.ldx + k;
+                    const bool ina = sp[0] >= p0 && sp[0] < p1, inf = sp[1] >= p0 && sp[1] < p1;
+                    if (ina || inf) {
+                        cpx<T> v = mk<T>(0, 0);
+                        if (ina) {
+                            const cpx<T> x = extract_real_forward(buf, lay, nf + sp[0] - c0, M, d.nkx, twn, k, inv_nx);
+                            const T K = (T)kxw[k];
+                            v = mk<T>(-K * x.y, K * x.x);
+                        }
+                        if (inf) v = v + extract_real_forward(buf, lay, nf + sp[1] - c0, M, d.nkx, twn, k, inv_nx);
+                        if ((!ina && sp[0] < p0) || (!inf && sp[1] < p0)) v = v + *ya;
+                        *ya = v;
+                    }
+                    if (pz >= p0 && pz < p1)
+                        ya[xf] = extract_real_forward(buf, lay, nf + pz - c0, M, d.nkx, twn, k, inv_nx);
                 }
             }
             __syncthreads();
@@ -263,22 +308,20 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
 }
 
 // ---------------------------------------------------------------------------
-// K3: per plane, kx tile and field: forward z transform of the three
-// products that feed the field, kz packing with 1/NZ, and the derivative
+// K3: per plane, kx tile and field: forward z transform of the two product
+// outputs that feed the field, kz packing with 1/NZ, and the derivative
 // combination into the nonlinear term (channel.f:410-571, 670-720):
 //   U1: -ikz P0 - ikx P1 - P5      U2: -ikx P3 - ikz P4 - P7
 //   U3: -ikx P0 - ikz P2 - P6      TH_n: -ikx P(8+3n) - ikz P(9+3n) - P(10+3n)
 // with P0 = U1U3, P1 = U1U1, P2 = U3U3, P3/P4 = (U1/U3 at GY) U2,
-// P5..P7 the y-flux differences.
+// P5..P7 the y-flux differences; the ikx and y-flux terms arrive already
+// summed from K2.
 // ---------------------------------------------------------------------------
+// The two product outputs of field f (see field_sources) and their use:
+// NL_f = -(z transform of output 2f) - ikz (z transform of output 2f+1).
 __device__ __forceinline__ void field_products(int f, int* p, int* mlt) {
-    if (f == 0) { p[0] = 0; mlt[0] = 2; p[1] = 1; mlt[1] = 1; p[2] = 5; mlt[2] = 0; }
-    else if (f == 1) { p[0] = 3; mlt[0] = 1; p[1] = 4; mlt[1] = 2; p[2] = 7; mlt[2] = 0; }
-    else if (f == 2) { p[0] = 0; mlt[0] = 1; p[1] = 2; mlt[1] = 2; p[2] = 6; mlt[2] = 0; }
-    else {
-        const int n = f - 3;
-        p[0] = 8 + 3 * n; mlt[0] = 1; p[1] = 9 + 3 * n; mlt[1] = 2; p[2] = 10 + 3 * n; mlt[2] = 0;
-    }
+    p[0] = 2 * f; mlt[0] = 0;
+    p[1] = 2 * f + 1; mlt[1] = 2;
 }
 
 // 16-byte asynchronous global -> shared copies (sm_80+ cp.async).
@@ -292,7 +335,7 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Block: kx tile of TX columns, field f, planes J0 .. J0+ZF_PLANES-1.  The
-// 3*ZF_PLANES product tiles it consumes stream through two shared buffers
+// 2*ZF_PLANES product tiles it consumes stream through two shared buffers
 // (cp.async), the next tile in flight while the current one is transformed.
 constexpr int ZF_PLANES = 8;
 constexpr int ZF_TX = 8;
@@ -316,14 +359,14 @@ __global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __rest
     const size_t xrow = (size_t)nz * d.ldx;
     const size_t xf = (size_t)d.nyp * xrow;
     const T inv_nz = T(1.0 / (double)nz);
-    int prod[3], mlt[3];
+    int prod[2], mlt[2];
     field_products(f, prod, mlt);
     const size_t sp = d.splane();
     const size_t sf = (size_t)d.nyp * sp;
     constexpr int CH = (int)(TX * sizeof(cpx<T>) / 16);           // 16-byte chunks per z row
     auto load = [&](int t, int buf) {                             // tile t = 3*plane + product
-        const int J = J0 + t / 3;
-        const cpx<T>* src = Y + (size_t)prod[t % 3] * xf + (size_t)J * xrow + kx0;
+        const int J = J0 + t / 2;
+        const cpx<T>* src = Y + (size_t)prod[t % 2] * xf + (size_t)J * xrow + kx0;
         unsigned char* dst = reinterpret_cast<unsigned char*>(bufs + (size_t)buf * nz * TX);
         for (int e = threadIdx.x; e < nz * CH; e += 256) {
             const int z = e / CH, q = e % CH;
@@ -332,11 +375,11 @@ __global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __rest
         }
         cp_async_commit();
     };
-    const int ntiles = 3 * nplanes;
+    const int ntiles = 2 * nplanes;
     load(0, 0);
     cpx<T> acc[QA];
     for (int t = 0; t < ntiles; ++t) {
-        const int pl = t / 3, r = t % 3;
+        const int pl = t / 2, r = t % 2;
         if (t + 1 < ntiles) {
             load(t + 1, (t + 1) & 1);
             cp_async_wait<1>();
@@ -380,7 +423,7 @@ __global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __rest
                 sacc[e] = a;
             }
         }
-        if (r == 2) {
+        if (r == 1) {
             cpx<T>* dst = NL + (size_t)f * sf + (size_t)(J0 + pl) * sp + kx0;
             if constexpr (NC > 0) {
 #pragma unroll
@@ -433,19 +476,20 @@ int products_group(int nx) {
 
 template <typename T>
 cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int jhi, int chunk,
-                            const double* dy, const double* dyf, const FftPlan& pm, const void* twm,
-                            const void* twn, cudaStream_t st) {
+                            const double* dy, const double* dyf, const double* kx, const FftPlan& pm,
+                            const void* twm, const void* twn, cudaStream_t st) {
     if (jhi < jlo) return cudaSuccess;
     const int group = products_group(d.nx);
     if (group < 1) return cudaErrorInvalidValue;
     const int M = d.nx / 2;
     const int rows = group < d.nf + d.np ? group : d.nf + d.np;
-    const size_t smem = sizeof(T) * (size_t)RING * d.nf * d.nx + sizeof(cpx<T>) * (size_t)rows * row_pitch(M);
+    const size_t smem = sizeof(T) * (size_t)RING * d.nf * d.nx + sizeof(cpx<T>) * (size_t)rows * row_pitch(M) +
+                        sizeof(cpx<T>) * 3 * (size_t)M;
     const int nchunks = (jhi - jlo + chunk) / chunk;
     dim3 grid(d.nz, nchunks);
     auto go = [&](auto kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, 256, smem, st>>>(d, (const cpx<T>*)X, (cpx<T>*)Y, jlo, jhi, chunk, group, dy, dyf, pm,
+        kern<<<grid, 256, smem, st>>>(d, (const cpx<T>*)X, (cpx<T>*)Y, jlo, jhi, chunk, group, dy, dyf, kx, pm,
                                       (const cpx<T>*)twm, (const cpx<T>*)twn);
     };
     switch (M) {
@@ -659,10 +703,10 @@ template cudaError_t launch_zinv<float>(const Dims&, const double2*, size_t, voi
 template cudaError_t launch_zinv<double>(const Dims&, const double2*, size_t, void*, size_t, int, int, int,
                                          const FftPlan&, const void*, cudaStream_t);
 template cudaError_t launch_products<float>(const Dims&, const void*, void*, int, int, int, const double*,
-                                            const double*, const FftPlan&, const void*, const void*,
+                                            const double*, const double*, const FftPlan&, const void*, const void*,
                                             cudaStream_t);
 template cudaError_t launch_products<double>(const Dims&, const void*, void*, int, int, int, const double*,
-                                             const double*, const FftPlan&, const void*, const void*,
+                                             const double*, const double*, const FftPlan&, const void*, const void*,
                                              cudaStream_t);
 template cudaError_t launch_zfwd_nl<float>(const Dims&, const void*, void*, int, int, const double*,
                                            const double*, const FftPlan&, const void*, cudaStream_t);
