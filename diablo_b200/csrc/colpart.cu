@@ -354,6 +354,7 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
     double2* sPh = sU;                              // phi (C-D), in the old-CU slots
     double* sR = reinterpret_cast<double*>(sF + NF2);
     signed char* sK = reinterpret_cast<signed char*>(sR + RT_COUNT * NROW);
+    double* sC = reinterpret_cast<double*>(sR + RT_COUNT * NROW) + (nf * NROW + 7) / 8;   // [MAXF][10]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const size_t ps = d.splane();
     const size_t fs = ps * nyp;
@@ -392,6 +393,25 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
         for (int e = tid; e < nf * NROW; e += NT) {
             const int f = e / NROW, j = e % NROW;
             sK[e] = j < nyp ? a.kind[f * nyp + j] : (signed char)1;
+        }
+        // per-field coefficients of the explicit terms (channel.f:77-293):
+        // nu_f, U1 and U3 couplings, CN factor, horizontal gravity, is-U2,
+        // KX / KZ selectors of the pressure gradient, first and last CF row
+        if (tid < nf) {
+            const int f = tid;
+            double* q = sC + f * 10;
+            double nuf = a.nu, cU1 = 0.0, cU3 = 0.0, cn_c = a.temp1 * a.nu_v_scale, cthv = 0.0, kxs = 0.0, kzs = 0.0;
+            if (f == 0) { cU3 = a.i_ro; kxs = 1.0; cthv = a.grav_x; }
+            else if (f == 2) { cU1 = -a.i_ro; kzs = 1.0; cthv = a.grav_z; }
+            else if (f >= 3) {
+                const int n = f - 3;
+                nuf = a.nu / a.pr[n];
+                cU1 = -a.drhodx[n];
+                cU3 = -a.drhodz[n];
+                cn_c = (a.temp1 / a.pr[n]) * a.nu_v_scale;
+            }
+            q[0] = nuf; q[1] = cU1; q[2] = cU3; q[3] = cn_c; q[4] = cthv; q[5] = f == 1 ? 1.0 : 0.0;
+            q[6] = kxs; q[7] = kzs; q[8] = (double)a.cf_lo[f]; q[9] = (double)a.cf_hi[f];
         }
         cp_async_wait_all();
     }
@@ -435,57 +455,48 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
         const bool zero_mode = zm0 && c == 0;
         const double KX = c ? KX1 : KX0;
         const double k2 = c ? k21 : k20;
+        const double fzm = zero_mode ? 1.0 : 0.0;
+        const double t3 = rk1 ? a.temp3 : 0.0;
         double2 Gv[NIT];
-        // all right-hand sides first, then the stores: the items interleave
+        // all right-hand sides first, then the stores; straight-line items
+        // (selects, predicated stores) so that they interleave
 #pragma unroll
         for (int it = 0; it < NIT; ++it) {
-            Gv[it] = zero;
-            if (tid + it * NT >= nitem) continue;
-            const int j = jj[it], f = ff[it];
-            double nuf = a.nu, cU1 = 0.0, cU3 = 0.0, cn_c = a.temp1 * a.nu_v_scale, Kf = 0.0, cthv = 0.0;
-            if (f == 0) { cU3 = a.i_ro; Kf = KX; cthv = a.grav_x; }
-            else if (f == 2) { cU1 = -a.i_ro; Kf = KZm; cthv = a.grav_z; }
-            else if (f >= 3) {
-                const int n = f - 3;
-                nuf = a.nu / a.pr[n];
-                cU1 = -a.drhodx[n];
-                cU3 = -a.drhodz[n];
-                cn_c = (a.temp1 / a.pr[n]) * a.nu_v_scale;
-            }
-            const bool isu2 = (f == 1);
+            const bool valid = tid + it * NT < nitem;
+            const int j = valid ? jj[it] : 0, f = valid ? ff[it] : 0;
+            const double* cq = sC + f * 10;
+            const double nuf = cq[0], cU1 = cq[1], cU3 = cq[2], cn_c = cq[3], cthv = cq[4], fu2 = cq[5];
+            const double Kf = cq[6] * KX + cq[7] * KZm;
+            const bool inr = j >= (int)cq[8] && j <= (int)cq[9];
+            const bool isu2 = fu2 != 0.0;
+            const int jm = j >= 1 ? j - 1 : 0, jp = j + 1 < nyp ? j + 1 : nyp - 1;
+            const double wm = j >= 1 ? 1.0 : 0.0, wp = j + 1 < nyp ? 1.0 : 0.0;
             const double2 w1 = sU[slot(f, j, c)];
-            double2 G = zero;
-            const int knd = sK[f * NROW + j];
-            if (j >= a.cf_lo[f] && j <= a.cf_hi[f]) {
-                const double2 w0 = j >= 1 ? sU[slot(f, j - 1, c)] : zero;
-                const double2 w2 = j + 1 < nyp ? sU[slot(f, j + 1, c)] : zero;   // row NY+2 is zero
-                double2 cpl = cU1 * sU[slot(0, j, c)] + cU3 * sU[slot(2, j, c)];
+            const double2 w0 = wm * sU[slot(f, jm, c)];
+            const double2 w2 = wp * sU[slot(f, jp, c)];          // row NY+2 is zero
+            double2 cpl = cU1 * sU[slot(0, j, c)] + cU3 * sU[slot(2, j, c)];
 #pragma unroll
-                for (int n = 0; n < NTHMAX; ++n) {
-                    if (n < d.nth) {
-                        const double2 thj = sU[slot(3 + n, j, c)];
-                        cpl = cpl + (a.ri[n] * cthv) * thj;
-                        if (isu2 && !zero_mode) {
-                            const double2 thm = j >= 1 ? sU[slot(3 + n, j - 1, c)] : zero;
-                            cpl = cpl + (a.ri[n] * a.grav_y) * (BY0[j] * thj + BY1[j] * thm);
-                        }
-                    }
-                }
-                const double2 CF = (-nuf * k2) * w1 + cpl + as_d2(nlv[it]);
-                if (a.store_cf) a.cf[(size_t)f * fs + (size_t)j * ps + g0 + c] = CF;
-                if (knd == 0) {
-                    const double2 cpj = sP[j * 2 + c];
-                    double2 R = w1;
-                    if (rk1) R = R + a.temp3 * sW[slot(f, j, c)];
-                    R = R - a.temp4 * ik(Kf, cpj);
-                    if (isu2) R = R - (a.temp4 * RDY[j]) * (cpj - (j >= 1 ? sP[(j - 1) * 2 + c] : zero));
-                    if (f == 0 && zero_mode) R.x -= a.forcing;
-                    R = R + a.temp5 * CF;
-                    const double ep = isu2 ? E2P[j] : E1P[j], em = isu2 ? E2M[j] : E1M[j];
-                    G = R + cn_c * (ep * (w2 - w1) - em * (w1 - w0));
+            for (int n = 0; n < NTHMAX; ++n) {
+                if (n < d.nth) {
+                    const double2 thj = sU[slot(3 + n, j, c)];
+                    const double2 thm = wm * sU[slot(3 + n, jm, c)];
+                    cpl = cpl + (a.ri[n] * cthv) * thj +
+                          (fu2 * (1.0 - fzm) * a.ri[n] * a.grav_y) * (BY0[j] * thj + BY1[j] * thm);
                 }
             }
+            const double2 CF = (-nuf * k2) * w1 + cpl + as_d2(nlv[it]);
+            const double2 cpj = sP[j * 2 + c];
+            const double2 cpm = wm * sP[jm * 2 + c];
+            const double2 cfo = rk1 ? sW[slot(f, j, c)] : zero;
+            double2 R = w1 + t3 * cfo - a.temp4 * ik(Kf, cpj) - (fu2 * a.temp4 * RDY[j]) * (cpj - cpm);
+            R.x -= (f == 0 ? fzm : 0.0) * a.forcing;
+            R = R + a.temp5 * CF;
+            const double ep = isu2 ? E2P[j] : E1P[j], em = isu2 ? E2M[j] : E1M[j];
+            const double2 Gi = R + cn_c * (ep * (w2 - w1) - em * (w1 - w0));
+            const int knd = sK[f * NROW + j];
+            double2 G = inr ? Gi : zero;
             if (knd != 0) G = zero_mode ? make_double2(a.bcv[f * nyp + j], 0.0) : zero;
+            if (valid && inr && a.store_cf) a.cf[(size_t)f * fs + (size_t)j * ps + g0 + c] = CF;
             Gv[it] = G;
         }
         __syncthreads();             // every old CF has been read
@@ -790,7 +801,7 @@ size_t colpart_smem(const Dims& d) {
     const size_t NROW = (size_t)NPART * RC;
     const size_t NF2 = NROW * 2 > NPART * 16 ? NROW * 2 : NPART * 16;
     return (NROW * 2 * ((size_t)d.nf * 2 + 1) + NF2) * sizeof(double2) + NROW * RT_COUNT * sizeof(double) +
-           NROW * (size_t)d.nf;
+           (NROW * (size_t)d.nf + 7) / 8 * 8 + MAXF * 10 * sizeof(double);
 }
 
 template <typename TN>
