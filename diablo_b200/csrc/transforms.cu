@@ -275,7 +275,43 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
                     dst[1] = -v.y;
                 }
             }
-            if (p1 > p0) {
+            if (p0 == 0 && p1 == np && d.nth <= 1) {
+                // every product is in this batch (N_TH <= 1): one thread per kx
+                // extracts each product spectrum once and forms the 2 outputs of
+                // every field (field_sources)
+                for (int k = threadIdx.x; k < d.ldx; k += 256) {
+                    cpx<T>* yk = Y + (size_t)jp * xrow + (size_t)z * d.ldx + k;
+                    if (k > d.nkx) {
+                        for (int q = 0; q < 2 * nf; ++q) yk[(size_t)q * xf] = mk<T>(0, 0);
+                        continue;
+                    }
+                    const int km = k == 0 ? 0 : M - k;
+                    const cpx<T> w = twn[k];
+                    const T hs = T(0.5) * inv_nx;
+                    const int ok = lay.at(k, 0), om = lay.at(km, 0);
+                    const int rs = lay.at(0, 1) - lay.at(0, 0);
+                    auto X = [&](int p) -> cpx<T> {
+                        const int row = (nf + p - c0) * rs;
+                        const cpx<T> zk = buf[row + ok], zm = buf[row + om];
+                        const cpx<T> E = mk<T>(zk.x + zm.x, zk.y - zm.y);
+                        const cpx<T> O = mk<T>(zk.y + zm.y, zm.x - zk.x);
+                        return (E + cmul(w, O)) * hs;
+                    };
+                    const T K = (T)kxw[k];
+                    auto ikx = [&](cpx<T> v) { return mk<T>(-K * v.y, K * v.x); };
+                    const cpx<T> x0 = X(0);
+                    yk[0 * xf] = ikx(X(1)) + X(5);
+                    yk[1 * xf] = x0;
+                    yk[2 * xf] = ikx(X(3)) + X(7);
+                    yk[3 * xf] = X(4);
+                    yk[4 * xf] = ikx(x0) + X(6);
+                    yk[5 * xf] = X(2);
+                    if (nf > 3) {
+                        yk[6 * xf] = ikx(X(8)) + X(10);
+                        yk[7 * xf] = X(9);
+                    }
+                }
+            } else if (p1 > p0) {
                 // outputs of field f: 2f = ikx*Pa + Pflux, 2f+1 = Pz (field_sources);
                 // an output whose sources span two batches is completed by adding to
                 // what the earlier batch stored
