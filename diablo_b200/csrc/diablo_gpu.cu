@@ -280,7 +280,8 @@ int smem_limits(const Handle* h) {
     const int group = products_group(d.nx);
     const int m = d.nx / 2;
     const int rows = group < d.nf + d.np ? group : d.nf + d.np;
-    const size_t smem = sizeof(double) * (size_t)4 * d.nf * d.nx + 16 * (size_t)rows * (m + m / 16 + 1) + 16 * 3 * (size_t)m;
+    const size_t smem = sizeof(double) * (size_t)4 * d.nf * d.nx + 16 * (size_t)rows * (m + m / 16 + 1) + 16 * 3 * (size_t)m +
+                        16 * 2 * (size_t)d.nf * d.ldx + 16;
     if (group < 1 || smem > 227 * 1024) return fail(DIABLO_EINVAL, "NX too large for the number of fields");
     // the column kernel holds whole columns: NY+2 <= 528 rows
     if (part_rows(d.nyp) == 0) return fail(DIABLO_EINVAL, "NY too large (at most 526)");

@@ -32,6 +32,16 @@ __device__ __forceinline__ cpx<T> ld(const double2* p) {
     return mk<T>((T)v.x, (T)v.y);
 }
 
+// 16-byte asynchronous global -> shared copies (sm_80+ cp.async).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // Packed kz index m in [0,TNKZ] -> full z index in [0,NZ) (mpi.f:1530-1539).
 __device__ __forceinline__ int m_to_z(int m, int nkz, int nz, int nkzt) {
     return m <= nkz ? m : m + nz - nkzt;
@@ -179,7 +189,7 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
                                                      const double* __restrict__ kxw, FftPlan pm,
                                                      const cpx<T>* __restrict__ twm,
                                                      const cpx<T>* __restrict__ twn) {
-    extern __shared__ unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int M = MC > 0 ? MC : d.nx / 2;
     const int nx = 2 * M;
     const int nf = d.nf, np = d.np, nrow = nf + np;
@@ -190,6 +200,10 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
     cpx<T>* stw = reinterpret_cast<cpx<T>*>(ring + (size_t)RING * nf * nx);  // twiddles: M then NX
     cpx<T>* buf = stw + 3 * M;                                                // [group][pitch]
     T* tbuf = reinterpret_cast<T*>(buf);
+    // [2][nf][ldx] x spectra of the fields, the next plane's in flight
+    cpx<T>* xs = reinterpret_cast<cpx<T>*>(
+        (reinterpret_cast<uintptr_t>(buf + (size_t)min(group, nrow) * (lay.at(0, 1) - lay.at(0, 0))) + 15) &
+        ~(uintptr_t)15);                                                      // 16-byte aligned
     for (int e = threadIdx.x; e < 3 * M; e += 256) stw[e] = e < M ? twm[e] : twn[e - M];
     twm = stw;
     twn = stw + M;
@@ -201,8 +215,29 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
     const size_t xf = (size_t)d.nyp * xrow;              // field stride of X / Y
     const T inv_nx = T(1.0 / (double)nx);
     auto slot = [&](int j) { return (j - (jb - 1)) % RING; };
+    constexpr int CPC = 16 / (int)sizeof(cpx<T>);      // complex numbers per 16-byte copy
+    auto stage = [&](int Jn) {
+        cpx<T>* dst = xs + (size_t)(Jn & 1) * nf * d.ldx;
+        const int nch = d.ldx / CPC;
+        for (int e = threadIdx.x; e < nf * nch; e += 256) {
+            const int f = e / nch, q = e % nch;
+            cp_async16(dst + (size_t)f * d.ldx + q * CPC,
+                       X + (size_t)f * xf + (size_t)Jn * xrow + (size_t)z * d.ldx + q * CPC);
+        }
+        cp_async_commit();
+    };
+    stage(jb - 1);
     for (int J = jb - 1; J <= je + 2; ++J) {
         const bool do_inv = (J <= je + 1);
+        if (do_inv) {
+            if (J + 1 <= je + 1) {
+                stage(J + 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+        }
         const int jp = J - 2;                            // plane whose products are formed
         const bool do_prod = (jp >= jb);
         const int r0 = do_inv ? 0 : nf, r1 = do_prod ? nrow : nf;
@@ -219,7 +254,7 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
             const int nfill = max(0, min(nf, c0 + nr) - c0);        // inverse rows in this chunk
             for (int e = threadIdx.x; e < nfill * M; e += 256) {
                 const int r = e / M, k = e % M;
-                const cpx<T>* xr = X + (size_t)(c0 + r) * xf + (size_t)J * xrow + (size_t)z * d.ldx;
+                const cpx<T>* xr = xs + ((size_t)(J & 1) * nf + c0 + r) * d.ldx;
                 fill_real_inverse(buf, lay, r, xr, M, d.nkx, twn, k);
                 buf[lay.at(k, r)].y = -buf[lay.at(k, r)].y;
             }
@@ -360,15 +395,6 @@ __device__ __forceinline__ void field_products(int f, int* p, int* mlt) {
     p[1] = 2 * f + 1; mlt[1] = 2;
 }
 
-// 16-byte asynchronous global -> shared copies (sm_80+ cp.async).
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
-                 "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Block: kx tile of TX columns, field f, planes J0 .. J0+ZF_PLANES-1.  The
 // 2*ZF_PLANES product tiles it consumes stream through two shared buffers
@@ -520,7 +546,7 @@ cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int 
     const int M = d.nx / 2;
     const int rows = group < d.nf + d.np ? group : d.nf + d.np;
     const size_t smem = sizeof(T) * (size_t)RING * d.nf * d.nx + sizeof(cpx<T>) * (size_t)rows * row_pitch(M) +
-                        sizeof(cpx<T>) * 3 * (size_t)M;
+                        sizeof(cpx<T>) * 3 * (size_t)M + sizeof(cpx<T>) * 2 * (size_t)d.nf * d.ldx + 16;
     const int nchunks = (jhi - jlo + chunk) / chunk;
     dim3 grid(d.nz, nchunks);
     auto go = [&](auto kern) {
