@@ -325,15 +325,13 @@ cudaError_t launch_cn_part(const Dims& d, const CnArgs& a, double* tabs, double*
 // ---------------------------------------------------------------------------
 // The column kernel: NW warps (2*nf <= NW), RC rows per lane and system.
 // Shared memory, [slot][row][column] with NROW = 32*RC rows:
-//   sU  nf slots   old CU                          (A1-A2)
-//   sW  nf slots   old CF -> RHS G -> solution x   (A1-D)
+//   sU  nf slots   old CU (A1-A2), then RHS G -> solution x (B-D)
 //   sP  1 slot     old CP                          (A1-D)
-//   sF  1 slot     phi factors of the pair          (A1-C)
-//   phi itself (C-D) takes the old-CU slots of sU
-//   sR  [RT_COUNT][NROW] grid-metric row tables    (A1-D)
-//   sK  [nf][NROW] row kinds                       (A1-A2)
-// The nonlinear term is read straight from global memory, each thread
-// issuing the loads of all its rows before it uses any.
+//   sPh 1 slot     phi                             (C-D)
+//   sF  1 slot     phi factors of the pair         (A1-C)
+//   sK  [nf][NROW] row kinds, sC per-field coefficients
+// The nonlinear term and the old CF are read straight from global memory,
+// each thread issuing the loads of all its rows before it uses any.
 // ---------------------------------------------------------------------------
 template <int NW, int RC, typename TN>
 __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 1)
@@ -348,13 +346,12 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
     const int nf = d.nf, ny = d.ny, nyp = d.nyp;
     extern __shared__ __align__(16) unsigned char smem[];
     double2* sU = reinterpret_cast<double2*>(smem);
-    double2* sW = sU + (size_t)nf * NROW * 2;
-    double2* sP = sW + (size_t)nf * NROW * 2;
-    double2* sF = sP + NROW * 2;                    // phi factors of the pair (A1-C)
-    double2* sPh = sU;                              // phi (C-D), in the old-CU slots
-    double* sR = reinterpret_cast<double*>(sF + NF2);
-    signed char* sK = reinterpret_cast<signed char*>(sR + RT_COUNT * NROW);
-    double* sC = reinterpret_cast<double*>(sR + RT_COUNT * NROW) + (nf * NROW + 7) / 8;   // [MAXF][10]
+    double2* sW = sU;                               // RHS G -> solution x, over the old CU (B-D)
+    double2* sP = sU + (size_t)nf * NROW * 2;
+    double2* sPh = sP + NROW * 2;                   // phi (C-D)
+    double2* sF = sPh + NROW * 2;                   // phi factors of the pair (A1-C)
+    signed char* sK = reinterpret_cast<signed char*>(sF + NF2);
+    double* sC = reinterpret_cast<double*>(sF + NF2) + (nf * NROW + 7) / 8;   // [MAXF][10]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const size_t ps = d.splane();
     const size_t fs = ps * nyp;
@@ -374,21 +371,11 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
         };
         for (int f = 0; f < nf; ++f) {
             stream(a.cu + (size_t)f * fs + g0, sU + slot(f, 0, 0));
-            if (rk1) stream(a.cf + (size_t)f * fs + g0, sW + slot(f, 0, 0));
         }
         stream(a.cp + g0, sP);
         if (proj) {   // the pair's phi factors, 2 x 4 KB, contiguous per column pair
             const double2* src = reinterpret_cast<const double2*>(A.phitab + g0 * (NPART * 16));
             for (int e = tid; e < NPART * 16; e += NT) cp_async16(sF + e, src + e);
-        }
-        constexpr int NRT = (RT_COUNT * NROW + NT - 1) / NT;
-#pragma unroll
-        for (int q = 0; q < NRT; ++q) {
-            const int e = tid + q * NT;
-            if (e < RT_COUNT * NROW) {
-                const int t = e / NROW, j = e % NROW;
-                sR[e] = j < nyp ? A.rows[t * nyp + j] : 0.0;
-            }
         }
         for (int e = tid; e < nf * NROW; e += NT) {
             const int f = e / NROW, j = e % NROW;
@@ -422,14 +409,15 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
     const double KX0 = a.kx[kx0], KX1 = a.kx[kx0 + 1], KZm = a.kz[m0];
     const double k20 = A.k2[g0], k21 = A.k2[g0 + 1];
     const bool zm0 = (kx0 == 0 && m0 == 0);
-    const double* RDY = sR + RT_RDY * NROW;
-    const double* RDYF = sR + RT_RDYF * NROW;
-    const double* E1P = sR + RT_E1P * NROW;
-    const double* E1M = sR + RT_E1M * NROW;
-    const double* E2P = sR + RT_E2P * NROW;
-    const double* E2M = sR + RT_E2M * NROW;
-    const double* BY0 = sR + RT_BY0 * NROW;
-    const double* BY1 = sR + RT_BY1 * NROW;
+    // grid-metric row tables (small, shared by all blocks: read through L1)
+    const double* RDY = A.rows + RT_RDY * nyp;
+    const double* RDYF = A.rows + RT_RDYF * nyp;
+    const double* E1P = A.rows + RT_E1P * nyp;
+    const double* E1M = A.rows + RT_E1M * nyp;
+    const double* E2P = A.rows + RT_E2P * nyp;
+    const double* E2M = A.rows + RT_E2M * nyp;
+    const double* BY0 = A.rows + RT_BY0 * nyp;
+    const double* BY1 = A.rows + RT_BY1 * nyp;
 
     // ---- A2: right-hand sides, row-parallel; new CF out -------------------
     {
@@ -449,9 +437,14 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
         }
         const int c = tid & 1;
         TN nlv[NIT];
+        double2 cfv[NIT];
 #pragma unroll
-        for (int it = 0; it < NIT; ++it)
-            if (tid + it * NT < nitem) nlv[it] = nl[(size_t)ff[it] * fs + (size_t)jj[it] * ps + g0 + c];
+        for (int it = 0; it < NIT; ++it) {
+            const bool v = tid + it * NT < nitem;
+            const size_t o = (size_t)ff[it] * fs + (size_t)jj[it] * ps + g0 + c;
+            if (v) nlv[it] = nl[o];
+            cfv[it] = (v && rk1) ? a.cf[o] : zero;
+        }
         const bool zero_mode = zm0 && c == 0;
         const double KX = c ? KX1 : KX0;
         const double k2 = c ? k21 : k20;
@@ -487,7 +480,7 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
             const double2 CF = (-nuf * k2) * w1 + cpl + as_d2(nlv[it]);
             const double2 cpj = sP[j * 2 + c];
             const double2 cpm = wm * sP[jm * 2 + c];
-            const double2 cfo = rk1 ? sW[slot(f, j, c)] : zero;
+            const double2 cfo = cfv[it];
             double2 R = w1 + t3 * cfo - a.temp4 * ik(Kf, cpj) - (fu2 * a.temp4 * RDY[j]) * (cpj - cpm);
             R.x -= (f == 0 ? fzm : 0.0) * a.forcing;
             R = R + a.temp5 * CF;
@@ -499,7 +492,7 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
             if (valid && inr && a.store_cf) a.cf[(size_t)f * fs + (size_t)j * ps + g0 + c] = CF;
             Gv[it] = G;
         }
-        __syncthreads();             // every old CF has been read
+        __syncthreads();             // every old CU has been read
 #pragma unroll
         for (int it = 0; it < NIT; ++it)
             if (tid + it * NT < nitem) sW[slot(ff[it], jj[it], c)] = Gv[it];
@@ -800,8 +793,8 @@ size_t colpart_smem(const Dims& d) {
     const int RC = part_rows(d.nyp);
     const size_t NROW = (size_t)NPART * RC;
     const size_t NF2 = NROW * 2 > NPART * 16 ? NROW * 2 : NPART * 16;
-    return (NROW * 2 * ((size_t)d.nf * 2 + 1) + NF2) * sizeof(double2) + NROW * RT_COUNT * sizeof(double) +
-           (NROW * (size_t)d.nf + 7) / 8 * 8 + MAXF * 10 * sizeof(double);
+    return (NROW * 2 * ((size_t)d.nf + 2) + NF2) * sizeof(double2) + (NROW * (size_t)d.nf + 7) / 8 * 8 +
+           MAXF * 10 * sizeof(double);
 }
 
 template <typename TN>
