@@ -38,14 +38,14 @@ METRIC = "RK3 steps/s at 512×257×384: FP32-split vs FP64 on 1 B200, err vs FP6
 FALLBACK_HBM_GBS = 6650.0
 
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) per
-# y-plane of the grid, from one ncu capture of each kernel at 512x65x384
-# (67 planes); scaled to a grid by its number of planes, the kernels
-# streaming planes.  FP32-split build.
+# y-plane of the grid, from one ncu capture (one pass, nothing replayed) of
+# each kernel at 512x257x384, FP32-split; scaled to other grids by their
+# number of planes.
 TRAFFIC_PER_PLANE = {
-    "zinv": (193.98e6 + 98.83e6) / 67.0,
-    "products": (146.79e6 + 330.22e6) / 67.0,
-    "zfwd_nl": (423.00e6 + 85.44e6) / 67.0,
-    "column": (735.09e6 + 629.72e6) / 67.0,
+    "zinv": (749.9e6 + 513.2e6) / 259.0,
+    "products": (570.4e6 + 1052.9e6) / 259.0,
+    "zfwd_nl": (1114.4e6 + 360.0e6) / 259.0,
+    "column": (2257.0e6 + 1629.2e6) / 259.0,
 }
 
 
