@@ -33,7 +33,8 @@ EXPORTS = [
     "diablo_gpu_poisson_p_chan", "diablo_gpu_apply_bc_vel", "diablo_gpu_courant", "diablo_gpu_stats",
     "diablo_gpu_synchronize", "diablo_gpu_kernel_launches", "diablo_gpu_last_error",
     "diablo_gpu_get_stream", "diablo_gpu_set_profiling", "diablo_gpu_kernel_times",
-    "diablo_gpu_rem_div_chan_noalloc",
+    "diablo_gpu_rem_div_chan_noalloc", "diablo_gpu_autotune", "diablo_gpu_batch_create",
+    "diablo_gpu_batch_step", "diablo_gpu_batch_destroy",
 ]
 KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
 
@@ -77,6 +78,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_set_profiling.argtypes = [vp, ip]
     L.diablo_gpu_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), dp]
     L.diablo_gpu_rem_div_chan_noalloc.argtypes = [ctypes.POINTER(DiabloParams), dp, dp, vp, vp, vp, vp, vp]
+    L.diablo_gpu_autotune.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    L.diablo_gpu_batch_create.argtypes = [ctypes.POINTER(vp), dp, ip, ctypes.POINTER(vp)]
+    L.diablo_gpu_batch_step.argtypes = [vp, ip]
+    L.diablo_gpu_batch_destroy.argtypes = [vp]
     _lib = L
     return L
 
@@ -242,6 +247,13 @@ class Channel:
         _check(self.L.diablo_gpu_fft_xz_to_physical(self._h, _dp(vv.view(np.float64)), _dp(v), jmin, jmax),
                "diablo_gpu_fft_xz_to_physical")
 
+    def autotune(self) -> tuple[int, int]:
+        """Pick the products plane chunk and the z-forward planes per block by
+        timing this instance's grid; the state is left as it was."""
+        pc, zp = ctypes.c_int(), ctypes.c_int()
+        _check(self.L.diablo_gpu_autotune(self._h, ctypes.byref(pc), ctypes.byref(zp)), "diablo_gpu_autotune")
+        return pc.value, zp.value
+
     def kernel_launches(self) -> int:
         return int(self.L.diablo_gpu_kernel_launches(self._h))
 
@@ -275,3 +287,44 @@ class Channel:
         self.upload(cu, new_fourier(p), cth)
         self.apply_bc_vel()
         self.rem_div_chan()
+
+
+class Batch:
+    """Many channel instances advanced together: one CUDA graph holds a full
+    RK3 step of every instance (one stream branch each); step(n) launches it n
+    times.  Instances need a fixed time step; they stay usable on their own
+    (upload / download) between batch steps."""
+
+    def __init__(self, channels: list[Channel], delta_t: list[float] | None = None):
+        self.L = load_library()
+        self.channels = list(channels)
+        n = len(self.channels)
+        hs = (ctypes.c_void_p * n)(*[c._h.value for c in self.channels])
+        dts = np.ascontiguousarray([c.delta_t for c in self.channels] if delta_t is None else delta_t,
+                                   dtype=np.float64)
+        self._b = ctypes.c_void_p()
+        _check(self.L.diablo_gpu_batch_create(hs, _dp(dts), n, ctypes.byref(self._b)), "diablo_gpu_batch_create")
+        self._dts = dts
+
+    def step(self, n: int = 1) -> None:
+        _check(self.L.diablo_gpu_batch_step(self._b, int(n)), "diablo_gpu_batch_step")
+        for c, dt in zip(self.channels, self._dts):
+            c.time += n * float(dt)
+            c.time_step += n
+
+    def close(self) -> None:
+        if getattr(self, "_b", None) and self._b.value:
+            self.L.diablo_gpu_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

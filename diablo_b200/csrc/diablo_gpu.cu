@@ -69,6 +69,8 @@ struct Handle {
     int bc_type[2 * MAXF];
     double bc_c1[2 * MAXF];
     long long launches = 0;
+    // launch shapes (diablo_gpu_autotune): planes per products block chunk, planes per z-forward block
+    int prod_chunk = 32, zf_planes = 8;
     // optional per-kernel event timing
     bool profiling = false;
     struct Rec { int kind; cudaEvent_t a, b; };
@@ -299,10 +301,10 @@ int run_transforms(Handle* h) {
     { ProfScope ps(h, DIABLO_KERNEL_ZINV);
       CK(launch_zinv<T>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, twz, h->st)); }
     { ProfScope ps(h, DIABLO_KERNEL_PRODUCTS);
-      CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, 32, h->d_dy, h->d_dyf, h->d_kx, h->pm, twm, twn,
+      CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, h->prod_chunk, h->d_dy, h->d_dyf, h->d_kx, h->pm, twm, twn,
                             h->st)); }
     { ProfScope ps(h, DIABLO_KERNEL_ZFWD_NL);
-      CK(launch_zfwd_nl<T>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->d_kx, h->d_kz, h->pz, twz, h->st)); }
+      CK(launch_zfwd_nl<T>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->zf_planes, h->d_kx, h->d_kz, h->pz, twz, h->st)); }
     h->launches += 3;
     return DIABLO_OK;
 }
@@ -924,6 +926,173 @@ int diablo_gpu_kernel_times(void* handle, long long* launches, double* ms) {
         }
     }
     drop_records(h);
+    return DIABLO_OK;
+}
+
+int diablo_gpu_autotune(void* handle, int* prod_chunk, int* zf_planes) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    if (h->profiling) return fail(DIABLO_EINVAL, "autotune with profiling on");
+    const Dims& d = h->d;
+    const size_t sb = sizeof(double2) * h->s_field;
+    double2* save = nullptr;
+    CK(cudaStreamSynchronize(h->st));
+    cudaError_t e = cudaMalloc((void**)&save, sb * (2 * (size_t)d.nf + 1));
+    if (e != cudaSuccess) return fail(DIABLO_ENOMEM, "autotune: state copy allocation failed");
+    auto copy_state = [&](bool restore) -> cudaError_t {
+        const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+        cudaError_t r = restore ? cudaMemcpyAsync(h->cu, save, sb * d.nf, k, h->st)
+                                : cudaMemcpyAsync(save, h->cu, sb * d.nf, k, h->st);
+        if (r == cudaSuccess)
+            r = restore ? cudaMemcpyAsync(h->cf, save + h->s_field * d.nf, sb * d.nf, k, h->st)
+                        : cudaMemcpyAsync(save + h->s_field * d.nf, h->cf, sb * d.nf, k, h->st);
+        if (r == cudaSuccess)
+            r = restore ? cudaMemcpyAsync(h->cp, save + 2 * h->s_field * d.nf, sb, k, h->st)
+                        : cudaMemcpyAsync(save + 2 * h->s_field * d.nf, h->cp, sb, k, h->st);
+        return r;
+    };
+    cudaEvent_t ea = nullptr, eb = nullptr;
+    int rc = DIABLO_OK;
+    double dt = 1e-6;
+    double hb[3] = {dt * 8.0 / 15.0, dt * 2.0 / 15.0, dt * 5.0 / 15.0};
+    const double bb[3] = {1.0, 25.0 / 8.0, 9.0 / 4.0}, zb[3] = {0.0, -17.0 / 8.0, -5.0 / 4.0};
+    // time of one substage (rk_step 2) with the current shapes: best of 3
+    auto time_one = [&](float* best) -> int {
+        *best = 1e30f;
+        for (int rep = 0; rep < 4; ++rep) {
+            if ((e = copy_state(true)) != cudaSuccess) return fail(DIABLO_ECUDA, "autotune: restore");
+            cudaEventRecord(ea, h->st);
+            int r = diablo_gpu_rk_chan_1(h, 2, 1, 0.0, &dt, hb, bb, zb);
+            if (r) return r;
+            cudaEventRecord(eb, h->st);
+            if ((e = cudaEventSynchronize(eb)) != cudaSuccess) return fail(DIABLO_ECUDA, "autotune: sync");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ea, eb);
+            if (rep > 0 && ms < *best) *best = ms;     // the first run warms up
+        }
+        return DIABLO_OK;
+    };
+    e = cudaEventCreate(&ea);
+    if (e == cudaSuccess) e = cudaEventCreate(&eb);
+    if (e == cudaSuccess) e = copy_state(false);
+    if (e != cudaSuccess) rc = fail(DIABLO_ECUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    if (!rc) {
+        // coordinate search: products chunk, then z-forward planes per block
+        const int chunks[] = {8, 16, 32, 64}, planes[] = {4, 8, 16};
+        float best = 1e30f;
+        int bc = h->prod_chunk, bz = h->zf_planes;
+        for (int c : chunks) {
+            h->prod_chunk = c;
+            float t;
+            if ((rc = time_one(&t))) break;
+            if (t < best) { best = t; bc = c; }
+        }
+        h->prod_chunk = bc;
+        if (!rc) {
+            best = 1e30f;
+            for (int z : planes) {
+                h->zf_planes = z;
+                float t;
+                if ((rc = time_one(&t))) break;
+                if (t < best) { best = t; bz = z; }
+            }
+            h->zf_planes = bz;
+        }
+    }
+    if (!rc && (e = copy_state(true)) != cudaSuccess) rc = fail(DIABLO_ECUDA, "autotune: restore");
+    cudaStreamSynchronize(h->st);
+    if (ea) cudaEventDestroy(ea);
+    if (eb) cudaEventDestroy(eb);
+    cudaFree(save);
+    if (rc) return rc;
+    if (prod_chunk) *prod_chunk = h->prod_chunk;
+    if (zf_planes) *zf_planes = h->zf_planes;
+    return DIABLO_OK;
+}
+
+}  // extern "C"
+
+namespace {
+struct Batch {
+    std::vector<Handle*> hs;
+    cudaStream_t origin = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+void free_batch(Batch* b) {
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (cudaEvent_t ev : b->join) if (ev) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->origin) cudaStreamDestroy(b->origin);
+    delete b;
+}
+}  // namespace
+
+extern "C" {
+
+int diablo_gpu_batch_create(void* const* handles, const double* delta_t, int n, void** batch) {
+    if (!handles || !delta_t || !batch || n < 1) return fail(DIABLO_EINVAL, "bad batch arguments");
+    *batch = nullptr;
+    for (int i = 0; i < n; ++i) {
+        Handle* h = (Handle*)handles[i];
+        if (!h) return fail(DIABLO_EINVAL, "null handle in batch");
+        if (h->p.variable_dt) return fail(DIABLO_ENOTSUP, "batched instances need a fixed time step (variable_dt = 0)");
+        if (h->p.f_type == 2) return fail(DIABLO_ENOTSUP, "batched instances cannot have time-dependent forcing");
+        if (h->profiling) return fail(DIABLO_EINVAL, "batched instance with profiling on");
+        if (!(delta_t[i] > 0.0)) return fail(DIABLO_EINVAL, "batched instance with delta_t <= 0");
+    }
+    Batch* b = new Batch();
+    auto bail = [&](int code, const std::string& msg) { free_batch(b); return fail(code, msg); };
+    for (int i = 0; i < n; ++i) b->hs.push_back((Handle*)handles[i]);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    b->join.assign(n, nullptr);
+    for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+    for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaStreamSynchronize(b->hs[i]->st);
+    if (e != cudaSuccess) return bail(DIABLO_ECUDA, std::string("batch set-up: ") + cudaGetErrorString(e));
+    e = cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return bail(DIABLO_ECUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+    int rc = DIABLO_OK;
+    if ((e = cudaEventRecord(b->fork, b->origin)) != cudaSuccess) rc = DIABLO_ECUDA;
+    for (int i = 0; i < n && !rc; ++i)
+        if ((e = cudaStreamWaitEvent(b->hs[i]->st, b->fork, 0)) != cudaSuccess) rc = DIABLO_ECUDA;
+    const double bb[3] = {1.0, 25.0 / 8.0, 9.0 / 4.0}, zb[3] = {0.0, -17.0 / 8.0, -5.0 / 4.0};
+    for (int i = 0; i < n && !rc; ++i) {
+        double dt = delta_t[i];
+        double hb[3] = {dt * 8.0 / 15.0, dt * 2.0 / 15.0, dt * 5.0 / 15.0};
+        for (int rk = 1; rk <= 3 && !rc; ++rk) rc = diablo_gpu_rk_chan_1(b->hs[i], rk, 1, 0.0, &dt, hb, bb, zb);
+        if (!rc && (e = cudaEventRecord(b->join[i], b->hs[i]->st)) != cudaSuccess) rc = DIABLO_ECUDA;
+        if (!rc && (e = cudaStreamWaitEvent(b->origin, b->join[i], 0)) != cudaSuccess) rc = DIABLO_ECUDA;
+    }
+    const std::string msg = rc ? g_err : std::string();
+    cudaError_t ee = cudaStreamEndCapture(b->origin, &b->graph);
+    if (rc) return bail(rc == DIABLO_ECUDA && msg.empty() ? DIABLO_ECUDA : rc,
+                        msg.empty() ? std::string("batch capture: ") + cudaGetErrorString(e) : msg);
+    if (ee != cudaSuccess) return bail(DIABLO_ECUDA, std::string("batch end capture: ") + cudaGetErrorString(ee));
+    e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    if (e != cudaSuccess) return bail(DIABLO_ECUDA, std::string("batch instantiate: ") + cudaGetErrorString(e));
+    *batch = b;
+    return DIABLO_OK;
+}
+
+int diablo_gpu_batch_step(void* batch, int nsteps) {
+    Batch* b = (Batch*)batch;
+    if (!b || nsteps < 0) return fail(DIABLO_EINVAL, "bad batch arguments");
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(b->exec, b->origin));
+    CK(cudaStreamSynchronize(b->origin));
+    return DIABLO_OK;
+}
+
+int diablo_gpu_batch_destroy(void* batch) {
+    Batch* b = (Batch*)batch;
+    if (!b) return fail(DIABLO_EINVAL, "null batch");
+    cudaStreamSynchronize(b->origin);
+    free_batch(b);
     return DIABLO_OK;
 }
 

@@ -27,11 +27,12 @@ cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int 
                             const double* dy, const double* dyf, const double* kx, const FftPlan& pm,
                             const void* twm, const void* twn, cudaStream_t st);
 
-// Per plane: forward z transform of the 2 product outputs of every field,
+// Per plane (zp planes per block, 0 = default): forward z transform of the 2
+// product outputs of every field,
 // kz packing and 1/NZ (mpi.f:1526-1540), then NL = -(first) - ikz (second)
 // -> NL (type T, S layout).
 template <typename T>
-cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int jhi,
+cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int jhi, int zp,
                            const double* kx, const double* kz, const FftPlan& pz, const void* twz,
                            cudaStream_t st);
 

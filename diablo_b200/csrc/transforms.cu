@@ -396,15 +396,16 @@ __device__ __forceinline__ void field_products(int f, int* p, int* mlt) {
 }
 
 
-// Block: kx tile of TX columns, field f, planes J0 .. J0+ZF_PLANES-1.  The
-// 2*ZF_PLANES product tiles it consumes stream through two shared buffers
+// Block: kx tile of TX columns, field f, planes J0 .. J0+zp-1 (zp, the planes
+// per block, is a launch parameter).  The 2*zp product tiles it consumes
+// stream through two shared buffers
 // (cp.async), the next tile in flight while the current one is transformed.
-constexpr int ZF_PLANES = 8;
+constexpr int ZF_PLANES = 8;   // default planes per block
 constexpr int ZF_TX = 8;
 
 template <typename T, int NC, int TX>
 __global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __restrict__ Y,
-                                                    cpx<T>* __restrict__ NL, int jlo, int jhi,
+                                                    cpx<T>* __restrict__ NL, int jlo, int jhi, int zp,
                                                     const double* __restrict__ kxw,
                                                     const double* __restrict__ kzw, FftPlan pz,
                                                     const cpx<T>* __restrict__ twz) {
@@ -416,8 +417,8 @@ __global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __rest
     cpx<T>* sacc = bufs + 2 * (size_t)nz * TX;                    // run-time path: [nkzt][TX]
     const int kx0 = blockIdx.x * TX;
     const int f = blockIdx.z;
-    const int J0 = jlo + blockIdx.y * ZF_PLANES;
-    const int nplanes = min(ZF_PLANES, jhi - J0 + 1);
+    const int J0 = jlo + blockIdx.y * zp;
+    const int nplanes = min(zp, jhi - J0 + 1);
     const size_t xrow = (size_t)nz * d.ldx;
     const size_t xf = (size_t)d.nyp * xrow;
     const T inv_nz = T(1.0 / (double)nz);
@@ -564,16 +565,18 @@ cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int 
 }
 
 template <typename T>
-cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int jhi,
+cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int jhi, int zp,
                            const double* kx, const double* kz, const FftPlan& pz, const void* twz,
                            cudaStream_t st) {
     constexpr int TX = ZF_TX;
     if (jhi < jlo) return cudaSuccess;
-    dim3 grid(d.ldx / TX, (jhi - jlo + ZF_PLANES) / ZF_PLANES, d.nf);
+    if (zp < 1) zp = ZF_PLANES;
+    dim3 grid(d.ldx / TX, (jhi - jlo + zp) / zp, d.nf);
     auto go = [&](auto kern, bool ct) {
         const size_t smem = sizeof(cpx<T>) * (2 * (size_t)d.nz * TX + (ct ? 0 : (size_t)d.nkzt * TX));
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, 256, smem, st>>>(d, (const cpx<T>*)Y, (cpx<T>*)NL, jlo, jhi, kx, kz, pz, (const cpx<T>*)twz);
+        kern<<<grid, 256, smem, st>>>(d, (const cpx<T>*)Y, (cpx<T>*)NL, jlo, jhi, zp, kx, kz, pz,
+                                      (const cpx<T>*)twz);
     };
     switch (d.nz) {
 #define CASE(N) case N: go(k_zfwd_nl<T, N, TX>, true); break;
@@ -770,9 +773,9 @@ template cudaError_t launch_products<float>(const Dims&, const void*, void*, int
 template cudaError_t launch_products<double>(const Dims&, const void*, void*, int, int, int, const double*,
                                              const double*, const double*, const FftPlan&, const void*, const void*,
                                              cudaStream_t);
-template cudaError_t launch_zfwd_nl<float>(const Dims&, const void*, void*, int, int, const double*,
+template cudaError_t launch_zfwd_nl<float>(const Dims&, const void*, void*, int, int, int, const double*,
                                            const double*, const FftPlan&, const void*, cudaStream_t);
-template cudaError_t launch_zfwd_nl<double>(const Dims&, const void*, void*, int, int, const double*,
+template cudaError_t launch_zfwd_nl<double>(const Dims&, const void*, void*, int, int, int, const double*,
                                             const double*, const FftPlan&, const void*, cudaStream_t);
 
 }  // namespace dgpu

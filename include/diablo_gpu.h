@@ -197,6 +197,30 @@ int diablo_gpu_rem_div_chan_noalloc(const diablo_params* p, const double* dy, co
                                     double* cu1, double* cu2, double* cu3, double* phi,
                                     void* stream);
 
+/* Launch shapes chosen by timing (no counterpart in the reference, which
+ * has no GPU code): planes per block of the products and z-forward kernels.
+ * Runs a few RK substages of the instance's own grid with each candidate and
+ * restores the state afterwards; the result of a step does not depend on the
+ * choice (the same arithmetic, only grouped differently).  prod_chunk and
+ * zf_planes receive the chosen values (either may be NULL).  Allocates a
+ * temporary copy of the state. */
+int diablo_gpu_autotune(void* handle, int* prod_chunk, int* zf_planes);
+
+/* Batched instances (configuration of many independent channels of uneven
+ * sizes; the reference's ensemble driver, dummy_code/ensem_dummy.f, is an
+ * empty stub).  diablo_gpu_batch_create captures one full RK3 step (the three
+ * RK_CHAN_1 substages) of every handle into one CUDA graph, one stream branch
+ * per instance, with the fixed time step delta_t[i] of instance i; each
+ * diablo_gpu_batch_step then advances every instance by nsteps steps, one
+ * graph launch per step.  Every instance must have variable_dt = 0 and no
+ * time-dependent forcing (f_type != 2), else DIABLO_ENOTSUP.  The handles
+ * stay owned by the caller and must outlive the batch; while the batch
+ * exists, calls on its handles other than upload/download/synchronize are
+ * not allowed to overlap a batch step. */
+int diablo_gpu_batch_create(void* const* handles, const double* delta_t, int n, void** batch);
+int diablo_gpu_batch_step(void* batch, int nsteps);
+int diablo_gpu_batch_destroy(void* batch);
+
 /* Wait for all work queued on the handle's stream. */
 int diablo_gpu_synchronize(void* handle);
 /* Sum over the last launches of the handle: number of kernels launched by
