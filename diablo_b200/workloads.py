@@ -9,6 +9,11 @@ Seeded synthetic fields stand in for any dataset (the reference ships none):
                    Lx=4pi, Lz=4pi/3, tanh-stretched y (CS=1.75) on [-1,1],
                    no-slip walls, constant pressure gradient, passive scalar
                    Pr=0.71, CFL-adaptive dt.
+* ``batched``   -- many independent shear layers of uneven sizes: NX from
+                   {64,96,128}, NY from {65,129}, NZ from {32,64,128}, Ri
+                   uniform in [0.05,0.3], Re uniform in [500,3000] (nu=1/Re),
+                   Pr=1, the ``kh`` domain and BCs, per-instance seeds,
+                   FP32-split, dt=0.01 fixed.
 * ``precision`` -- the benchmark grid 512x257x384: tanh-stretched y (CS=1.75)
                    on [-1,1]; the shear layer of ``kh`` rescaled to
                    thickness delta=0.1 (U1 = TH = tanh(y/delta), noise
@@ -69,3 +74,21 @@ def precision(nx: int = 512, ny: int = 257, nz: int = 384, prec: int = P.PREC_FP
     return Workload("precision", p, g, 1.0e-3, "shear", dict(seed=seed, amp=1e-3, delta=delta),
                     dict(nu=p.nu, ri=p.ri[0], pr=p.pr[0], lx=p.lx, lz=p.lz, delta=delta,
                          y="tanh CS=1.75 [-1,1]", dt=1.0e-3))
+
+
+def batched(n: int = 64, seed: int = 2024, prec: int = P.PREC_FP32SPLIT) -> list[Workload]:
+    """n shear-layer instances with sizes, Ri and Re drawn from a seeded
+    generator (the instance list is a pure function of n and seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nx = int(rng.choice([64, 96, 128]))
+        ny = int(rng.choice([65, 129]))
+        nz = int(rng.choice([32, 64, 128]))
+        w = kh(nx, ny, nz, precision=prec, seed=seed + 1 + i)
+        w.p.ri[0] = float(rng.uniform(0.05, 0.3))
+        w.p.nu = 1.0 / float(rng.uniform(500.0, 3000.0))
+        w.name = "batched"
+        w.meta.update(nu=w.p.nu, ri=w.p.ri[0], grid=(nx, ny, nz))
+        out.append(w)
+    return out
