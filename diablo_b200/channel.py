@@ -34,7 +34,7 @@ EXPORTS = [
     "diablo_gpu_synchronize", "diablo_gpu_kernel_launches", "diablo_gpu_last_error",
     "diablo_gpu_get_stream", "diablo_gpu_set_profiling", "diablo_gpu_kernel_times",
     "diablo_gpu_rem_div_chan_noalloc", "diablo_gpu_autotune", "diablo_gpu_batch_create",
-    "diablo_gpu_batch_step", "diablo_gpu_batch_destroy",
+    "diablo_gpu_batch_step", "diablo_gpu_batch_destroy", "diablo_gpu_filter_chan",
 ]
 KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
 
@@ -82,6 +82,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_batch_create.argtypes = [ctypes.POINTER(vp), dp, ip, ctypes.POINTER(vp)]
     L.diablo_gpu_batch_step.argtypes = [vp, ip]
     L.diablo_gpu_batch_destroy.argtypes = [vp]
+    L.diablo_gpu_filter_chan.argtypes = [vp, ip]
     _lib = L
     return L
 
@@ -246,6 +247,9 @@ class Channel:
         assert v.shape[-3:] == physical_shape(self.p) and vv.shape[-3:] == fourier_shape(self.p)
         _check(self.L.diablo_gpu_fft_xz_to_physical(self._h, _dp(vv.view(np.float64)), _dp(v), jmin, jmax),
                "diablo_gpu_fft_xz_to_physical")
+
+    def filter_chan(self, n: int = 1) -> None:
+        _check(self.L.diablo_gpu_filter_chan(self._h, n), "diablo_gpu_filter_chan")
 
     def autotune(self) -> tuple[int, int]:
         """Pick the products plane chunk and the z-forward planes per block by

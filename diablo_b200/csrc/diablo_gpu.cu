@@ -885,6 +885,18 @@ int diablo_gpu_stats(void* handle, double* profiles) {
     return DIABLO_OK;
 }
 
+int diablo_gpu_filter_chan(void* handle, int n) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    if (n < 1 || n > h->d.nth) return fail(DIABLO_EINVAL, "scalar index outside 1..N_TH");
+    { ProfScope ps(h, DIABLO_KERNEL_OTHER);
+      CK(launch_filter_chan(h->d, h->cu + (size_t)(3 + n - 1) * h->s_field, h->d_kx, h->d_kz, h->p.lx, h->p.lz,
+                            (double)(float)h->p.nx, (double)(float)h->p.nz, h->st)); }
+    h->launches += 1;
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
+}
+
 int diablo_gpu_synchronize(void* handle) {
     Handle* h = (Handle*)handle;
     if (!h) return fail(DIABLO_EINVAL, "null handle");

@@ -84,6 +84,10 @@ cudaError_t launch_poisson_column(const PoissonArgs& a, cudaStream_t st);
 cudaError_t launch_stats_planes(const Dims& d, const double* u1, const double* u2, const double* u3,
                                 const double* th, const double* me, const double* dy, const double* dyf, double* out,
                                 cudaStream_t st);
+// filter_chan (filter.f:1-98) on one scalar field of the S layout; fnx, fnz
+// are NX and NZ as the reference's FLOAT() gives them.
+cudaError_t launch_filter_chan(const Dims& d, double2* cth, const double* kx, const double* kz, double lx,
+                               double lz, double fnx, double fnz, cudaStream_t st);
 // rows transformed together by the products kernel for a given NX
 int products_group(int nx);
 // Record the one-line message returned by diablo_gpu_last_error; returns code.

@@ -197,6 +197,14 @@ int diablo_gpu_rem_div_chan_noalloc(const diablo_params* p, const double* dy, co
                                     double* cu1, double* cu2, double* cu3, double* phi,
                                     void* stream);
 
+/* filter_chan(n) (for/filter.f:1-98) on the device scalar n (1..N_TH): the
+ * sharpened raised-cosine filter in kx,kz on rows J = 0..NY and, for
+ * I >= 1, K >= 1, the vertical compact filter with alpha = 0 (an explicit
+ * 5-point stencil on J = 2..NY-1).  Row J = 0 keeps its horizontally
+ * filtered value, where the reference copies an element of its work array
+ * that it never sets. */
+int diablo_gpu_filter_chan(void* handle, int n);
+
 /* Launch shapes chosen by timing (no counterpart in the reference, which
  * has no GPU code): planes per block of the products and z-forward kernels.
  * Runs a few RK substages of the instance's own grid with each candidate and

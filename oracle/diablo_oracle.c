@@ -1325,3 +1325,39 @@ void orc_stats(orc_state* s, double* out) {
     }
     for (int c = 0; c < 3; ++c) free(u[c]);
 }
+
+/* ------------------------------------------------------------------------ */
+/* filter_chan(n) (filter.f:1-98) on scalar n (1..N_TH): a sharpened raised   */
+/* cosine in the horizontal on every mode and rows J = 0..NY, then, for       */
+/* I = 1..NKX and K = 1..TNKZ, the vertical compact filter with alpha = 0,    */
+/* i.e. the explicit stencil of VEC_C on rows J = 2..NY-1 (rows 1 and NY keep  */
+/* their values; the identity tridiagonal system returns VEC_C).  Row J = 0    */
+/* keeps its horizontally filtered value: the reference copies an element of  */
+/* VEC_C that it never sets there.                                            */
+/* ------------------------------------------------------------------------ */
+void orc_filter_chan(orc_state* s, int n) {
+    if (n < 1 || n > s->NTH) return;
+    const int NY = s->NY, NKX = s->NKX, TNKZ = s->TNKZ;
+    double* C = s->CTH + (size_t)(n - 1) * s->nreal;
+    const double alpha = 0.0;
+    const double f_a = (1.0 / 8.0) * (5.0 + 6.0 * alpha), f_b = 0.5 * (1.0 + 2.0 * alpha),
+                 f_c = (-1.0 / 8.0) * (1.0 - 2.0 * alpha);
+    for (int k = 0; k <= TNKZ; ++k)
+        for (int i = 0; i <= NKX; ++i) {
+            const double a1 = s->KX[i] * s->p.lx * 1.0 / (double)(float)s->NX;
+            const double a2 = s->KZ[k] * s->p.lz * 1.0 / (double)(float)s->NZ;
+            const double sigma0 = 0.5 * (1.0 + cos(sqrt(pow(a1, 2.0) + pow(a2, 2.0))));
+            const double sigma = pow(sigma0, 4.0) * (35.0 - 84.0 * sigma0 + 70.0 * pow(sigma0, 2.0) -
+                                                     20.0 * pow(sigma0, 3.0));
+            for (int j = 0; j <= NY; ++j) CX(C, i, k, j) = CX(C, i, k, j) * sigma;
+        }
+    cplx* vec = (cplx*)malloc(sizeof(cplx) * (size_t)(NY + 2));
+    for (int k = 1; k <= TNKZ; ++k)
+        for (int i = 1; i <= NKX; ++i) {
+            for (int j = 2; j <= NY - 1; ++j)
+                vec[j] = f_a * CX(C, i, k, j) + (f_b / 2.0) * (CX(C, i, k, j + 1) + CX(C, i, k, j - 1)) +
+                         (f_c / 2.0) * (CX(C, i, k, j + 2) + CX(C, i, k, j - 2));
+            for (int j = 2; j <= NY - 1; ++j) CX(C, i, k, j) = vec[j];
+        }
+    free(vec);
+}

@@ -70,6 +70,8 @@ void orc_apply_bc_scalar(orc_state* s);
 /* One time step of diablo.f:66-111 without I/O: three RK_CHAN_1 substages,
  * then TIME += DELTA_T and TIME_STEP += 1. */
 void orc_step(orc_state* s);
+/* filter_chan(n) of filter.f on scalar n (1..N_TH). */
+void orc_filter_chan(orc_state* s, int n);
 /* Statistics of SAVE_STATS_CHAN (DIABLO_STAT_* profiles, NY+2 each). */
 void orc_stats(orc_state* s, double* profiles);
 /* Plain complex DFT of length n (interleaved), sign -1 or +1, unnormalised;

@@ -51,6 +51,7 @@ def lib() -> ctypes.CDLL:
         L.orc_get_time.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_int), dp]
         L.orc_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, ip]
         L.orc_set_threads.argtypes = [ip]
+        L.orc_filter_chan.argtypes = [vp, ip]
         for name in ("orc_fft_xz_to_fourier", "orc_fft_xz_to_physical"):
             getattr(L, name).argtypes = [vp, dp, dp, ip, ip]
         L.orc_rk_chan_1.argtypes = [vp, ip]
@@ -179,6 +180,9 @@ class Oracle:
 
     def apply_bc_vel(self) -> None:
         lib().orc_apply_bc_vel(self._h)
+
+    def filter_chan(self, n: int = 1) -> None:
+        lib().orc_filter_chan(self._h, n)
 
     def stats(self) -> np.ndarray:
         out = np.zeros((17, self.p.ny + 2))
