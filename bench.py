@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--error-steps", type=int, default=500,
+                    help="steps after which FP32-split is compared with FP64 (besides 100)")
     return ap.parse_args()
 
 
@@ -195,6 +197,32 @@ def rel_errors(p, a, b):
     return out
 
 
+def profile_errors(p, a, b):
+    """Mean-profile errors (the (0,0) modes of U1 and TH, SAVE_STATS_CHAN's
+    ume/thme) relative to the profile's norm."""
+    out = {}
+    for name, x, y in (("ume", a["cu"][0], b["cu"][0]), ("thme", a["cth"][0], b["cth"][0])):
+        px, py = x[:, 0, 0].real, y[:, 0, 0].real
+        out[f"mean_profile_{name}"] = float(np.linalg.norm(px - py) / max(np.linalg.norm(py), 1e-300))
+    return out
+
+
+def divergence_norm(p, g, s):
+    """Discrete divergence of the downloaded velocity on J = 2..NY-1 (the rows
+    REM_DIV_CHAN makes divergence-free), relative L2 against the velocity
+    norm: ikx CU1 + (CU2(j+1)-CU2(j))/DYF(j) + ikz CU3."""
+    from diablo_b200.layout import dealiased
+    nkx, nkz = p.nx // 3, p.nz // 3
+    kx = np.arange(nkx + 1) * 2 * np.pi / p.lx
+    kz = np.concatenate([np.arange(nkz + 1), -np.arange(nkz, 0, -1)]) * 2 * np.pi / p.lz
+    u1, u2, u3 = (dealiased(p, s["cu"][c]) for c in range(3))
+    j = np.arange(2, p.ny)
+    div = (1j * kx[None, None, :] * u1[j] + (u2[j + 1] - u2[j]) / np.asarray(g.dyf)[j][:, None, None]
+           + 1j * kz[None, :, None] * u3[j])
+    scale = np.sqrt(sum(np.linalg.norm(x[j]) ** 2 for x in (u1, u2, u3)))
+    return float(np.linalg.norm(div) / scale)
+
+
 def e2e_rate(c, steps, torch):
     """Steps/s through the C ABI with pinned host buffers in the Fortran
     layout: every step uploads CU1..3, CP, CTH, runs the three substages and
@@ -314,14 +342,24 @@ def run_ours(args, rank, world, local_rank):
         c64, _, _ = make_channel(w, PREC_FP64, u, th)
         c64.step(args.warmup)
         ms64 = timed_steps(c64, args.steps, torch)
-        s32 = c32.download()
-        # re-run FP32-split from the same start for exactly the same steps
+        c64.close()
+        # error of FP32-split against the all-FP64 path from the same start,
+        # after 100 and args.error_steps time steps
+        c64, _, _ = make_channel(w, PREC_FP64, u, th)
         c32b, _, _ = make_channel(w, PREC_FP32SPLIT, u, th)
-        c32b.step(args.warmup + args.steps)
-        errs = rel_errors(w.p, c32b.download(), c64.download())
-        fp64 = {"steps_per_s": args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
-                "err_fp32split_vs_fp64_after_steps": args.warmup + args.steps, "err": errs}
-        del s32
+        errs = {}
+        done = 0
+        for n in sorted({100, args.error_steps}):
+            c64.step(n - done)
+            c32b.step(n - done)
+            done = n
+            a32, a64 = c32b.download(), c64.download()
+            e = rel_errors(w.p, a32, a64)
+            e.update(profile_errors(w.p, a32, a64))
+            e["divergence_fp32split"] = divergence_norm(w.p, w.grid, a32)
+            e["divergence_fp64"] = divergence_norm(w.p, w.grid, a64)
+            errs[f"after_{n}_steps"] = e
+        fp64 = {"steps_per_s": args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps, "err": errs}
         c64.close()
         c32b.close()
 
