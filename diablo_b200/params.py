@@ -47,6 +47,7 @@ class DiabloParams(ctypes.Structure):
         ("ri", ctypes.c_double * MAX_TH), ("pr", ctypes.c_double * MAX_TH),
         ("drhodx", ctypes.c_double * MAX_TH), ("drhodz", ctypes.c_double * MAX_TH),
         ("precision", ctypes.c_int),
+        ("les_model_type", ctypes.c_int),
     ]
 
     def copy(self) -> "DiabloParams":
@@ -191,7 +192,7 @@ def read_input_chan_dat(text: str, p: DiabloParams, ctl: RunControl) -> None:
     if time_ad_meth != 1:
         raise ValueError("RK_CHAN_2 is not supported (for/channel.f:1076-1100)")
     r.skip()
-    r.read()  # LES_MODEL_TYPE
+    p.les_model_type = int(_num(r.read()[0]))
     r.skip()
     t = r.read()
     ctl.ic_type, ctl.kick = int(_num(t[0])), _num(t[1])
@@ -238,7 +239,12 @@ def validate(p: DiabloParams) -> None:
     if not (0 <= p.n_th <= MAX_TH):
         raise ValueError(f"N_TH must be in 0..{MAX_TH}")
     if p.les:
-        raise ValueError("the LES branch is not provided")
+        if p.les_model_type != 1:
+            # les.f:269-272 stops for the dynamic models
+            raise ValueError("LES_MODEL_TYPE must be 1 (constant Smagorinsky)")
+        if p.v_bc_ymin == 2 or p.v_bc_ymax == 2:
+            # APPLY_BC_VEL_PHYS stops for V_BC = 2 (channel.f:2554, 2656)
+            raise ValueError("LES needs V_BC_YMIN, V_BC_YMAX in 0, 1")
 
 
 def kelvin_helmholtz(nx: int = 64, ny: int = 65, nz: int = 64, precision: int = PREC_FP64) -> DiabloParams:

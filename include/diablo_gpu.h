@@ -59,7 +59,7 @@ typedef struct diablo_params {
     double nu_v_scale;
     int variable_dt, update_dt;
     double cfl;
-    int les;                       /* must be 0: the LES branch is not built */
+    int les;                       /* LES flag of input.dat */
     int create_new_flow;
     /* input_chan.dat */
     double i_ro;
@@ -76,6 +76,9 @@ typedef struct diablo_params {
     double drhodx[DIABLO_MAX_TH], drhodz[DIABLO_MAX_TH];
     /* library options */
     int precision;                 /* DIABLO_PREC_* */
+    /* input_chan.dat LES_MODEL_TYPE (for/channel.f:1477); only 1, the
+     * constant-Smagorinsky model, is run (for/les.f:269-272 stops for 2, 3) */
+    int les_model_type;
 } diablo_params;
 
 /* Create a channel instance on the current CUDA device.

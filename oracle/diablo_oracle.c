@@ -115,6 +115,10 @@ struct orc_state {
     double *U1, *U2, *U3, *P, *R1, *R2, *R3, *F1, *F2, *F3, *S1;
     /* not equivalenced (header:256-258) */
     double *TH, *CTH, *FTH, *CFTH, *RTH, *CRTH;
+    /* LES (allocated when p.les): NU_T at GY points, which also serves as
+     * KAPPA_T (channel.f:314-322 copies it for every scalar); Sij<->CSij and
+     * TEMP<->CTEMP share one buffer each as header_les:31-37 equivalences them */
+    double *NU_T, *SIJ[6], *TEMP;
     fftplan px_plan, pz_plan;
 };
 
@@ -199,6 +203,11 @@ orc_state* orc_create(const diablo_params* p, const double* gy, const double* gy
     s->CFTH = (double*)calloc(s->nreal * nth, sizeof(double));
     s->RTH = (double*)calloc(s->nreal * nth, sizeof(double));
     s->CRTH = (double*)calloc(s->nreal * nth, sizeof(double));
+    if (p->les) {
+        s->NU_T = (double*)calloc(s->nreal, sizeof(double));
+        s->TEMP = (double*)calloc(s->nreal, sizeof(double));
+        for (int q = 0; q < 6; ++q) s->SIJ[q] = (double*)calloc(s->nreal, sizeof(double));
+    }
     return s;
 }
 
@@ -206,7 +215,9 @@ void orc_destroy(orc_state* s) {
     if (!s) return;
     double* bufs[] = {s->GY, s->GYF, s->DY, s->DYF, s->KX, s->KX2, s->KZ, s->KZ2,
                       s->U1, s->U2, s->U3, s->P, s->R1, s->R2, s->R3, s->F1, s->F2,
-                      s->F3, s->S1, s->TH, s->CTH, s->FTH, s->CFTH, s->RTH, s->CRTH};
+                      s->F3, s->S1, s->TH, s->CTH, s->FTH, s->CFTH, s->RTH, s->CRTH,
+                      s->NU_T, s->TEMP, s->SIJ[0], s->SIJ[1], s->SIJ[2], s->SIJ[3], s->SIJ[4],
+                      s->SIJ[5]};
     for (size_t q = 0; q < sizeof(bufs) / sizeof(bufs[0]); ++q) free(bufs[q]);
     plan_free(&s->px_plan);
     plan_free(&s->pz_plan);
@@ -227,6 +238,7 @@ double* orc_array(orc_state* s, int which) {
         case ORC_GYF: return s->GYF; case ORC_DY: return s->DY;
         case ORC_DYF: return s->DYF; case ORC_KX: return s->KX;
         case ORC_KZ: return s->KZ;
+        case ORC_NU_T: return s->NU_T;
     }
     return NULL;
 }
@@ -237,6 +249,7 @@ size_t orc_array_doubles(orc_state* s, int which) {
     if (which <= ORC_DYF) return (size_t)s->NY + 2;
     if (which == ORC_KX) return (size_t)s->NXP + 1;
     if (which == ORC_KZ) return (size_t)s->TNKZ + 1;
+    if (which == ORC_NU_T) return s->NU_T ? s->nreal : 0;
     return 0;
 }
 
@@ -526,8 +539,10 @@ static int serial_k(orc_state* s) {
 
 typedef enum { SOLVE_TH, SOLVE_U2, SOLVE_U1, SOLVE_U3 } solve_kind;
 
-/* One implicit CN solve over all (x,z) columns (channel.f:762-1029). */
-static void cn_solve(orc_state* s, solve_kind kind, int n, double TEMP1) {
+/* One implicit CN solve over all (x,z) columns (channel.f:762-1029), with the
+ * eddy viscosity / diffusivity rows of the LES build (channel.f:793-805,
+ * 862-874, 927-939, 991-1003) when p.les. */
+static void cn_solve(orc_state* s, solve_kind kind, int n, double TEMP1, double TEMP2) {
     const int NX = s->NX, NY = s->NY, NZP = s->NZP;
     const size_t msz = (size_t)NX * (NY + 2);
     double* field = kind == SOLVE_TH ? s->TH + (size_t)n * s->nreal
@@ -556,6 +571,15 @@ static void cn_solve(orc_state* s, solve_kind kind, int n, double TEMP1) {
                         MR(U, i, j) = -c / (s->DY[j + 1] * s->DYF[j]);
                         MR(V, i, j) = PH(rhs, i, k, j);
                     }
+                if (s->p.les)
+                    for (int j = jlo; j <= jhi; ++j)
+                        for (int i = 0; i <= s->NXM; ++i) {
+                            const double kj = PH(s->NU_T, i, k, j), kp = PH(s->NU_T, i, k, j + 1);
+                            MR(L, i, j) = MR(L, i, j) - TEMP2 * kj / (s->DY[j] * s->DYF[j]);
+                            MR(D, i, j) = MR(D, i, j) + TEMP2 * kp / (s->DY[j + 1] * s->DYF[j]) +
+                                          TEMP2 * kj / (s->DY[j] * s->DYF[j]);
+                            MR(U, i, j) = MR(U, i, j) - TEMP2 * kp / (s->DY[j + 1] * s->DYF[j]);
+                        }
                 bc_th(s, L, D, U, V, n);
                 jc0 = jlo - 1; jc1 = jhi + 1;
             } else if (kind == SOLVE_U2) {
@@ -567,6 +591,16 @@ static void cn_solve(orc_state* s, solve_kind kind, int n, double TEMP1) {
                         MR(U, i, j) = -TEMP1 * nuv / (s->DYF[j] * s->DY[j]);
                         MR(V, i, j) = PH(rhs, i, k, j);
                     }
+                if (s->p.les)
+                    for (int j = 2; j <= NY; ++j)
+                        for (int i = 0; i <= s->NXM; ++i) {
+                            const double nm = PH(s->NU_T, i, k, j) + PH(s->NU_T, i, k, j - 1);
+                            const double np = PH(s->NU_T, i, k, j) + PH(s->NU_T, i, k, j + 1);
+                            MR(L, i, j) = MR(L, i, j) - TEMP2 * 0.5 * nm / (s->DYF[j - 1] * s->DY[j]);
+                            MR(D, i, j) = MR(D, i, j) + TEMP2 * 0.5 * np / (s->DYF[j] * s->DY[j]) +
+                                          TEMP2 * 0.5 * nm / (s->DYF[j - 1] * s->DY[j]);
+                            MR(U, i, j) = MR(U, i, j) - TEMP2 * 0.5 * np / (s->DYF[j] * s->DY[j]);
+                        }
                 bc_u2(s, L, D, U, V);
                 jc0 = 1; jc1 = NY + 1;
             } else {
@@ -579,6 +613,15 @@ static void cn_solve(orc_state* s, solve_kind kind, int n, double TEMP1) {
                         MR(U, i, j) = -TEMP1 * nuv / (s->DY[j + 1] * s->DYF[j]);
                         MR(V, i, j) = PH(rhs, i, k, j);
                     }
+                if (s->p.les)
+                    for (int j = jlo; j <= jhi; ++j)
+                        for (int i = 0; i <= s->NXM; ++i) {
+                            const double nj = PH(s->NU_T, i, k, j), nq = PH(s->NU_T, i, k, j + 1);
+                            MR(L, i, j) = MR(L, i, j) - TEMP2 * nj / (s->DY[j] * s->DYF[j]);
+                            MR(D, i, j) = MR(D, i, j) + TEMP2 * nq / (s->DY[j + 1] * s->DYF[j]) +
+                                          TEMP2 * nj / (s->DY[j] * s->DYF[j]);
+                            MR(U, i, j) = MR(U, i, j) - TEMP2 * nq / (s->DY[j + 1] * s->DYF[j]);
+                        }
                 if (kind == SOLVE_U1)
                     bc_u13(s, L, D, U, V, s->p.u_bc_ymin, s->p.u_bc_ymin_c1, s->p.u_bc_ymax,
                            s->p.u_bc_ymax_c1);
@@ -597,7 +640,270 @@ static void cn_solve(orc_state* s, solve_kind kind, int n, double TEMP1) {
 #undef MR
 
 /* ------------------------------------------------------------------------ */
-/* RK_CHAN_1 (channel.f:62-1073), non-LES branch.                             */
+/* LES, constant-Smagorinsky model (LES_MODEL_TYPE = 1).                      */
+/* ------------------------------------------------------------------------ */
+
+/* APPLY_BC_LES (les.f:805-865): Neumann walls copy the last interior row of
+ * CU1 / CU3 into the ghost rows (the upper wall rewrites row NY too). */
+static void apply_bc_les(orc_state* s) {
+    const int NY = s->NY, NXP = s->NXP, TNKZ = s->TNKZ;
+    const diablo_params* p = &s->p;
+    double* CU[2] = {s->U1, s->U3};
+    const int top[2] = {p->u_bc_ymax, p->w_bc_ymax}, bot[2] = {p->u_bc_ymin, p->w_bc_ymin};
+    for (int c = 0; c < 2; ++c) {
+        double* C = CU[c];
+        if (top[c] == 1)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i) {
+                    CX(C, i, k, NY) = CX(C, i, k, NY - 1);
+                    CX(C, i, k, NY + 1) = CX(C, i, k, NY);
+                }
+    }
+    for (int c = 0; c < 2; ++c) {
+        double* C = CU[c];
+        if (bot[c] == 1)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i) {
+                    CX(C, i, k, 1) = CX(C, i, k, 2);
+                    CX(C, i, k, 0) = CX(C, i, k, 1);
+                }
+    }
+}
+
+/* APPLY_BC_VEL_PHYS_LOWER / _UPPER (channel.f:2495-2660) on U1..U3 in
+ * physical space.  V_BC = 2 stops the reference there, so it never gets here. */
+static void apply_bc_vel_phys(orc_state* s) {
+    const int NY = s->NY, NZP = s->NZP, NXM = s->NXM;
+    const diablo_params* p = &s->p;
+    const double* DY = s->DY;
+    const double* DYF = s->DYF;
+    double *U1 = s->U1, *U2 = s->U2, *U3 = s->U3;
+    for (int k = 0; k <= NZP - 1; ++k)
+        for (int i = 0; i <= NXM; ++i) {
+            /* lower wall */
+            if (p->u_bc_ymin == 0) {
+                PH(U1, i, k, 0) = p->u_bc_ymin_c1; PH(U1, i, k, 1) = p->u_bc_ymin_c1;
+            } else {
+                PH(U1, i, k, 1) = PH(U1, i, k, 2) - DY[2] * p->u_bc_ymin_c1;
+                PH(U1, i, k, 0) = PH(U1, i, k, 1) - DY[1] * p->u_bc_ymin_c1;
+            }
+            if (p->w_bc_ymin == 0) {
+                PH(U3, i, k, 0) = p->w_bc_ymin_c1; PH(U3, i, k, 1) = p->w_bc_ymin_c1;
+            } else {
+                PH(U3, i, k, 1) = PH(U3, i, k, 2) - DY[2] * p->w_bc_ymin_c1;
+                PH(U3, i, k, 0) = PH(U3, i, k, 1) - DY[1] * p->w_bc_ymin_c1;
+            }
+            if (p->v_bc_ymin == 0) {
+                PH(U2, i, k, 1) = 2.0 * p->v_bc_ymin_c1 - PH(U2, i, k, 2);
+                PH(U2, i, k, 0) = PH(U2, i, k, 1);
+            } else {
+                PH(U2, i, k, 1) = PH(U2, i, k, 2) - DYF[1] * p->v_bc_ymin_c1;
+                PH(U2, i, k, 0) = PH(U2, i, k, 1) - DYF[1] * p->v_bc_ymin_c1;
+            }
+            /* upper wall */
+            if (p->u_bc_ymax == 0) {
+                PH(U1, i, k, NY) = p->u_bc_ymax_c1; PH(U1, i, k, NY + 1) = p->u_bc_ymax_c1;
+            } else {
+                PH(U1, i, k, NY) = PH(U1, i, k, NY - 1) + DY[NY] * p->u_bc_ymax_c1;
+                PH(U1, i, k, NY + 1) = PH(U1, i, k, NY) + DY[NY] * p->u_bc_ymax_c1;
+            }
+            if (p->w_bc_ymax == 0) {
+                PH(U3, i, k, NY) = p->w_bc_ymax_c1; PH(U3, i, k, NY + 1) = p->w_bc_ymax_c1;
+            } else {
+                PH(U3, i, k, NY) = PH(U3, i, k, NY - 1) + DY[NY] * p->w_bc_ymax_c1;
+                PH(U3, i, k, NY + 1) = PH(U3, i, k, NY) + DY[NY] * p->w_bc_ymax_c1;
+            }
+            if (p->v_bc_ymax == 0)
+                PH(U2, i, k, NY + 1) = 2.0 * p->v_bc_ymax_c1 - PH(U2, i, k, NY);
+            else
+                PH(U2, i, k, NY + 1) = PH(U2, i, k, NY) + DY[NY] * p->v_bc_ymax_c1;
+        }
+}
+
+/* Filter widths with -2 C_s^2 absorbed, C_s = 0.13, beta_sgs = 1
+ * (les.f:196-217): at GYF (dyf = DYF) or GY (dyf = DY) points. */
+static double smag_width(orc_state* s, double dyj) {
+    const double C_SMAG = 0.13, beta_sgs = 1.0;
+    return -2.0 * (C_SMAG * C_SMAG) * pow(s->DX * beta_sgs * dyj * 2.0 * s->DZ * beta_sgs, 2.0 / 3.0);
+}
+
+/* les_chan (les.f:1-267, 280-336), LES_MODEL_TYPE = 1, NPROCY = NPROCZ = 1.
+ * On exit U1..U3 are in physical space, NU_T is set and CF1..CF3 hold the
+ * subgrid-stress divergence and the explicit cross terms. */
+static void les_chan(orc_state* s) {
+    const int NY = s->NY, NXP = s->NXP, TNKZ = s->TNKZ, NZP = s->NZP, NXM = s->NXM;
+    const int JSTART = s->JSTART, JEND = s->JEND;
+    const double* DY = s->DY;
+    const double* DYF = s->DYF;
+    double *CU1 = s->U1, *CU2 = s->U2, *CU3 = s->U3;
+    double *U1 = s->U1, *U3 = s->U3;
+    double *CF1 = s->F1, *CF2 = s->F2, *CF3 = s->F3;
+    double *S1 = s->S1, *TEMP = s->TEMP, *NU_T = s->NU_T;
+    double *Sij1 = s->SIJ[0], *Sij2 = s->SIJ[1], *Sij3 = s->SIJ[2];
+    double *Sij4 = s->SIJ[3], *Sij5 = s->SIJ[4], *Sij6 = s->SIJ[5];
+    const cplx CI = I;
+    /* ghost cells (les.f:64-77): APPLY_BC_VEL_MPI, then APPLY_BC_LES */
+    orc_apply_bc_vel(s);
+    apply_bc_les(s);
+    /* compute_strain_chan (les.f:526-569) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 1; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(Sij1, i, k, j) = CI * s->KX[i] * CX(CU1, i, k, j);
+                CX(Sij2, i, k, j) = (CX(CU2, i, k, j + 1) - CX(CU2, i, k, j)) / DYF[j];
+                CX(Sij3, i, k, j) = CI * s->KZ[k] * CX(CU3, i, k, j);
+                CX(Sij5, i, k, j) = 0.5 * (CI * s->KZ[k] * CX(CU1, i, k, j) + CI * s->KX[i] * CX(CU3, i, k, j));
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 1; j <= NY + 1; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(Sij4, i, k, j) =
+                    0.5 * ((CX(CU1, i, k, j) - CX(CU1, i, k, j - 1)) / DY[j] + CI * s->KX[i] * CX(CU2, i, k, j));
+                CX(Sij6, i, k, j) =
+                    0.5 * (CI * s->KZ[k] * CX(CU2, i, k, j) + (CX(CU3, i, k, j) - CX(CU3, i, k, j - 1)) / DY[j]);
+            }
+    for (int q = 0; q < 6; ++q) orc_fft_xz_to_physical(s, s->SIJ[q], s->SIJ[q], 0, NY + 1);
+    /* mean profiles (les.f:87-92) */
+    double* U1_bar = (double*)malloc(sizeof(double) * (NY + 2));
+    double* U3_bar = (double*)malloc(sizeof(double) * (NY + 2));
+    for (int j = 0; j <= NY + 1; ++j) {
+        U1_bar[j] = creal(CX(CU1, 0, 0, j));
+        U3_bar[j] = creal(CX(CU3, 0, 0, j));
+    }
+    orc_fft_xz_to_physical(s, CU1, U1, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CU2, s->U2, 0, NY + 1);
+    orc_fft_xz_to_physical(s, CU3, U3, 0, NY + 1);
+    /* |S| at GYF points with the mean shear removed (les.f:113-137) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = JSTART; j <= JEND; ++j)
+        for (int k = 0; k <= NZP - 1; ++k)
+            for (int i = 0; i <= NXM; ++i) {
+                const double a4 = 0.5 * (PH(Sij4, i, k, j + 1) + PH(Sij4, i, k, j) -
+                                         0.5 * (U1_bar[j] - U1_bar[j - 1]) / DY[j] -
+                                         0.5 * (U1_bar[j + 1] - U1_bar[j]) / DY[j + 1]);
+                const double a6 = 0.5 * (PH(Sij6, i, k, j + 1) + PH(Sij6, i, k, j) -
+                                         0.5 * (U3_bar[j] - U3_bar[j - 1]) / DY[j] -
+                                         0.5 * (U3_bar[j + 1] - U3_bar[j]) / DY[j + 1]);
+                const double s1 = PH(Sij1, i, k, j), s2 = PH(Sij2, i, k, j), s3 = PH(Sij3, i, k, j);
+                const double s5 = PH(Sij5, i, k, j);
+                PH(S1, i, k, j) = sqrt(2.0 * (s1 * s1) + 4.0 * (a4 * a4) + 4.0 * (s5 * s5) + 2.0 * (s2 * s2) +
+                                       4.0 * (a6 * a6) + 2.0 * (s3 * s3));
+            }
+    /* |S| at GY points (les.f:140-160) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY + 1; ++j)
+        for (int k = 0; k <= NZP - 1; ++k)
+            for (int i = 0; i <= NXM; ++i) {
+                const double g1 = (PH(Sij1, i, k, j) * DYF[j - 1] + PH(Sij1, i, k, j - 1) * DYF[j]) / (2.0 * DY[j]);
+                const double g5 = (PH(Sij5, i, k, j) * DYF[j - 1] + PH(Sij5, i, k, j - 1) * DYF[j]) / (2.0 * DY[j]);
+                const double g2 = (PH(Sij2, i, k, j) * DYF[j - 1] + PH(Sij2, i, k, j - 1) * DYF[j]) / (2.0 * DY[j]);
+                const double g3 = (PH(Sij3, i, k, j) * DYF[j - 1] + PH(Sij3, i, k, j - 1) * DYF[j]) / (2.0 * DY[j]);
+                const double b4 = PH(Sij4, i, k, j) - 0.5 * (U1_bar[j] - U1_bar[j - 1]) / DY[j];
+                const double b6 = PH(Sij6, i, k, j) - 0.5 * (U3_bar[j] - U3_bar[j - 1]) / DY[j];
+                PH(TEMP, i, k, j) = sqrt(2.0 * (g1 * g1) + 4.0 * (b4 * b4) + 4.0 * (g5 * g5) + 2.0 * (g2 * g2) +
+                                         4.0 * (b6 * b6) + 2.0 * (g3 * g3));
+            }
+    free(U1_bar);
+    free(U3_bar);
+    /* |S| S_ij: GYF components (les.f:165-177), Sij2 left to the implicit
+     * eddy viscosity; GY components without the implicit dU/dy part
+     * (les.f:181-194) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = JSTART; j <= JEND; ++j)
+        for (int k = 0; k <= NZP - 1; ++k)
+            for (int i = 0; i <= NXM; ++i) {
+                PH(Sij1, i, k, j) = PH(S1, i, k, j) * PH(Sij1, i, k, j);
+                PH(Sij5, i, k, j) = PH(S1, i, k, j) * PH(Sij5, i, k, j);
+                PH(Sij2, i, k, j) = 0.0;
+                PH(Sij3, i, k, j) = PH(S1, i, k, j) * PH(Sij3, i, k, j);
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY + 1; ++j)
+        for (int k = 0; k <= NZP - 1; ++k)
+            for (int i = 0; i <= NXM; ++i) {
+                PH(Sij4, i, k, j) = PH(TEMP, i, k, j) * (PH(Sij4, i, k, j) - 0.5 * (PH(U1, i, k, j) - PH(U1, i, k, j - 1)) / DY[j]);
+                PH(Sij6, i, k, j) = PH(TEMP, i, k, j) * (PH(Sij6, i, k, j) - 0.5 * (PH(U3, i, k, j) - PH(U3, i, k, j - 1)) / DY[j]);
+            }
+    double* DELTA_YF = (double*)calloc(NY + 2, sizeof(double));
+    double* DELTA_Y = (double*)calloc(NY + 2, sizeof(double));
+    for (int j = 1; j <= NY + 1; ++j) {
+        DELTA_YF[j] = smag_width(s, DYF[j]);
+        DELTA_Y[j] = smag_width(s, DY[j]);
+    }
+    /* NU_T = C_s^2 Delta^2 |S| at GY points (les.f:219-227); GHOST_LES_MPI
+     * zeroes rows 1, 2, NY and NY+1 (mpi.f:494-507) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= NZP - 1; ++k)
+            for (int i = 0; i <= NXM; ++i) PH(NU_T, i, k, j) = -0.5 * DELTA_Y[j] * PH(TEMP, i, k, j);
+    for (int k = 0; k <= NZP - 1; ++k)
+        for (int i = 0; i <= NXM; ++i) {
+            PH(NU_T, i, k, 1) = 0.0; PH(NU_T, i, k, 2) = 0.0;
+            PH(NU_T, i, k, NY) = 0.0; PH(NU_T, i, k, NY + 1) = 0.0;
+        }
+    /* tau_ij in Fourier space (les.f:235-262) */
+    orc_fft_xz_to_fourier(s, Sij1, Sij1, 0, NY + 1);
+    orc_fft_xz_to_fourier(s, Sij3, Sij3, 0, NY + 1);
+    orc_fft_xz_to_fourier(s, Sij4, Sij4, 0, NY + 1);
+    orc_fft_xz_to_fourier(s, Sij5, Sij5, 0, NY + 1);
+    orc_fft_xz_to_fourier(s, Sij6, Sij6, 0, NY + 1);
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 1; j <= NY + 1; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(Sij1, i, k, j) = DELTA_YF[j] * CX(Sij1, i, k, j);
+                CX(Sij5, i, k, j) = DELTA_YF[j] * CX(Sij5, i, k, j);
+                CX(Sij3, i, k, j) = DELTA_YF[j] * CX(Sij3, i, k, j);
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY + 1; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(Sij4, i, k, j) = DELTA_Y[j] * CX(Sij4, i, k, j);
+                CX(Sij6, i, k, j) = DELTA_Y[j] * CX(Sij6, i, k, j);
+            }
+    free(DELTA_YF);
+    free(DELTA_Y);
+    /* CF_i -= d tau_ij / dx_j (les.f:280-304); J1 = JSTART, J2 = NY-1 on the
+     * rank at the upper wall, which NPROCY = 1 makes the only one (les.f:46-59) */
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = JSTART; j <= NY - 1; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                CX(CF1, i, k, j) = CX(CF1, i, k, j) - CI * s->KX[i] * CX(Sij1, i, k, j) -
+                                   (CX(Sij4, i, k, j + 1) - CX(Sij4, i, k, j)) / DYF[j] -
+                                   CI * s->KZ[k] * CX(Sij5, i, k, j);
+                CX(CF3, i, k, j) = CX(CF3, i, k, j) - CI * s->KX[i] * CX(Sij5, i, k, j) -
+                                   (CX(Sij6, i, k, j + 1) - CX(Sij6, i, k, j)) / DYF[j] -
+                                   CI * s->KZ[k] * CX(Sij3, i, k, j);
+            }
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i)
+                CX(CF2, i, k, j) = CX(CF2, i, k, j) - CI * s->KX[i] * CX(Sij4, i, k, j) -
+                                   CI * s->KZ[k] * CX(Sij6, i, k, j);
+    /* explicit cross terms (les.f:307-336) */
+    for (int c = 0; c < 2; ++c) {
+        const double* U = c == 0 ? U1 : U3;
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = 2; j <= NY; ++j)
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i)
+                    PH(TEMP, i, k, j) = PH(NU_T, i, k, j) * (PH(U, i, k, j) - PH(U, i, k, j - 1)) / DY[j];
+        orc_fft_xz_to_fourier(s, TEMP, TEMP, 2, NY);
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = 2; j <= NY; ++j)
+            for (int k = 0; k <= TNKZ; ++k)
+                for (int i = 0; i <= NXP - 1; ++i)
+                    CX(CF2, i, k, j) = CX(CF2, i, k, j) + CI * (c == 0 ? s->KX[i] : s->KZ[k]) * CX(TEMP, i, k, j);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* RK_CHAN_1 (channel.f:62-1073).                                             */
 /* ------------------------------------------------------------------------ */
 void orc_rk_chan_1(orc_state* s, int rk_step) {
     const int NY = s->NY, NXP = s->NXP, TNKZ = s->TNKZ, NZP = s->NZP, NXM = s->NXM;
@@ -610,7 +916,6 @@ void orc_rk_chan_1(orc_state* s, int rk_step) {
     const double TEMP3 = s->ZETA_BAR[r] * s->H_BAR[r];
     const double TEMP4 = s->H_BAR[r];
     const double TEMP5 = s->BETA_BAR[r] * s->H_BAR[r];
-    (void)TEMP2;
     double *CU1 = s->U1, *CU2 = s->U2, *CU3 = s->U3, *CP = s->P;
     double *CR1 = s->R1, *CR2 = s->R2, *CR3 = s->R3;
     double *CF1 = s->F1, *CF2 = s->F2, *CF3 = s->F3, *CS1 = s->S1;
@@ -750,10 +1055,42 @@ void orc_rk_chan_1(orc_state* s, int rk_step) {
                                          CX(CU3, i, k, j) * p->drhodz[n];
     }
     /* USER_RHS_CHAN_FOURIER: empty hook (user_rhs.f:77-121). */
-    /* non-LES branch: transforms to physical space (channel.f:389-399) */
-    orc_fft_xz_to_physical(s, CU1, U1, 0, NY + 1);
-    orc_fft_xz_to_physical(s, CU2, U2, 0, NY + 1);
-    orc_fft_xz_to_physical(s, CU3, U3, 0, NY + 1);
+    if (p->les && (!p->create_new_flow || s->TIME_STEP > 100)) {
+        /* LES branch (channel.f:303-384): subgrid stress into CF, U to
+         * physical space, physical BCs re-applied, then the explicit
+         * horizontal eddy diffusivity of every scalar with KAPPA_T = NU_T */
+        les_chan(s);
+        apply_bc_vel_phys(s);
+        for (int n = 0; n < s->NTH; ++n) {
+            const double* CTHn = s->CTH + (size_t)n * s->nreal;
+            double* CFTHn = s->CFTH + (size_t)n * s->nreal;
+            for (int c = 0; c < 2; ++c) {
+#pragma omp parallel for num_threads(nthreads())
+                for (int j = 1; j <= NY + 1; ++j)
+                    for (int k = 0; k <= TNKZ; ++k)
+                        for (int i = 0; i <= NXP - 1; ++i)
+                            CX(CS1, i, k, j) = CI * (c == 0 ? s->KX[i] : s->KZ[k]) * CX(CTHn, i, k, j);
+                orc_fft_xz_to_physical(s, CS1, S1, 0, NY + 1);
+#pragma omp parallel for num_threads(nthreads())
+                for (int j = 1; j <= NY + 1; ++j)
+                    for (int k = 0; k <= NZP - 1; ++k)
+                        for (int i = 0; i <= NXM; ++i) PH(S1, i, k, j) = PH(s->NU_T, i, k, j) * PH(S1, i, k, j);
+                orc_fft_xz_to_fourier(s, S1, CS1, 0, NY + 1);
+#pragma omp parallel for num_threads(nthreads())
+                for (int j = s->JSTART_TH[n]; j <= s->JEND_TH[n]; ++j)
+                    for (int k = 0; k <= TNKZ; ++k)
+                        for (int i = 0; i <= NXP - 1; ++i)
+                            CX(CFTHn, i, k, j) =
+                                CX(CFTHn, i, k, j) + CI * (c == 0 ? s->KX[i] : s->KZ[k]) * CX(CS1, i, k, j);
+            }
+        }
+    } else {
+        /* non-LES branch: transforms to physical space (channel.f:389-391) */
+        orc_fft_xz_to_physical(s, CU1, U1, 0, NY + 1);
+        orc_fft_xz_to_physical(s, CU2, U2, 0, NY + 1);
+        orc_fft_xz_to_physical(s, CU3, U3, 0, NY + 1);
+    }
+    /* scalars to physical space (channel.f:380-384, 394-398) */
     for (int n = 0; n < s->NTH; ++n) {
         memcpy(CS1, s->CTH + (size_t)n * s->nreal, sizeof(double) * s->nreal);
         orc_fft_xz_to_physical(s, CS1, S1, 0, NY + 1);
@@ -853,6 +1190,31 @@ void orc_rk_chan_1(orc_state* s, int rk_step) {
                 PH(R2, i, k, j) = PH(R2, i, k, j) + TEMP1 * nuv *
                     (((PH(U2, i, k, j + 1) - PH(U2, i, k, j)) / DYF[j] -
                       (PH(U2, i, k, j) - PH(U2, i, k, j - 1)) / DYF[j - 1]) / DY[j]);
+    if (p->les) {
+        /* eddy-viscosity part of the explicit CN half, NU_T at GY points
+         * (channel.f:631-660) */
+        const double* NU_T = s->NU_T;
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = JSTART; j <= JEND; ++j)
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i) {
+                    PH(R1, i, k, j) = PH(R1, i, k, j) + TEMP2 *
+                        ((PH(NU_T, i, k, j + 1) * (PH(U1, i, k, j + 1) - PH(U1, i, k, j)) / DY[j + 1] -
+                          PH(NU_T, i, k, j) * (PH(U1, i, k, j) - PH(U1, i, k, j - 1)) / DY[j]) / DYF[j]);
+                    PH(R3, i, k, j) = PH(R3, i, k, j) + TEMP2 *
+                        ((PH(NU_T, i, k, j + 1) * (PH(U3, i, k, j + 1) - PH(U3, i, k, j)) / DY[j + 1] -
+                          PH(NU_T, i, k, j) * (PH(U3, i, k, j) - PH(U3, i, k, j - 1)) / DY[j]) / DYF[j]);
+                }
+#pragma omp parallel for num_threads(nthreads())
+        for (int j = 2; j <= NY; ++j)
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i)
+                    PH(R2, i, k, j) = PH(R2, i, k, j) + TEMP2 *
+                        ((0.5 * (PH(NU_T, i, k, j) + PH(NU_T, i, k, j + 1)) * (PH(U2, i, k, j + 1) - PH(U2, i, k, j)) /
+                              DYF[j] -
+                          0.5 * (PH(NU_T, i, k, j) + PH(NU_T, i, k, j - 1)) * (PH(U2, i, k, j) - PH(U2, i, k, j - 1)) /
+                              DYF[j - 1]) / DY[j]);
+    }
 
     /* scalars (channel.f:666-840) */
     for (int n = 0; n < s->NTH; ++n) {
@@ -882,14 +1244,25 @@ void orc_rk_chan_1(orc_state* s, int rk_step) {
                     PH(RTHn, i, k, j) = PH(RTHn, i, k, j) + c *
                         (((PH(THn, i, k, j + 1) - PH(THn, i, k, j)) / DY[j + 1] -
                           (PH(THn, i, k, j) - PH(THn, i, k, j - 1)) / DY[j]) / DYF[j]);
-        cn_solve(s, SOLVE_TH, n, TEMP1);
+        if (p->les) {
+            /* eddy diffusivity KAPPA_T = NU_T (channel.f:748-760) */
+            const double* K = s->NU_T;
+#pragma omp parallel for num_threads(nthreads())
+            for (int j = j0; j <= j1; ++j)
+                for (int k = 0; k <= NZP - 1; ++k)
+                    for (int i = 0; i <= NXM; ++i)
+                        PH(RTHn, i, k, j) = PH(RTHn, i, k, j) + TEMP2 *
+                            ((PH(K, i, k, j + 1) * (PH(THn, i, k, j + 1) - PH(THn, i, k, j)) / DY[j + 1] -
+                              PH(K, i, k, j) * (PH(THn, i, k, j) - PH(THn, i, k, j - 1)) / DY[j]) / DYF[j]);
+        }
+        cn_solve(s, SOLVE_TH, n, TEMP1, TEMP2);
     }
 #undef PRODUCT
 #undef ACCUM
     /* velocity solves: U2, U1, U3 (channel.f:842-1029) */
-    cn_solve(s, SOLVE_U2, 0, TEMP1);
-    cn_solve(s, SOLVE_U1, 0, TEMP1);
-    cn_solve(s, SOLVE_U3, 0, TEMP1);
+    cn_solve(s, SOLVE_U2, 0, TEMP1, TEMP2);
+    cn_solve(s, SOLVE_U1, 0, TEMP1, TEMP2);
+    cn_solve(s, SOLVE_U3, 0, TEMP1, TEMP2);
     /* CFL (channel.f:1037-1040) */
     if (p->variable_dt && rk_step == 3 && (s->TIME_STEP % p->update_dt) == 0) orc_courant(s);
     /* back to Fourier space (channel.f:1043-1050) */

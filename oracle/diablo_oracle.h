@@ -40,6 +40,7 @@ enum {
     ORC_F1, ORC_F2, ORC_F3, ORC_S1,
     ORC_TH, ORC_CTH, ORC_FTH, ORC_CFTH, ORC_RTH, ORC_CRTH,
     ORC_GY, ORC_GYF, ORC_DY, ORC_DYF, ORC_KX, ORC_KZ,
+    ORC_NU_T,
     ORC_NARRAYS
 };
 

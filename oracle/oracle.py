@@ -21,7 +21,7 @@ _LIB = os.path.join(_HERE, "liboracle.so")
 
 (ORC_U1, ORC_U2, ORC_U3, ORC_P, ORC_R1, ORC_R2, ORC_R3, ORC_F1, ORC_F2, ORC_F3, ORC_S1,
  ORC_TH, ORC_CTH, ORC_FTH, ORC_CFTH, ORC_RTH, ORC_CRTH,
- ORC_GY, ORC_GYF, ORC_DY, ORC_DYF, ORC_KX, ORC_KZ) = range(23)
+ ORC_GY, ORC_GYF, ORC_DY, ORC_DYF, ORC_KX, ORC_KZ, ORC_NU_T) = range(24)
 
 
 def build() -> str:
@@ -137,6 +137,13 @@ class Oracle:
     @property
     def cfth(self) -> np.ndarray:
         return self.fourier(ORC_CFTH)[: self.p.n_th]
+
+    @property
+    def nu_t(self) -> np.ndarray:
+        """NU_T(0:NX-1, 0:NZ-1, 0:NY+1) at GY points, as [J][K][I] (LES only)."""
+        if not self.p.les:
+            raise ValueError("NU_T exists only when LES is set")
+        return self.physical(ORC_NU_T, 0)[:, : self.p.nz, : self.p.nx]
 
     @property
     def phi(self) -> np.ndarray:

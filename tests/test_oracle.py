@@ -120,6 +120,7 @@ def test_input_file_parsers_on_reference_kh_files():
     assert p.f_type == 3 and p.px0 == -1.0
     assert (p.u_bc_ymin, p.v_bc_ymin, p.w_bc_ymin, p.u_bc_ymax, p.v_bc_ymax, p.w_bc_ymax) == (1, 0, 1, 1, 0, 1)
     assert p.th_bc_ymin[0] == 1 and p.th_bc_ymax[0] == 1
+    assert p.les_model_type == 1
     P.validate(p)
 
 
