@@ -34,7 +34,7 @@ EXPORTS = [
     "diablo_gpu_synchronize", "diablo_gpu_kernel_launches", "diablo_gpu_last_error",
     "diablo_gpu_get_stream", "diablo_gpu_set_profiling", "diablo_gpu_kernel_times",
     "diablo_gpu_rem_div_chan_noalloc", "diablo_gpu_autotune", "diablo_gpu_batch_create",
-    "diablo_gpu_batch_step", "diablo_gpu_batch_destroy", "diablo_gpu_filter_chan",
+    "diablo_gpu_batch_step", "diablo_gpu_batch_destroy", "diablo_gpu_filter_chan", "diablo_gpu_download_nu_t",
 ]
 KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
 
@@ -83,6 +83,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_batch_step.argtypes = [vp, ip]
     L.diablo_gpu_batch_destroy.argtypes = [vp]
     L.diablo_gpu_filter_chan.argtypes = [vp, ip]
+    L.diablo_gpu_download_nu_t.argtypes = [vp, dp]
     _lib = L
     return L
 
@@ -191,6 +192,12 @@ class Channel:
         phi = new_fourier(self.p)
         _check(self.L.diablo_gpu_download_phi(self._h, _dp(phi.view(np.float64))), "diablo_gpu_download_phi")
         return phi
+
+    def download_nu_t(self) -> np.ndarray:
+        """NU_T at GY points as [J][K][I] (NY+2, NZ, NX); LES only."""
+        buf = np.zeros(physical_shape(self.p))
+        _check(self.L.diablo_gpu_download_nu_t(self._h, _dp(buf)), "diablo_gpu_download_nu_t")
+        return buf[:, : self.p.nz, : self.p.nx].copy()
 
     # --- routines of the reference ------------------------------------------
     def rk_chan_1(self, rk_step: int) -> None:

@@ -63,6 +63,14 @@ struct Handle {
     double* dtmin = nullptr;
     double* d_k2 = nullptr;       // (KX^2+KZ^2)**BETA per padded column
     double* d_rows = nullptr;     // [RT_COUNT][nyp] reciprocal grid metrics
+    // LES branch (allocated when p.les): NU_T at GY points, physical fields
+    // (lu: U1..U3, TH; la, lb: work fields), spectral work (ls: 7 fields, lr:
+    // the nf right-hand sides), the x-spectrum work lx and the filter widths
+    // Delta_YF, Delta_Y ([2][nyp])
+    double *nut = nullptr, *lu = nullptr, *la = nullptr, *lb = nullptr, *d_delta = nullptr;
+    double2 *ls = nullptr, *lr = nullptr;
+    void* lx = nullptr;
+    bool nut_set = false;         // NU_T has been computed at least once
     FftPlan pm, pz;   // NX/2-point complex plan (real x transforms), NZ-point plan
     void *twn_d = nullptr, *twm_d = nullptr, *twz_d = nullptr;   // exp(-2 pi i k/n), n = NX, NX/2, NZ
     void *twn_f = nullptr, *twm_f = nullptr, *twz_f = nullptr;
@@ -127,7 +135,7 @@ void free_handle(Handle* h) {
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
                     h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_tabs, h->d_phitab,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
-                    h->twz_f};
+                    h->twz_f, h->nut, h->lu, h->la, h->lb, h->d_delta, h->ls, h->lr, h->lx};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (h->st) cudaStreamDestroy(h->st);
@@ -260,7 +268,11 @@ int validate(const diablo_params* p) {
     if (p->nx > 1536 || p->nz > 512) return fail(DIABLO_EINVAL, "NX <= 1536 and NZ <= 512 are supported");
     if (p->ny < 4) return fail(DIABLO_EINVAL, "NY must be >= 4");
     if (p->n_th < 0 || p->n_th > DIABLO_MAX_TH) return fail(DIABLO_EINVAL, "N_TH must be in 0..4");
-    if (p->les) return fail(DIABLO_ENOTSUP, "LES is not supported");
+    if (p->les) {
+        // les.f:269-272 stops for the dynamic models
+        if (p->les_model_type != 1) return fail(DIABLO_ENOTSUP, "LES_MODEL_TYPE must be 1 (constant Smagorinsky)");
+        if (p->precision != DIABLO_PREC_FP64) return fail(DIABLO_ENOTSUP, "the LES branch runs in FP64 only");
+    }
     auto bc01 = [](int t) { return t == 0 || t == 1; };
     if (!bc01(p->u_bc_ymin) || !bc01(p->u_bc_ymax) || !bc01(p->w_bc_ymin) || !bc01(p->w_bc_ymax) ||
         !bc01(p->v_bc_ymin) || !bc01(p->v_bc_ymax))
@@ -402,6 +414,18 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = dmalloc((void**)&h->dtmin, sizeof(double));
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_k2, sizeof(double) * d.splane());
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_rows, sizeof(double) * RT_COUNT * nyp);
+    if (p->les) {
+        const size_t pf = sizeof(double) * nyp * d.nz * d.nx;
+        const int nw = d.nf > 7 ? d.nf : 7;
+        if (e == cudaSuccess) e = dmalloc((void**)&h->nut, pf);
+        if (e == cudaSuccess) e = dmalloc((void**)&h->lu, pf * d.nf);
+        if (e == cudaSuccess) e = dmalloc((void**)&h->la, pf * nw);
+        if (e == cudaSuccess) e = dmalloc((void**)&h->lb, pf * 7);
+        if (e == cudaSuccess) e = dmalloc((void**)&h->ls, sb * 7);
+        if (e == cudaSuccess) e = dmalloc((void**)&h->lr, sb * d.nf);
+        if (e == cudaSuccess) e = dmalloc(&h->lx, sizeof(double2) * h->x_field * nw);
+        if (e == cudaSuccess) e = dmalloc((void**)&h->d_delta, sizeof(double) * 2 * nyp);
+    }
     if (e != cudaSuccess) {
         free_handle(h);
         return fail(e == cudaErrorMemoryAllocation ? DIABLO_ENOMEM : DIABLO_ECUDA,
@@ -441,6 +465,17 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = cudaMemcpy(h->d_dy, dy, sizeof(double) * nyp, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(h->d_dyf, dyf, sizeof(double) * nyp, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(h->d_gyf, gyf, sizeof(double) * nyp, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && p->les) {
+        // filter widths with -2 C_s^2 absorbed, C_s = 0.13, beta_sgs = 1
+        // (les.f:196-217), Delta_YF at GYF and Delta_Y at GY points, J = 1..NY+1
+        std::vector<double> w(2 * nyp, 0.0);
+        const double C_SMAG = 0.13, beta_sgs = 1.0;
+        for (size_t j = 1; j < nyp; ++j) {
+            w[j] = -2.0 * (C_SMAG * C_SMAG) * std::pow(h->dx * beta_sgs * dyf[j] * 2.0 * h->dz * beta_sgs, 2.0 / 3.0);
+            w[nyp + j] = -2.0 * (C_SMAG * C_SMAG) * std::pow(h->dx * beta_sgs * dy[j] * 2.0 * h->dz * beta_sgs, 2.0 / 3.0);
+        }
+        e = cudaMemcpy(h->d_delta, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) h->twn_d = make_twiddles<double>(d.nx, &e);
     if (e == cudaSuccess) h->twm_d = make_twiddles<double>(d.nx / 2, &e);
     if (e == cudaSuccess) h->twz_d = make_twiddles<double>(d.nz, &e);
@@ -540,8 +575,9 @@ static int rem_div(Handle* h, int update_cp, double inv_h) {
 }
 
 // COURANT (courant.f:1-66): the a-priori limits on the host, the velocity
-// minimum on the device from the state's current CU1..CU3.
-static int courant(Handle* h, double* delta_t, double* h_bar) {
+// minimum on the device from the state's current CU1..CU3, or from physical
+// fields U1..U3 when phys is given (the LES branch's solved velocity).
+static int courant(Handle* h, double* delta_t, double* h_bar, const double* phys = nullptr) {
     const diablo_params& p = h->p;
     const Dims& d = h->d;
     double dt = 999.0;
@@ -555,10 +591,16 @@ static int courant(Handle* h, double* delta_t, double* h_bar) {
         }
     const double inf = HUGE_VAL;
     CK(cudaMemcpyAsync(h->dtmin, &inf, sizeof(double), cudaMemcpyHostToDevice, h->st));
-    { ProfScope ps(h, DIABLO_KERNEL_CFL);
-      CK(launch_zinv<double>(d, h->cu, h->s_field, h->xb, h->x_field, 3, 0, d.nyp, h->pz, h->twz_d, h->st));
-      CK(launch_cfl(d, h->xb, h->x_field, h->pm, h->twm_d, h->twn_d, h->d_dy, p.cfl, h->dx, h->dz, h->dtmin, h->st)); }
-    h->launches += 2;
+    if (phys) {
+        ProfScope ps(h, DIABLO_KERNEL_CFL);
+        CK(launch_les_cfl(d, phys, h->d_dy, p.cfl, h->dx, h->dz, h->dtmin, h->st));
+        h->launches += 1;
+    } else {
+        ProfScope ps(h, DIABLO_KERNEL_CFL);
+        CK(launch_zinv<double>(d, h->cu, h->s_field, h->xb, h->x_field, 3, 0, d.nyp, h->pz, h->twz_d, h->st));
+        CK(launch_cfl(d, h->xb, h->x_field, h->pm, h->twm_d, h->twn_d, h->d_dy, p.cfl, h->dx, h->dz, h->dtmin, h->st));
+        h->launches += 2;
+    }
     double vmin = inf;
     CK(cudaMemcpyAsync(&vmin, h->dtmin, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
@@ -574,6 +616,175 @@ static int courant(Handle* h, double* delta_t, double* h_bar) {
     return DIABLO_OK;
 }
 
+// The constants and row ranges of RK_CHAN_1 (channel.f:77-81, INIT_CHAN_MPI
+// for NPROCY = 1) as the LES kernels take them.
+static CnArgs substage_args(Handle* h, int rk_step, double time, const double* h_bar, const double* beta_bar,
+                            const double* zeta_bar) {
+    const diablo_params& p = h->p;
+    const Dims& d = h->d;
+    const int r = rk_step - 1;
+    const double TEMP4 = h_bar[r];
+    CnArgs a;
+    a.d = d;
+    a.cu = h->cu;
+    a.cf = h->cf;
+    a.cp = h->cp;
+    a.kx = h->d_kx;
+    a.kz = h->d_kz;
+    a.dy = h->d_dy;
+    a.dyf = h->d_dyf;
+    a.bcv = h->bcv;
+    a.kind = h->kind;
+    for (int f = 0; f < MAXF; ++f) { a.cf_lo[f] = 2; a.cf_hi[f] = d.ny; a.cb_lo[f] = 1; }
+    for (int n = 0; n < d.nth; ++n) {
+        a.cf_lo[3 + n] = h->jstart_th[n];
+        a.cf_hi[3 + n] = h->jend_th[n];
+        a.cb_lo[3 + n] = h->jstart_th[n] - 1;
+    }
+    a.temp1 = p.nu * h_bar[r] / 2.0;
+    a.temp3 = zeta_bar[r] * h_bar[r];
+    a.temp4 = TEMP4;
+    a.temp5 = beta_bar[r] * h_bar[r];
+    a.nu = p.nu; a.beta = p.beta; a.nu_v_scale = p.nu_v_scale; a.i_ro = p.i_ro;
+    a.grav_x = p.grav_x; a.grav_y = p.grav_y; a.grav_z = p.grav_z;
+    for (int n = 0; n < 4; ++n) {
+        a.ri[n] = n < d.nth ? p.ri[n] : 0.0;
+        a.pr[n] = n < d.nth ? p.pr[n] : 1.0;
+        a.drhodx[n] = n < d.nth ? p.drhodx[n] : 0.0;
+        a.drhodz[n] = n < d.nth ? p.drhodz[n] : 0.0;
+    }
+    a.forcing = 0.0;
+    if (p.f_type == 1) a.forcing = TEMP4 * p.px0;
+    else if (p.f_type == 2) a.forcing = TEMP4 * (p.px0 + p.amp_omega0 * std::cos(p.omega0 * time));
+    a.rk_step = rk_step;
+    a.store_cf = 1;
+    return a;
+}
+
+// Spectral fields [0,nfld) of S (stride s_field) -> physical fields of P
+// (stride pf), planes j0..j0+np-1, FP64.
+static cudaError_t les_to_phys(Handle* h, const double2* S, int nfld, double* P, int j0, int np) {
+    const Dims& d = h->d;
+    const size_t pf = (size_t)d.nyp * d.nz * d.nx;
+    cudaError_t e = launch_zinv<double>(d, S, h->s_field, h->lx, h->x_field, nfld, j0, np, h->pz, h->twz_d, h->st);
+    for (int f = 0; f < nfld && e == cudaSuccess; ++f)
+        e = launch_xinv(d, (const double2*)h->lx + (size_t)f * h->x_field, P + (size_t)f * pf, j0, np, h->pm, h->twm_d,
+                        h->twn_d, h->st);
+    h->launches += 1 + nfld;
+    return e;
+}
+
+// Physical fields -> spectral fields (FFT_XZ_TO_FOURIER), planes j0..j0+np-1.
+static cudaError_t les_to_fourier(Handle* h, const double* P, int nfld, double2* S, int j0, int np) {
+    const Dims& d = h->d;
+    const size_t pf = (size_t)d.nyp * d.nz * d.nx;
+    cudaError_t e = cudaSuccess;
+    for (int f = 0; f < nfld && e == cudaSuccess; ++f) {
+        double2* X = (double2*)h->lx + (size_t)f * h->x_field;
+        e = launch_xfwd(d, P + (size_t)f * pf, X, j0, np, h->pm, h->twm_d, h->twn_d, h->st);
+        if (e == cudaSuccess) e = launch_zfwd_pack(d, X, S + (size_t)f * h->s_field, j0, np, h->pz, h->twz_d, h->st);
+    }
+    h->launches += 2 * nfld;
+    return e;
+}
+
+// RK_CHAN_1 with LES set (channel.f:62-1073 with the LES branches), in the
+// reference's order: Fourier right-hand sides; when the subgrid model runs
+// (sgs), les_chan (strain rates, |S|, NU_T, tau_ij and the cross terms into
+// CF), the physical velocity BCs and the scalars' horizontal eddy
+// diffusivity; the nonlinear terms from the physical fields; CR to physical
+// space, the explicit CN half with the eddy-viscosity terms; one tridiagonal
+// solve per physical column and field; COURANT at the last substage on the
+// solved physical velocity; the fields back to Fourier space, the projection
+// and the pressure update.
+static int les_substage(Handle* h, int rk_step, int time_step, double time, double* delta_t, double* h_bar,
+                        const double* beta_bar, const double* zeta_bar, bool sgs) {
+    const diablo_params& p = h->p;
+    const Dims& d = h->d;
+    const int r = rk_step - 1;
+    const size_t pf = (size_t)d.nyp * d.nz * d.nx;
+    const int nyp = d.nyp;
+    const double* delta_yf = h->d_delta;
+    const double* delta_y = h->d_delta + nyp;
+    CnArgs a = substage_args(h, rk_step, time, h_bar, beta_bar, zeta_bar);
+    ProfScope ps(h, DIABLO_KERNEL_OTHER);
+    CK(launch_les_pre(a, h->d_k2, h->lr, h->st));
+    h->launches += 1;
+    if (sgs) {
+        // les_chan: ghost cells (APPLY_BC_VEL_MPI, APPLY_BC_LES), strain rates
+        dim3 grid((d.nkxp + 127) / 128, d.nkzt);
+        k_apply_bc_vel<<<grid, 128, 0, h->st>>>(d, h->cu, h->d_dy, h->d_dyf, p);
+        CK(cudaGetLastError());
+        CK(launch_les_bc(d, h->cu, p, h->st));
+        CK(launch_les_strain(d, h->cu, h->d_kx, h->d_kz, h->d_dy, h->d_dyf, h->ls, h->st));
+        h->launches += 3;
+        CK(les_to_phys(h, h->ls, 6, h->la, 0, nyp));
+        CK(les_to_phys(h, h->cu, 3, h->lu, 0, nyp));
+        CK(launch_les_sgs(d, h->la, h->lu, h->cu, h->d_dy, h->d_dyf, delta_y, h->lb, h->nut, h->st));
+        CK(launch_phys_bc_vel(d, h->lu, h->d_dy, h->d_dyf, p, h->st));
+        h->launches += 2;
+        h->nut_set = true;
+        CK(les_to_fourier(h, h->lb, 7, h->ls, 0, nyp));
+        CK(launch_les_tau_cf(d, h->ls, h->cf, h->d_kx, h->d_kz, h->d_dyf, delta_yf, delta_y, h->st));
+        h->launches += 1;
+        // horizontal eddy diffusivity of each scalar, KAPPA_T = NU_T
+        for (int n = 0; n < d.nth; ++n) {
+            const double2* cth = h->cu + (size_t)(3 + n) * h->s_field;
+            CK(launch_les_kgrad(d, cth, h->d_kx, h->d_kz, h->ls, h->st));
+            CK(les_to_phys(h, h->ls, 2, h->la, 0, nyp));
+            CK(launch_les_kmul(d, h->la, h->nut, h->st));
+            CK(les_to_fourier(h, h->la, 2, h->ls, 0, nyp));
+            CK(launch_les_kcf(d, h->ls, h->cf + (size_t)(3 + n) * h->s_field, h->d_kx, h->d_kz, h->jstart_th[n],
+                              h->jend_th[n], h->st));
+            h->launches += 3;
+        }
+    } else {
+        CK(les_to_phys(h, h->cu, 3, h->lu, 0, nyp));
+    }
+    if (d.nth > 0) CK(les_to_phys(h, h->cu + 3 * h->s_field, d.nth, h->lu + 3 * pf, 0, nyp));
+    // nonlinear terms from the physical fields: x spectra, then the products
+    // and z-forward kernels of the Fourier-space path
+    for (int f = 0; f < d.nf; ++f)
+        CK(launch_xfwd(d, h->lu + (size_t)f * pf, (double2*)h->xb + (size_t)f * h->x_field, 0, nyp, h->pm, h->twm_d,
+                       h->twn_d, h->st));
+    CK(launch_products<double>(d, h->xb, h->yb, h->jlo_prod, d.ny, h->prod_chunk, h->d_dy, h->d_dyf, h->d_kx, h->pm,
+                               h->twm_d, h->twn_d, h->st));
+    CK(launch_zfwd_nl<double>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->zf_planes, h->d_kx, h->d_kz, h->pz, h->twz_d,
+                              h->st));
+    CK(launch_les_post(a, (const double2*)h->nl, h->lr, h->st));
+    h->launches += d.nf + 3;
+    // CN in physical space
+    CK(les_to_phys(h, h->lr, d.nf, h->la, 0, nyp));
+    LesArgs la;
+    la.d = d;
+    la.dy = h->d_dy;
+    la.dyf = h->d_dyf;
+    la.temp1 = a.temp1;
+    la.temp2 = h_bar[r] / 2.0;
+    la.nu_v_scale = p.nu_v_scale;
+    for (int n = 0; n < 4; ++n) la.pr[n] = a.pr[n];
+    for (int f = 0; f < MAXF; ++f) {
+        la.j_lo[f] = a.cf_lo[f];
+        la.j_hi[f] = a.cf_hi[f];
+        la.out_lo[f] = a.cb_lo[f];
+        la.bc_type[f][0] = h->bc_type[2 * f];
+        la.bc_type[f][1] = h->bc_type[2 * f + 1];
+        la.bc_c1[f][0] = h->bc_c1[2 * f];
+        la.bc_c1[f][1] = h->bc_c1[2 * f + 1];
+    }
+    CK(launch_les_explicit(la, h->lu, h->la, h->nut, h->st));
+    for (int f = 0; f < d.nf; ++f)
+        CK(launch_les_solve(la, f, h->la + (size_t)f * pf, h->nut, h->lb, h->lb + pf, h->lu + (size_t)f * pf, h->st));
+    h->launches += 1 + d.nf;
+    const double inv_h = 1.0 / a.temp4;
+    if (p.variable_dt && rk_step == 3 && (time_step % p.update_dt) == 0) {
+        int rc = courant(h, delta_t, h_bar, h->lu);
+        if (rc) return rc;
+    }
+    CK(les_to_fourier(h, h->lu, d.nf, h->cu, 0, nyp));
+    return rem_div(h, 1, inv_h);
+}
+
 int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, double* delta_t,
                          double* h_bar, const double* beta_bar, const double* zeta_bar) {
     Handle* h = (Handle*)handle;
@@ -582,6 +793,13 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     const diablo_params& p = h->p;
     const Dims& d = h->d;
     const int r = rk_step - 1;
+    if (p.les) {
+        // the subgrid model waits for the spin-up of a new flow (channel.f:303);
+        // until NU_T is first computed it is zero and the LES terms add
+        // nothing, so the Fourier-space path gives the same step
+        const bool sgs = !p.create_new_flow || time_step > 100;
+        if (sgs || h->nut_set) return les_substage(h, rk_step, time_step, time, delta_t, h_bar, beta_bar, zeta_bar, sgs);
+    }
     // constants of channel.f:77-81
     const double TEMP1 = p.nu * h_bar[r] / 2.0;
     const double TEMP3 = zeta_bar[r] * h_bar[r];
@@ -646,6 +864,15 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     // pressure update with the h of this substage
     if ((rc = courant(h, delta_t, h_bar))) return rc;
     return rem_div(h, 1, 1.0 / TEMP4);
+}
+
+int diablo_gpu_download_nu_t(void* handle, double* nu_t) {
+    Handle* h = (Handle*)handle;
+    if (!h || !nu_t) return fail(DIABLO_EINVAL, "null pointer argument");
+    if (!h->p.les) return fail(DIABLO_EINVAL, "NU_T exists only when LES is set");
+    CK(copy_physical(h, h->nut, nullptr, nu_t, 0, h->d.nyp));
+    CK(cudaStreamSynchronize(h->st));
+    return DIABLO_OK;
 }
 
 int diablo_gpu_rk_chan_2(void* handle) {
@@ -1055,6 +1282,7 @@ int diablo_gpu_batch_create(void* const* handles, const double* delta_t, int n, 
         if (!h) return fail(DIABLO_EINVAL, "null handle in batch");
         if (h->p.variable_dt) return fail(DIABLO_ENOTSUP, "batched instances need a fixed time step (variable_dt = 0)");
         if (h->p.f_type == 2) return fail(DIABLO_ENOTSUP, "batched instances cannot have time-dependent forcing");
+        if (h->p.les) return fail(DIABLO_ENOTSUP, "batched instances cannot run the LES branch");
         if (h->profiling) return fail(DIABLO_EINVAL, "batched instance with profiling on");
         if (!(delta_t[i] > 0.0)) return fail(DIABLO_EINVAL, "batched instance with delta_t <= 0");
     }

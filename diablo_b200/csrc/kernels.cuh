@@ -103,6 +103,19 @@ struct RemDivArgs {
     int update_cp;        // CP += phi/h on J = 2..NY
 };
 
+// Physical-space CN steps of the LES branch (les.cu).
+struct LesArgs {
+    Dims d;
+    const double* dy;
+    const double* dyf;
+    double temp1, temp2, nu_v_scale;
+    double pr[4];
+    int j_lo[MAXF], j_hi[MAXF];     // interior rows of each field's system
+    int out_lo[MAXF];               // first row copied back (the last is NY+1)
+    int bc_type[MAXF][2];
+    double bc_c1[MAXF][2];
+};
+
 // POISSON_P_CHAN column solve (poisson_stats.cu).
 struct PoissonArgs {
     Dims d;

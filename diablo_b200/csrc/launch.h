@@ -5,6 +5,7 @@
 
 #include <string>
 
+#include "../../include/diablo_gpu.h"
 #include "kernels.cuh"
 
 namespace dgpu {
@@ -88,6 +89,30 @@ cudaError_t launch_stats_planes(const Dims& d, const double* u1, const double* u
 // are NX and NZ as the reference's FLOAT() gives them.
 cudaError_t launch_filter_chan(const Dims& d, double2* cth, const double* kx, const double* kz, double lx,
                                double lz, double fnx, double fnz, cudaStream_t st);
+// Constant-Smagorinsky LES branch (les.cu, FP64).  Spectral kernels run over
+// the retained modes of planes 0..NY+1, physical ones over P[J][z][x].
+cudaError_t launch_les_pre(const CnArgs& a, const double* k2, double2* r, cudaStream_t st);
+cudaError_t launch_les_bc(const Dims& d, double2* cu, const diablo_params& p, cudaStream_t st);
+cudaError_t launch_les_strain(const Dims& d, const double2* cu, const double* kx, const double* kz, const double* dy,
+                              const double* dyf, double2* sij, cudaStream_t st);
+cudaError_t launch_les_sgs(const Dims& d, const double* sij, const double* u, const double2* cu, const double* dy,
+                           const double* dyf, const double* delta_y, double* out, double* nut, cudaStream_t st);
+cudaError_t launch_phys_bc_vel(const Dims& d, double* u, const double* dy, const double* dyf, const diablo_params& p,
+                               cudaStream_t st);
+cudaError_t launch_les_tau_cf(const Dims& d, const double2* tau, double2* cf, const double* kx, const double* kz,
+                              const double* dyf, const double* delta_yf, const double* delta_y, cudaStream_t st);
+cudaError_t launch_les_kgrad(const Dims& d, const double2* cth, const double* kx, const double* kz, double2* out,
+                             cudaStream_t st);
+cudaError_t launch_les_kmul(const Dims& d, double* a, const double* nut, cudaStream_t st);
+cudaError_t launch_les_kcf(const Dims& d, const double2* g2, double2* cfth, const double* kx, const double* kz, int j0,
+                           int j1, cudaStream_t st);
+cudaError_t launch_les_post(const CnArgs& a, const double2* nl, double2* r, cudaStream_t st);
+cudaError_t launch_les_explicit(const LesArgs& a, const double* u, double* r, const double* nut, cudaStream_t st);
+cudaError_t launch_les_solve(const LesArgs& a, int f, const double* r, const double* nut, double* piv, double* rhs,
+                             double* out, cudaStream_t st);
+// COURANT's velocity minimum over physical rows 1..NY of U1..U3 (u: 3 fields).
+cudaError_t launch_les_cfl(const Dims& d, const double* u, const double* dy, double cfl, double dx, double dz,
+                           double* dtmin, cudaStream_t st);
 // rows transformed together by the products kernel for a given NX
 int products_group(int nx);
 // Record the one-line message returned by diablo_gpu_last_error; returns code.

@@ -108,10 +108,20 @@ int diablo_gpu_download_state(void* handle, double* cu1, double* cu2, double* cu
  * and COURANT at rk_step 3 when variable_dt and mod(time_step,update_dt)==0
  * (channel.f:1037-1040).  h_bar/beta_bar/zeta_bar are /RKW3_PARAMS/
  * (for/header:173-174).  delta_t and h_bar are updated in place when
- * COURANT runs, exactly as courant.f:49-62 updates DELTA_T and H_BAR. */
+ * COURANT runs, exactly as courant.f:49-62 updates DELTA_T and H_BAR.
+ * With p.les set (LES_MODEL_TYPE 1, FP64) the substage includes the
+ * constant-Smagorinsky branch (for/les.f:1-336, channel.f:303-384 and the
+ * eddy-viscosity terms) once LES and (not CREATE_NEW_FLOW or
+ * time_step > 100), and then solves the CN systems per physical column as
+ * the reference does. */
 int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time,
                          double* delta_t, double* h_bar, const double* beta_bar,
                          const double* zeta_bar);
+/* NU_T(0:NX+1,0:NZP+1,0:NY+1) of COMMON /LES_VARS/ (for/header:164-168) in
+ * the host physical layout (entries with I >= NX or K >= NZ untouched): the
+ * eddy viscosity at GY points of the last LES substage, zero before the
+ * first.  DIABLO_EINVAL without LES. */
+int diablo_gpu_download_nu_t(void* handle, double* nu_t);
 /* RK_CHAN_2 (for/channel.f:1076-1100) is a stub in the reference that prints
  * "not supported" and stops; this returns DIABLO_ENOTSUP. */
 int diablo_gpu_rk_chan_2(void* handle);

@@ -1,0 +1,92 @@
+"""GPU parity of the constant-Smagorinsky LES branch against the oracle: the
+state after several RK3 steps and the eddy viscosity NU_T, through the
+C ABI, to the FP64 bar of the other parity tests (1e-10 relative L2, the
+small velocity components and the pressure measured against the velocity
+and pressure scales)."""
+import pytest
+
+from diablo_b200 import grid as G, ics, params as P
+from diablo_b200.channel import Batch, Channel, DiabloError, DIABLO_ENOTSUP
+from oracle.oracle import Oracle
+from test_gpu_parity import TOL64, relerr, state_errors
+
+pytestmark = pytest.mark.gpu
+
+
+def les_channel(nx=32, ny=33, nz=24, n_th=1, neumann_top=False, variable_dt=False, create_new_flow=0):
+    p = P.turbulent_channel(nx, ny, nz, re_tau=180.0, variable_dt=variable_dt)
+    p.les, p.les_model_type, p.create_new_flow = 1, 1, create_new_flow
+    p.n_th = n_th
+    for n in range(1, n_th):
+        p.pr[n], p.ri[n] = 1.0 + n, 0.0
+        p.th_bc_ymin[n], p.th_bc_ymax[n] = 1, 0      # Neumann bottom: JSTART_TH = 1
+        p.th_bc_ymin_c1[n], p.th_bc_ymax_c1[n] = 0.5, 1.0
+    if neumann_top:
+        p.u_bc_ymax = p.w_bc_ymax = 1
+        p.u_bc_ymax_c1, p.w_bc_ymax_c1 = 0.1, -0.05
+    g = G.channel_grid(G.create_grid(1, p.ny, 2.0, 1.75))
+    u, th = ics.poiseuille(p, g, u_center=10.0, seed=3, noise=0.5)
+    if n_th > 1:
+        th[1:] = th[:1] * 0.5 + 0.1
+    return p, g, u, th
+
+
+def run(p, g, u, th, dt, steps, start_step=0):
+    o = Oracle(p, g, dt)
+    o.init_from_physical(u, th)
+    c = Channel(p, g, dt)
+    c.upload([x.copy() for x in o.cu], o.cp.copy(), o.cth.copy())
+    if start_step:
+        t, d, _, _ = o.time()
+        o.set_time(t, d, start_step)
+        c.time_step = start_step
+    with c:
+        for _ in range(steps):
+            o.step()
+            c.step()
+            if p.variable_dt:
+                assert c.delta_t == pytest.approx(o.time()[1], rel=1e-12)
+        err = state_errors(p, c, o, scaled=True)
+        plain = state_errors(p, c, o)
+        nut = relerr(c.download_nu_t(), o.nu_t)
+    return err, plain, nut, o
+
+
+def test_les_channel_dirichlet():
+    """Closed channel, no-slip walls, one scalar: 4 steps with the model on."""
+    p, g, u, th = les_channel()
+    err, plain, nut, o = run(p, g, u, th, 2e-4, 4)
+    assert o.nu_t.max() > 0.0
+    assert nut < TOL64, nut
+    assert max(err.values()) < TOL64, (err, plain)
+
+
+def test_les_neumann_top_two_scalars_variable_dt():
+    """Stress-free upper wall (APPLY_BC_LES rewrites row NY), a second scalar
+    with a Neumann lower wall (JSTART_TH = 1), CFL-adaptive dt, radix-3 x."""
+    p, g, u, th = les_channel(nx=48, ny=33, nz=24, n_th=2, neumann_top=True, variable_dt=True)
+    err, plain, nut, _ = run(p, g, u, th, 2e-4, 3)
+    assert nut < TOL64, nut
+    assert max(err.values()) < TOL64, (err, plain)
+
+
+def test_les_spin_up_switch():
+    """CREATE_NEW_FLOW: step 100 runs without the model, 101 and 102 with it."""
+    p, g, u, th = les_channel(create_new_flow=1)
+    err, plain, nut, o = run(p, g, u, th, 2e-4, 3, start_step=99)
+    assert o.nu_t.max() > 0.0
+    assert nut < TOL64, nut
+    assert max(err.values()) < TOL64, (err, plain)
+
+
+def test_les_rejected_configurations():
+    p, g, _, _ = les_channel()
+    q = p.copy()
+    q.precision = P.PREC_FP32SPLIT
+    with pytest.raises(DiabloError) as e:
+        Channel(q, g, 2e-4)
+    assert e.value.code == DIABLO_ENOTSUP
+    with Channel(p, g, 2e-4) as c:
+        with pytest.raises(DiabloError) as e:
+            Batch([c])
+        assert e.value.code == DIABLO_ENOTSUP
