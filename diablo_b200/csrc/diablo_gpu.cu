@@ -759,6 +759,7 @@ static int les_substage(Handle* h, int rk_step, int time_step, double time, doub
     la.d = d;
     la.dy = h->d_dy;
     la.dyf = h->d_dyf;
+    la.rows = h->d_rows;
     la.temp1 = a.temp1;
     la.temp2 = h_bar[r] / 2.0;
     la.nu_v_scale = p.nu_v_scale;
@@ -773,9 +774,8 @@ static int les_substage(Handle* h, int rk_step, int time_step, double time, doub
         la.bc_c1[f][1] = h->bc_c1[2 * f + 1];
     }
     CK(launch_les_explicit(la, h->lu, h->la, h->nut, h->st));
-    for (int f = 0; f < d.nf; ++f)
-        CK(launch_les_solve(la, f, h->la + (size_t)f * pf, h->nut, h->lb, h->lb + pf, h->lu + (size_t)f * pf, h->st));
-    h->launches += 1 + d.nf;
+    CK(launch_les_solve(la, h->la, h->nut, h->lb, h->lu, h->st));
+    h->launches += 2;
     const double inv_h = 1.0 / a.temp4;
     if (p.variable_dt && rk_step == 3 && (time_step % p.update_dt) == 0) {
         int rc = courant(h, delta_t, h_bar, h->lu);

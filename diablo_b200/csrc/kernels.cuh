@@ -108,6 +108,7 @@ struct LesArgs {
     Dims d;
     const double* dy;
     const double* dyf;
+    const double* rows;             // [RT_COUNT][nyp] reciprocal row tables
     double temp1, temp2, nu_v_scale;
     double pr[4];
     int j_lo[MAXF], j_hi[MAXF];     // interior rows of each field's system

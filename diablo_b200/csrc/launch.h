@@ -108,8 +108,10 @@ cudaError_t launch_les_kcf(const Dims& d, const double2* g2, double2* cfth, cons
                            int j1, cudaStream_t st);
 cudaError_t launch_les_post(const CnArgs& a, const double2* nl, double2* r, cudaStream_t st);
 cudaError_t launch_les_explicit(const LesArgs& a, const double* u, double* r, const double* nut, cudaStream_t st);
-cudaError_t launch_les_solve(const LesArgs& a, int f, const double* r, const double* nut, double* piv, double* rhs,
-                             double* out, cudaStream_t st);
+// All fields' column solves; r (nf physical fields) is overwritten, piv holds
+// nf fields of pivots, out receives the solution rows.
+cudaError_t launch_les_solve(const LesArgs& a, double* r, const double* nut, double* piv, double* out,
+                             cudaStream_t st);
 // COURANT's velocity minimum over physical rows 1..NY of U1..U3 (u: 3 fields).
 cudaError_t launch_les_cfl(const Dims& d, const double* u, const double* dy, double cfl, double dx, double dz,
                            double* dtmin, cudaStream_t st);

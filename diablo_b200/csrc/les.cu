@@ -354,37 +354,29 @@ __global__ void __launch_bounds__(TB) k_les_explicit(LesArgs a, const double* __
 // eddy-viscosity terms (channel.f:786-805, 851-874, 916-939, 980-1003), then
 // the BC rows of APPLY_BC_TH_*, APPLY_BC_2_*, APPLY_BC_1_* / _3_*
 // (channel.f:1660-2202) written over it, in the reference's order.  Rows
-// outside the system are the identity with a zero right-hand side.
+// outside the system are the identity with a zero right-hand side.  The
+// grid metrics come from the reciprocal row tables (RT_E*), so a row costs
+// no division.
 __device__ __forceinline__ void les_row(const LesArgs& a, int f, int j, double n0, double np, double nm, double rv,
                                         double& L, double& D, double& U, double& V) {
     const int ny = a.d.ny;
-    const double* dy = a.dy;
-    const double* dyf = a.dyf;
+    const int nyp = a.d.nyp;
     L = 0.0; D = 1.0; U = 0.0; V = 0.0;
     if (j >= a.j_lo[f] && j <= a.j_hi[f]) {
-        const double t1 = a.temp1, t2 = a.temp2, nuv = a.nu_v_scale;
+        const double t2 = a.temp2;
         if (f == 1) {
-            L = -t1 * nuv / (dyf[j - 1] * dy[j]);
-            D = 1. + t1 * nuv / (dyf[j] * dy[j]) + t1 * nuv / (dyf[j - 1] * dy[j]);
-            U = -t1 * nuv / (dyf[j] * dy[j]);
-            L = L - t2 * 0.5 * (n0 + nm) / (dyf[j - 1] * dy[j]);
-            D = D + t2 * 0.5 * (n0 + np) / (dyf[j] * dy[j]) + t2 * 0.5 * (n0 + nm) / (dyf[j - 1] * dy[j]);
-            U = U - t2 * 0.5 * (n0 + np) / (dyf[j] * dy[j]);
-        } else if (f == 0 || f == 2) {
-            L = -t1 * nuv / (dy[j] * dyf[j]);
-            D = 1. - t1 * nuv * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
-            U = -t1 * nuv / (dy[j + 1] * dyf[j]);
-            L = L - t2 * n0 / (dy[j] * dyf[j]);
-            D = D + t2 * np / (dy[j + 1] * dyf[j]) + t2 * n0 / (dy[j] * dyf[j]);
-            U = U - t2 * np / (dy[j + 1] * dyf[j]);
+            const double em = a.rows[RT_E2M * nyp + j], ep = a.rows[RT_E2P * nyp + j];
+            const double c = a.temp1 * a.nu_v_scale;
+            const double sm = t2 * 0.5 * (n0 + nm), sp = t2 * 0.5 * (n0 + np);
+            L = -c * em - sm * em;
+            D = 1. + c * ep + c * em + sp * ep + sm * em;
+            U = -c * ep - sp * ep;
         } else {
-            const double c = t1 / a.pr[f - 3] * nuv;
-            L = -c / (dy[j] * dyf[j]);
-            D = 1. + c / (dy[j + 1] * dyf[j]) + c / (dy[j] * dyf[j]);
-            U = -c / (dy[j + 1] * dyf[j]);
-            L = L - t2 * n0 / (dy[j] * dyf[j]);
-            D = D + t2 * np / (dy[j + 1] * dyf[j]) + t2 * n0 / (dy[j] * dyf[j]);
-            U = U - t2 * np / (dy[j + 1] * dyf[j]);
+            const double em = a.rows[RT_E1M * nyp + j], ep = a.rows[RT_E1P * nyp + j];
+            const double c = f < 3 ? a.temp1 * a.nu_v_scale : a.temp1 / a.pr[f - 3] * a.nu_v_scale;
+            L = -c * em - t2 * n0 * em;
+            D = 1. + c * ep + c * em + t2 * np * ep + t2 * n0 * em;
+            U = -c * ep - t2 * np * ep;
         }
         V = rv;
     }
@@ -395,64 +387,77 @@ __device__ __forceinline__ void les_row(const LesArgs& a, int f, int j, double n
         if (bmin == 0) {
             if (j == 1 || j == 2) set(0.0, 1.0, 0.0, cmin);
         } else if (j == 1) {
-            set(0.0, -1.0, 1.0, dyf[1] * cmin);
+            set(0.0, -1.0, 1.0, a.dyf[1] * cmin);
         }
         if (j == 0) set(0.0, 1.0, 0.0, 0.0);
         if (bmax == 0) {
             if (j == ny + 1 || j == ny) set(0.0, 1.0, 0.0, cmax);
         } else if (j == ny + 1) {
-            set(-1.0, 1.0, 0.0, dyf[ny] * cmax);
+            set(-1.0, 1.0, 0.0, a.dyf[ny] * cmax);
         }
     } else {        // U1, U3 and the scalars share the GYF-point rows
         if (j == 0) set(0.0, 1.0, 0.0, 0.0);
         if (j == 1) {
             if (bmin == 0) set(0.0, 1.0, 0.0, cmin);
-            else set(0.0, -1.0, 1.0, dy[2] * cmin);
+            else set(0.0, -1.0, 1.0, a.dy[2] * cmin);
         }
         if (j == ny + 1) set(0.0, 1.0, 0.0, 0.0);
         if (j == ny) {
             if (bmax == 0) set(0.0, 1.0, 0.0, cmax);
-            else set(-1.0, 1.0, 0.0, dy[ny] * cmax);
+            else set(-1.0, 1.0, 0.0, a.dy[ny] * cmax);
         }
     }
 }
 
-// THOMAS_FORWARD/BACKWARD_REAL_MPI (mpi.f:630-697, 757-809) with NPROCY = 1
-// for field f, one thread per physical (x,z) column: forward elimination over
-// rows 1..NY+1 keeping the pivots and the eliminated right-hand side in
-// scratch, back substitution from NY+1 down to 0 (zero where a pivot is
-// zero), result written on the rows the reference copies back.
-__global__ void __launch_bounds__(TB) k_les_solve(LesArgs a, int f, const double* __restrict__ r,
-                                                  const double* __restrict__ nut, double* __restrict__ piv,
-                                                  double* __restrict__ rhs, double* __restrict__ out) {
+// THOMAS_FORWARD/BACKWARD_REAL_MPI (mpi.f:630-697, 757-809) with NPROCY = 1,
+// one thread per physical (x,z) column and field (blockIdx.y): forward
+// elimination over rows 1..NY+1, the eliminated right-hand side written over
+// the right-hand side r and the pivots kept in piv; back substitution from
+// NY+1 down to 0 (zero where a pivot is zero), the result written on the
+// rows the reference copies back.
+__global__ void __launch_bounds__(TB) k_les_solve(LesArgs a, double* __restrict__ r, const double* __restrict__ nut,
+                                                  double* __restrict__ piv, double* __restrict__ out) {
     const Dims& d = a.d;
-    const size_t pp = plane_pts(d);
+    const size_t pp = plane_pts(d), pf = pp * d.nyp;
     const size_t g = (size_t)blockIdx.x * TB + threadIdx.x;
+    const int f = blockIdx.y;
     if (g >= pp) return;
     const int ny = d.ny;
-    auto N = [&](int j) { return (j >= 0 && j <= ny + 1) ? nut[(size_t)j * pp + g] : 0.0; };
+    r += (size_t)f * pf;
+    piv += (size_t)f * pf;
+    out += (size_t)f * pf;
     double L, D, U, V;
-    les_row(a, f, 0, N(0), N(1), 0.0, r[g], L, D, U, V);
+    double nm = 0.0, n0 = nut[g], np = nut[pp + g];
+    les_row(a, f, 0, n0, np, nm, r[g], L, D, U, V);
     double Bp = D, Gp = V, Up = U;
     piv[g] = Bp;
-    rhs[g] = Gp;
+    r[g] = Gp;
     for (int j = 1; j <= ny + 1; ++j) {
         const size_t q = (size_t)j * pp + g;
-        les_row(a, f, j, N(j), N(j + 1), N(j - 1), r[q], L, D, U, V);
+        nm = n0;
+        n0 = np;
+        np = j + 1 <= ny + 1 ? nut[q + pp] : 0.0;
+        les_row(a, f, j, n0, np, nm, r[q], L, D, U, V);
         const double A = -L / Bp;
         Bp = D + A * Up;
         Gp = V + A * Gp;
         Up = U;
         piv[q] = Bp;
-        rhs[q] = Gp;
+        r[q] = Gp;
     }
     double x = Gp / Bp;
     if (ny + 1 >= a.out_lo[f]) out[(size_t)(ny + 1) * pp + g] = x;
+    np = 0.0;
+    n0 = nut[(size_t)(ny + 1) * pp + g];
+    nm = nut[(size_t)ny * pp + g];
     for (int j = ny; j >= 0; --j) {
         const size_t q = (size_t)j * pp + g;
-        les_row(a, f, j, N(j), N(j + 1), N(j - 1), 0.0, L, D, U, V);
+        np = n0;
+        n0 = nm;
+        nm = j >= 1 ? nut[q - pp] : 0.0;
+        les_row(a, f, j, n0, np, nm, 0.0, L, D, U, V);
         const double b = piv[q];
-        x = b != 0.0 ? (rhs[q] - U * x) / b : 0.0;
+        x = b != 0.0 ? (r[q] - U * x) / b : 0.0;
         if (j >= a.out_lo[f]) out[q] = x;
     }
 }
@@ -548,9 +553,10 @@ cudaError_t launch_les_explicit(const LesArgs& a, const double* u, double* r, co
     return cudaGetLastError();
 }
 
-cudaError_t launch_les_solve(const LesArgs& a, int f, const double* r, const double* nut, double* piv, double* rhs,
-                             double* out, cudaStream_t st) {
-    k_les_solve<<<blocks(plane_pts(a.d)), TB, 0, st>>>(a, f, r, nut, piv, rhs, out);
+cudaError_t launch_les_solve(const LesArgs& a, double* r, const double* nut, double* piv, double* out,
+                             cudaStream_t st) {
+    dim3 grid(blocks(plane_pts(a.d)), a.d.nf);
+    k_les_solve<<<grid, TB, 0, st>>>(a, r, nut, piv, out);
     return cudaGetLastError();
 }
 

@@ -592,55 +592,67 @@ cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int 
 }
 
 // ---------------------------------------------------------------------------
-// Transform-API helpers (FP64, one field, run-time lengths).
-// Rows r = (J - j0)*NZ + z; a block handles `group` consecutive rows.
+// Transform-API helpers (FP64, one field).  Rows r = (J - j0)*NZ + z; a block
+// handles `group` consecutive rows: PROD_G rows through the compile-time FFT
+// when M = NX/2 has one (MC > 0), else a smaller group through the run-time
+// FFT.  The M- and NX-point twiddles are staged in shared memory.
 // ---------------------------------------------------------------------------
+template <int MC>
 __global__ void __launch_bounds__(256) k_xinv(Dims d, const cpx<double>* __restrict__ X,
                                               double* __restrict__ P, int j0, int nrows, int group,
                                               FftPlan pm, const cpx<double>* __restrict__ twm,
                                               const cpx<double>* __restrict__ twn) {
-    extern __shared__ unsigned char smem_raw[];
-    cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
-    const int M = d.nx / 2;
-    RowLayoutRT lay{row_pitch(M)};
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int M = MC > 0 ? MC : d.nx / 2;
+    using Lay = typename std::conditional<(MC > 0), RowLayoutCT<MC>, RowLayoutRT>::type;
+    Lay lay;
+    if constexpr (MC == 0) lay.pitch = row_pitch(M);
+    cpx<double>* stw = reinterpret_cast<cpx<double>*>(smem_raw);
+    cpx<double>* buf = stw + 3 * M;
+    for (int e = threadIdx.x; e < 3 * M; e += 256) stw[e] = e < M ? twm[e] : twn[e - M];
+    __syncthreads();
     const int r0 = blockIdx.x * group;
     const int nr = min(group, nrows - r0);
-    for (int e = threadIdx.x; e < nr * M; e += blockDim.x) {
+    for (int e = threadIdx.x; e < nr * M; e += 256) {
         const int r = e / M, k = e % M;
-        fill_real_inverse(buf, lay, r, X + ((size_t)j0 * d.nz + r0 + r) * d.ldx, M, d.nkx, twn, k);
+        fill_real_inverse(buf, lay, r, X + ((size_t)j0 * d.nz + r0 + r) * d.ldx, M, d.nkx, stw + M, k);
     }
     __syncthreads();
-    smem_fft<double, RT_VMAX>(buf, nr, lay, pm, twm, +1);
-    for (int e = threadIdx.x; e < nr * M; e += blockDim.x) {
+    row_fft<double, MC, +1>(buf, nr, lay, pm, stw);
+    for (int e = threadIdx.x; e < nr * M; e += 256) {
         const int r = e / M, m = e % M;
         const cpx<double> v = buf[lay.at(m, r)];
-        double* dst = P + ((size_t)j0 * d.nz + r0 + r) * d.nx + 2 * m;
-        dst[0] = v.x;
-        dst[1] = v.y;
+        double2* dst = reinterpret_cast<double2*>(P + ((size_t)j0 * d.nz + r0 + r) * d.nx) + m;
+        *dst = make_double2(v.x, v.y);
     }
 }
 
+template <int MC>
 __global__ void __launch_bounds__(256) k_xfwd(Dims d, const double* __restrict__ P,
                                               cpx<double>* __restrict__ X, int j0, int nrows, int group,
                                               FftPlan pm, const cpx<double>* __restrict__ twm,
                                               const cpx<double>* __restrict__ twn) {
-    extern __shared__ unsigned char smem_raw[];
-    cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
-    const int M = d.nx / 2;
-    RowLayoutRT lay{row_pitch(M)};
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int M = MC > 0 ? MC : d.nx / 2;
+    using Lay = typename std::conditional<(MC > 0), RowLayoutCT<MC>, RowLayoutRT>::type;
+    Lay lay;
+    if constexpr (MC == 0) lay.pitch = row_pitch(M);
+    cpx<double>* stw = reinterpret_cast<cpx<double>*>(smem_raw);
+    cpx<double>* buf = stw + 3 * M;
+    for (int e = threadIdx.x; e < 3 * M; e += 256) stw[e] = e < M ? twm[e] : twn[e - M];
     const int r0 = blockIdx.x * group;
     const int nr = min(group, nrows - r0);
-    for (int e = threadIdx.x; e < nr * M; e += blockDim.x) {
+    for (int e = threadIdx.x; e < nr * M; e += 256) {
         const int r = e / M, m = e % M;
-        const double* src = P + ((size_t)j0 * d.nz + r0 + r) * d.nx + 2 * m;
-        buf[lay.at(m, r)] = mk<double>(src[0], src[1]);
+        const double2 v = reinterpret_cast<const double2*>(P + ((size_t)j0 * d.nz + r0 + r) * d.nx)[m];
+        buf[lay.at(m, r)] = mk<double>(v.x, v.y);
     }
     __syncthreads();
-    smem_fft<double, RT_VMAX>(buf, nr, lay, pm, twm, -1);
-    for (int e = threadIdx.x; e < nr * d.ldx; e += blockDim.x) {
+    row_fft<double, MC, -1>(buf, nr, lay, pm, stw);
+    for (int e = threadIdx.x; e < nr * d.ldx; e += 256) {
         const int r = e / d.ldx, k = e % d.ldx;
         X[((size_t)j0 * d.nz + r0 + r) * d.ldx + k] =
-            extract_real_forward(buf, lay, r, M, d.nkx, twn, k, 1.0 / (double)d.nx);
+            extract_real_forward(buf, lay, r, M, d.nkx, stw + M, k, 1.0 / (double)d.nx);
     }
 }
 
@@ -649,31 +661,54 @@ static int api_group(int nx) {
     return g > 8 ? 8 : g;
 }
 
-cudaError_t launch_xinv(const Dims& d, const void* X, double* P, int j0, int nplanes, const FftPlan& pm,
-                        const void* twm, const void* twn, cudaStream_t st) {
-    const int group = api_group(d.nx);
+static bool ct_length(int m) {
+    switch (m) {
+#define CASE(N) case N: return true;
+        DGPU_M_LIST(CASE)
+#undef CASE
+        default: return false;
+    }
+}
+
+template <bool INV>
+static cudaError_t launch_xapi(const Dims& d, const void* src, void* dst, int j0, int nplanes, const FftPlan& pm,
+                               const void* twm, const void* twn, cudaStream_t st) {
+    const int M = d.nx / 2;
+    const int group = ct_length(M) ? PROD_G : api_group(d.nx);
     const int nrows = nplanes * d.nz;
     if (nrows <= 0) return cudaSuccess;
-    const size_t smem = sizeof(cpx<double>) * (size_t)group * row_pitch(d.nx / 2);
-    cudaFuncSetAttribute(k_xinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_xinv<<<(nrows + group - 1) / group, 256, smem, st>>>(d, (const cpx<double>*)X, P, j0, nrows, group, pm,
-                                                          (const cpx<double>*)twm, (const cpx<double>*)twn);
+    const size_t smem = sizeof(cpx<double>) * ((size_t)group * row_pitch(M) + 3 * (size_t)M);
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if constexpr (INV)
+            kern<<<(nrows + group - 1) / group, 256, smem, st>>>(d, (const cpx<double>*)src, (double*)dst, j0, nrows,
+                                                                group, pm, (const cpx<double>*)twm,
+                                                                (const cpx<double>*)twn);
+        else
+            kern<<<(nrows + group - 1) / group, 256, smem, st>>>(d, (const double*)src, (cpx<double>*)dst, j0, nrows,
+                                                                group, pm, (const cpx<double>*)twm,
+                                                                (const cpx<double>*)twn);
+    };
+    switch (M) {
+#define CASE(N) case N: if constexpr (INV) go(k_xinv<N>); else go(k_xfwd<N>); break;
+        DGPU_M_LIST(CASE)
+#undef CASE
+        default: if constexpr (INV) go(k_xinv<0>); else go(k_xfwd<0>); break;
+    }
     return cudaGetLastError();
+}
+
+cudaError_t launch_xinv(const Dims& d, const void* X, double* P, int j0, int nplanes, const FftPlan& pm,
+                        const void* twm, const void* twn, cudaStream_t st) {
+    return launch_xapi<true>(d, X, P, j0, nplanes, pm, twm, twn, st);
 }
 
 cudaError_t launch_xfwd(const Dims& d, const double* P, void* X, int j0, int nplanes, const FftPlan& pm,
                         const void* twm, const void* twn, cudaStream_t st) {
-    const int group = api_group(d.nx);
-    const int nrows = nplanes * d.nz;
-    if (nrows <= 0) return cudaSuccess;
-    const size_t smem = sizeof(cpx<double>) * (size_t)group * row_pitch(d.nx / 2);
-    cudaFuncSetAttribute(k_xfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_xfwd<<<(nrows + group - 1) / group, 256, smem, st>>>(d, P, (cpx<double>*)X, j0, nrows, group, pm,
-                                                          (const cpx<double>*)twm, (const cpx<double>*)twn);
-    return cudaGetLastError();
+    return launch_xapi<false>(d, P, X, j0, nplanes, pm, twm, twn, st);
 }
 
-template <int TX>
+template <int NC, int TX>
 __global__ void __launch_bounds__(256) k_zfwd_pack(Dims d, const cpx<double>* __restrict__ X,
                                                    double2* __restrict__ S, int j0, FftPlan pz,
                                                    const cpx<double>* __restrict__ twz) {
@@ -688,7 +723,7 @@ __global__ void __launch_bounds__(256) k_zfwd_pack(Dims d, const cpx<double>* __
         buf[e] = src[(size_t)z * d.ldx + c];
     }
     __syncthreads();
-    col_fft<double, 0, TX, -1>(buf, pz, twz);
+    col_fft<double, NC, TX, -1>(buf, pz, twz);
     const double inv_nz = 1.0 / (double)nz;
     double2* dst = S + (size_t)J * d.splane() + kx0;
     for (int e = threadIdx.x; e < d.nkzt * TX; e += blockDim.x) {
@@ -703,9 +738,17 @@ cudaError_t launch_zfwd_pack(const Dims& d, const void* X, double2* S, int j0, i
     constexpr int TX = ZTile<double>::TX;
     if (nplanes <= 0) return cudaSuccess;
     const size_t smem = sizeof(cpx<double>) * (size_t)d.nz * TX;
-    cudaFuncSetAttribute(k_zfwd_pack<TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid(d.ldx / TX, nplanes);
-    k_zfwd_pack<TX><<<grid, 256, smem, st>>>(d, (const cpx<double>*)X, S, j0, pz, (const cpx<double>*)twz);
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 256, smem, st>>>(d, (const cpx<double>*)X, S, j0, pz, (const cpx<double>*)twz);
+    };
+    switch (d.nz) {
+#define CASE(N) case N: go(k_zfwd_pack<N, TX>); break;
+        DGPU_NZ_LIST(CASE)
+#undef CASE
+        default: go(k_zfwd_pack<0, TX>); break;
+    }
     return cudaGetLastError();
 }
 
