@@ -10,7 +10,9 @@ products in FP32, solves, state and the projection in FP64).  Besides the
 device-timed value the line carries: the all-FP64 path's steps/s and its
 difference from the FP32-split state after the same steps, the end-to-end
 rate through the C ABI with host buffers, the roofline of the dominant
-kernel, a CPU baseline and the SM clocks seen during the timed region.
+kernel, a CPU baseline, the SM clocks seen during the timed region, the
+batched form, and the constant-Smagorinsky LES step against the FP64 DNS
+step.
 
 Multi-GPU: independent replicas, one process per GPU (torchrun); no data-path
 collective (the single-instance path does not shard).  The reference arm
@@ -60,6 +62,7 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-les", action="store_true")
     ap.add_argument("--error-steps", type=int, default=500,
                     help="steps after which FP32-split is compared with FP64 (besides 100)")
     return ap.parse_args()
@@ -294,6 +297,57 @@ def batched_rates(steps: int, n: int = 64) -> dict:
             "timing": "wall clock around synchronised calls"}
 
 
+def les_rates(w, u, th, steps: int, warmup: int, torch, cpu: bool) -> dict:
+    """The constant-Smagorinsky LES branch (LES_MODEL_TYPE 1, CREATE_NEW_FLOW
+    off so the model runs from the first step) on the same grid and fields,
+    FP64, against the FP64 DNS step; device time on the library's stream.
+    With cpu, the oracle's LES step on the bounded y-sample of cpu_sample."""
+    from diablo_b200.params import PREC_FP64
+    from diablo_b200.channel import Channel
+
+    out = {"workload": "same grid and initial fields, LES=1, LES_MODEL_TYPE=1 (C_s=0.13), "
+                       "CREATE_NEW_FLOW=F, FP64"}
+    for les in (0, 1):
+        p = w.p.copy()
+        p.precision = PREC_FP64
+        p.les, p.les_model_type, p.create_new_flow = les, 1, 0
+        c = Channel(p, w.grid, w.dt)
+        c.init_from_physical(u, th)
+        c.step(warmup)
+        n0 = c.kernel_launches()
+        ms = timed_steps(c, steps, torch)
+        launches = c.kernel_launches() - n0
+        key = "les" if les else "dns"
+        out[f"{key}_steps_per_s"] = steps / (ms / 1e3)
+        out[f"{key}_ms_per_step"] = ms / steps
+        out[f"{key}_gpu_launches_per_step"] = launches / steps
+        if les:
+            out["nu_t_max"] = float(c.download_nu_t().max())
+        c.close()
+    out["les_cost_vs_dns"] = out["les_ms_per_step"] / out["dns_ms_per_step"]
+    if cpu:
+        from diablo_b200 import workloads
+        from oracle.oracle import Oracle
+        nx, ny, nz = w.p.nx, w.p.ny, w.p.nz
+        nys = min(SAMPLE_NY, ny)
+        ws = workloads.precision(nx, nys, nz)
+        p = ws.p.copy()
+        p.les, p.les_model_type, p.create_new_flow = 1, 1, 0
+        o = Oracle(p, ws.grid, ws.dt)
+        uu, tt = ws.initial_fields()
+        o.init_from_physical(uu, tt)
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(1)
+        el = time.perf_counter() - t0
+        scale = (ny + 2) / (nys + 2)
+        cores = os.cpu_count() or 1
+        out["cpu_baseline"] = {"value": 1.0 / (el * scale), "unit": "steps/s", "cores": cores, "kind": "port",
+                               "sample": f"1 LES RK3 step of {nx}x{nys}x{nz}, {el:.3f} s scaled x{scale:.2f}; "
+                                         f"OpenMP on {cores} threads"}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from diablo_b200 import build, workloads
@@ -372,6 +426,11 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_batched:
         batched = batched_rates(max(3, min(args.steps, 20)))
 
+    les = None
+    if not args.no_les:
+        les = les_rates(w, u, th, max(3, min(args.steps, 20)), 3, torch,
+                        cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
+
     peak, peak_kind = hbm_peak()
     alg = algorithmic_bytes(w.p, "fp32split")
     dom = max(ktimes, key=lambda k: ktimes[k][1])
@@ -406,7 +465,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(), "fp64": fp64,
         "fp32_split_speedup_vs_fp64": (value / world) / fp64["steps_per_s"] if fp64 else None,
-        "kernel_ms_per_step": kernel_ms, "batched": batched,
+        "kernel_ms_per_step": kernel_ms, "batched": batched, "les": les,
     }
     print(json.dumps(line), flush=True)
 
