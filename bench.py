@@ -63,6 +63,8 @@ def parse_args():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-les", action="store_true")
+    ap.add_argument("--only", choices=["les"], default=None,
+                    help="run one leg alone and print its JSON (for profiling captures)")
     ap.add_argument("--error-steps", type=int, default=500,
                     help="steps after which FP32-split is compared with FP64 (besides 100)")
     return ap.parse_args()
@@ -363,6 +365,15 @@ def run_ours(args, rank, world, local_rank):
                                 device_id=torch.device("cuda", local_rank))
     nx, ny, nz = (int(v) for v in args.grid.split(","))
     w = workloads.precision(nx, ny, nz)
+    if args.only == "les":
+        u, th = w.initial_fields()
+        out = les_rates(w, u, th, args.steps, args.warmup, torch, cpu=False)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"grid": [nx, ny, nz], "les": out}), flush=True)
+        return
     try:
         uuid = str(torch.cuda.get_device_properties(local_rank).uuid)
     except Exception:
