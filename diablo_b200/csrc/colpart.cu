@@ -773,7 +773,172 @@ __global__ void __launch_bounds__(128) k_phi_part(Dims d, const double* __restri
     pt[PB_RBT * NPART + k] = rcp_guard(be);
 }
 
+// ---------------------------------------------------------------------------
+// REM_DIV_CHAN on its own (channel.f:1103-1214, with the rows of
+// APPLY_BC_REM_DIV_MPI, mpi.f:1239-1278) and the pressure update
+// CP += phi/h (channel.f:1059-1065): the projection step of k_colpart
+// without the CN solves.  Four adjacent columns per block; CU1..CU3 of the
+// four are staged row by row (64-byte runs), warp c solves column c's phi
+// system by the partition method with the column's factors from
+// k_phi_part, and the corrections are written back row-parallel.
+// Shared memory: [3][NROW][4] velocity (staged with cp.async, all rows in
+// flight at once), [NROW][4] phi.
+// ---------------------------------------------------------------------------
+template <int RC>
+__global__ void __launch_bounds__(128) k_proj(RemDivArgs a) {
+    constexpr int NROW = NPART * RC;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* sV = reinterpret_cast<double2*>(smem);   // [3][NROW][4]
+    double2* sPh = sV + 3 * NROW * 4;                 // [NROW][4]
+    const Dims& d = a.d;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ny = d.ny, nyp = d.nyp;
+    const size_t ps = d.splane(), fs = ps * d.nyp;
+    const size_t g0 = (size_t)blockIdx.x * 4;
+    const double2 zero = make_double2(0.0, 0.0);
+    const double* RDY = a.rows + RT_RDY * nyp;
+    const double* RDYF = a.rows + RT_RDYF * nyp;
+    const double* E1P = a.rows + RT_E1P * nyp;
+    const double* E1M = a.rows + RT_E1M * nyp;
+    auto live = [&](int c) {
+        const size_t g = g0 + c;
+        return (int)(g % d.ldx) < d.nkxp && (int)(g / d.ldx) < d.nkzt;
+    };
+    for (int e = tid; e < 3 * nyp * 4; e += 128) {
+        const int c = e & 3, r = e >> 2;
+        const int j = r % nyp, f = r / nyp;
+        cp_async16(sV + ((size_t)f * NROW + j) * 4 + c, a.cu + (size_t)f * fs + (size_t)j * ps + g0 + c);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    {
+        const int c = warp, k = lane;
+        const size_t g = g0 + c;
+        const int kx = (int)(g % d.ldx), m = (int)(g / d.ldx);
+        if (live(c)) {
+            const bool zero_mode = (kx == 0 && m == 0);
+            const double KX = a.kx[kx], KZ = a.kz[m];
+            const double K2 = KX * KX + KZ * KZ;
+            auto coef = [&](int j, double& A_, double& B_, double& C_) {
+                A_ = 0.0; B_ = 1.0; C_ = 0.0;
+                if (j == ny) { A_ = 1.0; B_ = -1.0; }
+                else if (j == 1) { C_ = zero_mode ? 0.0 : -1.0; }
+                else if (j >= 2 && j < ny) { A_ = E1M[j]; B_ = -K2 - E1P[j] - E1M[j]; C_ = E1P[j]; }
+            };
+            auto V = [&](int f, int j) { return sV[((size_t)f * NROW + j) * 4 + c]; };
+            const int jb = k * RC;
+            double2 y[RC];
+#pragma unroll
+            for (int r = 0; r < RC; ++r) {
+                const int j = jb + r;
+                double2 G = zero;
+                if (j >= 2 && j < ny) G = ik(KX, V(0, j)) + RDYF[j] * (V(1, j + 1) - V(1, j)) + ik(KZ, V(2, j));
+                y[r] = G;
+            }
+            double rb[RC], pp[RC], qq[RC];
+            {
+                double A_, B_, C_, Cp;
+                coef(jb + 1, A_, B_, C_);
+                double beta = B_;
+                rb[1] = rcp_nr(beta);
+                pp[1] = -A_;
+                Cp = C_;
+#pragma unroll
+                for (int r = 2; r <= RC - 2; ++r) {
+                    coef(jb + r, A_, B_, C_);
+                    const double mlt = A_ * rb[r - 1];
+                    beta = B_ - mlt * Cp;
+                    rb[r] = rcp_nr(beta);
+                    y[r] = y[r] - mlt * y[r - 1];
+                    pp[r] = -mlt * pp[r - 1];
+                    Cp = C_;
+                }
+                y[RC - 2] = rb[RC - 2] * y[RC - 2];
+                pp[RC - 2] = rb[RC - 2] * pp[RC - 2];
+                qq[RC - 2] = -Cp * rb[RC - 2];
+#pragma unroll
+                for (int r = RC - 3; r >= 1; --r) {
+                    coef(jb + r, A_, B_, C_);
+                    y[r] = rb[r] * (y[r] - C_ * y[r + 1]);
+                    pp[r] = rb[r] * (pp[r] - C_ * pp[r + 1]);
+                    qq[r] = -C_ * qq[r + 1] * rb[r];
+                }
+            }
+            double2 Ds, De;
+            {
+                double A_, B_, C_;
+                coef(jb, A_, B_, C_);
+                Ds = y[0] - C_ * y[1];
+                coef(jb + RC - 1, A_, B_, C_);
+                De = y[RC - 1] - A_ * y[RC - 2];
+            }
+            const double* pt = a.phitab + g * (NPART * 16);
+            const double2 Dsn = shfl_dn2(Ds, 1);
+            double2 rk = De - pt[PB_W1 * NPART + k] * Ds - pt[PB_W2 * NPART + k] * Dsn;
+#pragma unroll
+            for (int st = 0; st < NPCR; ++st) {
+                const int sg = 1 << st;
+                const double2 rl = shfl_up2(rk, sg);
+                const double2 rh = shfl_dn2(rk, sg);
+                rk = rk - pt[(PB_PA0 + st) * NPART + k] * rl - pt[(PB_PG0 + st) * NPART + k] * rh;
+            }
+            const double2 t = pt[PB_RBT * NPART + k] * rk;
+            double2 tp = shfl_up2(t, 1);
+            if (k == 0) tp = zero;
+            const double2 u = pt[PB_RBS * NPART + k] * Ds - pt[PB_AS * NPART + k] * tp - pt[PB_CS * NPART + k] * t;
+#pragma unroll
+            for (int r = 0; r < RC; ++r) {
+                const int j = jb + r;
+                double2 phi = (r == 0) ? u : (r == RC - 1) ? t : y[r] + pp[r] * u + qq[r] * t;
+                if (j < 1 || j > ny) phi = zero;
+                sPh[j * 4 + c] = phi;
+            }
+        }
+    }
+    __syncthreads();
+    // corrected velocity (rows 1..NY; CU2 rows 2..NY), CP += phi/h (rows
+    // 2..NY) and phi (rows 1..NY), row-parallel
+    for (int e = tid; e < 5 * ny * 4; e += 128) {
+        const int c = e & 3, r = e >> 2;
+        const int j = 1 + r % ny, q = r / ny;
+        if (!live(c)) continue;
+        const size_t g = g0 + c;
+        const size_t o = (size_t)j * ps + g;
+        const double2 phi = sPh[j * 4 + c];
+        if (q == 0) {
+            a.cu[o] = sV[((size_t)0 * NROW + j) * 4 + c] - ik(a.kx[g % d.ldx], phi);
+        } else if (q == 2) {
+            a.cu[2 * fs + o] = sV[((size_t)2 * NROW + j) * 4 + c] - ik(a.kz[g / d.ldx], phi);
+        } else if (q == 1) {
+            if (j >= 2) a.cu[fs + o] = sV[((size_t)1 * NROW + j) * 4 + c] - RDY[j] * (phi - sPh[(j - 1) * 4 + c]);
+        } else if (q == 3) {
+            if (a.update_cp && j >= 2) a.cp[o] = a.cp[o] + a.inv_h * phi;
+        } else {
+            a.phi[o] = phi;
+        }
+    }
+}
+
 size_t phi_table_doubles(const Dims& d) { return d.splane() * (size_t)(NPART * 16); }
+
+cudaError_t launch_remdiv(const RemDivArgs& a, cudaStream_t st) {
+    const Dims& d = a.d;
+    const int RC = part_rows(d.nyp);
+    const size_t smem = sizeof(double2) * 4 * (size_t)NPART * RC * 4;
+    const unsigned nblk = (unsigned)(d.splane() / 4);
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<nblk, 128, smem, st>>>(a);
+    };
+    switch (RC) {
+        case 3: go(k_proj<3>); break;
+        case 5: go(k_proj<5>); break;
+        case 9: go(k_proj<9>); break;
+        case 17: go(k_proj<17>); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launch_phi_part(const Dims& d, const double* rows, const double* kx, const double* kz, double* tab,
                             cudaStream_t st) {

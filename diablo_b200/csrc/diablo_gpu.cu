@@ -561,8 +561,8 @@ static int rem_div(Handle* h, int update_cp, double inv_h) {
     a.cu = h->cu;
     a.cp = h->cp;
     a.phi = h->phi;
-    a.bsc = h->bsc;
-    a.gsc = h->gsc;
+    a.rows = h->d_rows;
+    a.phitab = h->d_phitab;
     a.kx = h->d_kx;
     a.kz = h->d_kz;
     a.dy = h->d_dy;

@@ -93,8 +93,8 @@ struct RemDivArgs {
     double2* cu;          // S, velocity fields 0..2
     double2* cp;          // S
     double2* phi;         // S, phi (J = 1..NY)
-    double* bsc;          // scratch pivots  [J][m][kx]
-    double2* gsc;         // scratch RHS     [J][m][kx]
+    const double* rows;   // [RT_COUNT][nyp] reciprocal row tables
+    const double* phitab; // per-column phi partition factors (k_phi_part)
     const double* kx;
     const double* kz;
     const double* dy;
