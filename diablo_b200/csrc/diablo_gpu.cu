@@ -68,6 +68,7 @@ struct Handle {
     // the nf right-hand sides), the x-spectrum work lx and the filter widths
     // Delta_YF, Delta_Y ([2][nyp])
     double *nut = nullptr, *lu = nullptr, *la = nullptr, *lb = nullptr, *d_delta = nullptr;
+    double* d_dyn = nullptr;      // dynamic model: [2][nyp] plane sums, [2][nyp] widths
     double2 *ls = nullptr, *lr = nullptr;
     void* lx = nullptr;
     bool nut_set = false;         // NU_T has been computed at least once
@@ -135,7 +136,7 @@ void free_handle(Handle* h) {
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
                     h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_tabs, h->d_phitab,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
-                    h->twz_f, h->nut, h->lu, h->la, h->lb, h->d_delta, h->ls, h->lr, h->lx};
+                    h->twz_f, h->nut, h->lu, h->la, h->lb, h->d_delta, h->ls, h->lr, h->lx, h->d_dyn};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (h->st) cudaStreamDestroy(h->st);
@@ -269,8 +270,10 @@ int validate(const diablo_params* p) {
     if (p->ny < 4) return fail(DIABLO_EINVAL, "NY must be >= 4");
     if (p->n_th < 0 || p->n_th > DIABLO_MAX_TH) return fail(DIABLO_EINVAL, "N_TH must be in 0..4");
     if (p->les) {
-        // les.f:269-272 stops for the dynamic models
-        if (p->les_model_type != 1) return fail(DIABLO_ENOTSUP, "LES_MODEL_TYPE must be 1 (constant Smagorinsky)");
+        // 1: constant Smagorinsky (les.f); 2: this library's dynamic model; the
+        // reference stops for 2 and 3 (les.f:269-272)
+        if (p->les_model_type != 1 && p->les_model_type != 2)
+            return fail(DIABLO_ENOTSUP, "LES_MODEL_TYPE must be 1 (constant) or 2 (dynamic Smagorinsky)");
         if (p->precision != DIABLO_PREC_FP64) return fail(DIABLO_ENOTSUP, "the LES branch runs in FP64 only");
     }
     auto bc01 = [](int t) { return t == 0 || t == 1; };
@@ -425,6 +428,7 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
         if (e == cudaSuccess) e = dmalloc((void**)&h->lr, sb * d.nf);
         if (e == cudaSuccess) e = dmalloc(&h->lx, sizeof(double2) * h->x_field * nw);
         if (e == cudaSuccess) e = dmalloc((void**)&h->d_delta, sizeof(double) * 2 * nyp);
+        if (e == cudaSuccess) e = dmalloc((void**)&h->d_dyn, sizeof(double) * 4 * nyp);
     }
     if (e != cudaSuccess) {
         free_handle(h);
@@ -704,8 +708,10 @@ static int les_substage(Handle* h, int rk_step, int time_step, double time, doub
     const int r = rk_step - 1;
     const size_t pf = (size_t)d.nyp * d.nz * d.nx;
     const int nyp = d.nyp;
-    const double* delta_yf = h->d_delta;
-    const double* delta_y = h->d_delta + nyp;
+    // filter widths with -2 C^2 absorbed: the constant model's, or the
+    // dynamic model's of this substage
+    const double* delta_yf = p.les_model_type == 2 ? h->d_dyn + 2 * nyp : h->d_delta;
+    const double* delta_y = delta_yf + nyp;
     CnArgs a = substage_args(h, rk_step, time, h_bar, beta_bar, zeta_bar);
     ProfScope ps(h, DIABLO_KERNEL_OTHER);
     CK(launch_les_pre(a, h->d_k2, h->lr, h->st));
@@ -720,6 +726,11 @@ static int les_substage(Handle* h, int rk_step, int time_step, double time, doub
         h->launches += 3;
         CK(les_to_phys(h, h->ls, 6, h->la, 0, nyp));
         CK(les_to_phys(h, h->cu, 3, h->lu, 0, nyp));
+        if (p.les_model_type == 2) {
+            CK(launch_dyn_widths(d, h->la, h->lu, h->cu, h->d_dy, h->d_dyf, std::pow(9.0, 2.0 / 3.0), h->d_dyn,
+                                 h->d_dyn + 2 * nyp, h->st));
+            h->launches += 2;
+        }
         CK(launch_les_sgs(d, h->la, h->lu, h->cu, h->d_dy, h->d_dyf, delta_y, h->lb, h->nut, h->st));
         CK(launch_phys_bc_vel(d, h->lu, h->d_dy, h->d_dyf, p, h->st));
         h->launches += 2;

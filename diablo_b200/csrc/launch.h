@@ -112,6 +112,11 @@ cudaError_t launch_les_explicit(const LesArgs& a, const double* u, double* r, co
 // nf fields of pivots, out receives the solution rows.
 cudaError_t launch_les_solve(const LesArgs& a, double* r, const double* nut, double* piv, double* out,
                              cudaStream_t st);
+// Dynamic Smagorinsky widths: plane sums of L_ij M_ij and M_ij M_ij (sums,
+// 2*(NY+2) doubles, zeroed here), then widths[0..NY+1] = Delta_YF and
+// widths[NY+2..] = Delta_Y.  sij: the six physical strain fields, u: U1..U3.
+cudaError_t launch_dyn_widths(const Dims& d, const double* sij, const double* u, const double2* cu, const double* dy,
+                              const double* dyf, double R, double* sums, double* widths, cudaStream_t st);
 // COURANT's velocity minimum over physical rows 1..NY of U1..U3 (u: 3 fields).
 cudaError_t launch_les_cfl(const Dims& d, const double* u, const double* dy, double cfl, double dx, double dz,
                            double* dtmin, cudaStream_t st);

@@ -462,6 +462,136 @@ __global__ void __launch_bounds__(TB) k_les_solve(LesArgs a, double* __restrict_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Dynamic Smagorinsky (LES_MODEL_TYPE 2).  The reference stops for this model
+// type (les.f:269-272); the model is this library's: Germano's identity with
+// Lilly's least squares over each x-z plane at GYF points J = 2..NY,
+//   L_ij = (u_i u_j)^ - u^_i u^_j,  M_ij = R |S^| S^_ij - (|S| S_ij)^,
+//   (C Delta^2)(J) = max(0, -<L_ij M_ij> / (2 <M_ij M_ij>)),
+// ^ the 5-point test filter of les_filter_chan (les.f:572-712) in x then z,
+// R = (Delta^/Delta)^2, |S| and |S^| with the mean shear removed.
+//
+// k_dyn_sums: one block per (32 x-points, 8 z-points, plane).  The ten base
+// values of the 36 x 12 points the stencils reach (periodic) are computed
+// into shared memory; the x-filtered 21 quantities of the 32 x 12 points
+// follow; each thread z-filters its point, forms L_ij M_ij and M_ij M_ij,
+// and the block's sums are added to the plane's.
+// ---------------------------------------------------------------------------
+constexpr int DX_T = 32, DZ_T = 8, DX_S = DX_T + 4, DZ_S = DZ_T + 4, NB = 10, NQ = 21;
+
+__global__ void __launch_bounds__(256) k_dyn_sums(Dims d, const double* __restrict__ sij, const double* __restrict__ u,
+                                                  const double2* __restrict__ cu, const double* __restrict__ dy,
+                                                  double R, double* __restrict__ sums) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* sb = reinterpret_cast<double*>(smem);   // [NB][DZ_S][DX_S]
+    double* sx = sb + NB * DZ_S * DX_S;              // [NQ][DZ_S][DX_T]
+    __shared__ double red[2][8];
+    const int nx = d.nx, nz = d.nz;
+    const int i0 = blockIdx.x * DX_T, k0 = blockIdx.y * DZ_T, J = 2 + blockIdx.z;
+    const size_t pp = plane_pts(d), pf = pp * d.nyp;
+    const size_t ps = d.splane(), fs = ps * d.nyp;
+    auto ub = [&](int c, int j) { return cu[(size_t)c * fs + (size_t)j * ps].x; };
+    const double dm1 = 0.5 * (ub(0, J) - ub(0, J - 1)) / dy[J], dp1 = 0.5 * (ub(0, J + 1) - ub(0, J)) / dy[J + 1];
+    const double dm3 = 0.5 * (ub(2, J) - ub(2, J - 1)) / dy[J], dp3 = 0.5 * (ub(2, J + 1) - ub(2, J)) / dy[J + 1];
+    const double m1 = dm1 + dp1, m3 = dm3 + dp3;
+    for (int e = threadIdx.x; e < DZ_S * DX_S; e += 256) {
+        const int kk = e / DX_S, ii = e % DX_S;
+        const int i = (i0 - 2 + ii + nx) % nx, k = (k0 - 2 + kk + nz) % nz;
+        const size_t c = (size_t)k * nx + i;
+        auto S = [&](int q, int j) { return sij[(size_t)q * pf + (size_t)j * pp + c]; };
+        auto U = [&](int q, int j) { return u[(size_t)q * pf + (size_t)j * pp + c]; };
+        const double s11 = S(0, J), s22 = S(1, J), s33 = S(2, J), s13 = S(4, J);
+        const double a4 = 0.5 * (S(3, J + 1) + S(3, J) - dm1 - dp1);
+        const double a6 = 0.5 * (S(5, J + 1) + S(5, J) - dm3 - dp3);
+        const double sm = sqrt(2.0 * (s11 * s11) + 4.0 * (a4 * a4) + 4.0 * (s13 * s13) + 2.0 * (s22 * s22) +
+                               4.0 * (a6 * a6) + 2.0 * (s33 * s33));
+        const double v[NB] = {U(0, J), 0.5 * (U(1, J) + U(1, J + 1)), U(2, J), s11, s22, s33,
+                              0.5 * (S(3, J) + S(3, J + 1)), s13, 0.5 * (S(5, J) + S(5, J + 1)), sm};
+#pragma unroll
+        for (int q = 0; q < NB; ++q) sb[(q * DZ_S + kk) * DX_S + ii] = v[q];
+    }
+    __syncthreads();
+    // the 21 quantities of each point, filtered in x (les.f:656-662 order)
+    const double W[5] = {1.0 / 8.0, 1.0 / 4.0, 1.0 / 4.0, 1.0 / 4.0, 1.0 / 8.0};
+    for (int e = threadIdx.x; e < DZ_S * DX_T; e += 256) {
+        const int kk = e / DX_T, tx = e % DX_T;
+        double acc[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+#pragma unroll
+        for (int t = 0; t < 5; ++t) {
+            const int ii = tx + t;
+            double b[NB];
+#pragma unroll
+            for (int q = 0; q < NB; ++q) b[q] = sb[(q * DZ_S + kk) * DX_S + ii];
+            const double v[NQ] = {b[0], b[1], b[2], b[0] * b[0], b[1] * b[1], b[2] * b[2], b[0] * b[1], b[0] * b[2],
+                                  b[1] * b[2], b[3], b[4], b[5], b[6], b[7], b[8],
+                                  b[9] * b[3], b[9] * b[4], b[9] * b[5], b[9] * b[6], b[9] * b[7], b[9] * b[8]};
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) acc[q] = t == 0 ? W[0] * v[q] : acc[q] + W[t] * v[q];
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) sx[(q * DZ_S + kk) * DX_T + tx] = acc[q];
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % DX_T, tz = threadIdx.x / DX_T;
+    double num = 0.0, den = 0.0;
+    if (i0 + tx < nx && k0 + tz < nz) {
+        double h[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double a = W[0] * sx[(q * DZ_S + tz) * DX_T + tx];
+#pragma unroll
+            for (int t = 1; t < 5; ++t) a = a + W[t] * sx[(q * DZ_S + tz + t) * DX_T + tx];
+            h[q] = a;
+        }
+        const double a12 = h[12] - 0.5 * m1, a23 = h[14] - 0.5 * m3;
+        const double sh = sqrt(2.0 * (h[9] * h[9]) + 4.0 * (a12 * a12) + 4.0 * (h[13] * h[13]) + 2.0 * (h[10] * h[10]) +
+                               4.0 * (a23 * a23) + 2.0 * (h[11] * h[11]));
+        const double L11 = h[3] - h[0] * h[0], L22 = h[4] - h[1] * h[1], L33 = h[5] - h[2] * h[2];
+        const double L12 = h[6] - h[0] * h[1], L13 = h[7] - h[0] * h[2], L23 = h[8] - h[1] * h[2];
+        const double M11 = R * sh * h[9] - h[15], M22 = R * sh * h[10] - h[16], M33 = R * sh * h[11] - h[17];
+        const double M12 = R * sh * h[12] - h[18], M13 = R * sh * h[13] - h[19], M23 = R * sh * h[14] - h[20];
+        num = L11 * M11 + L22 * M22 + L33 * M33 + 2.0 * (L12 * M12 + L13 * M13 + L23 * M23);
+        den = M11 * M11 + M22 * M22 + M33 * M33 + 2.0 * (M12 * M12 + M13 * M13 + M23 * M23);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        num += __shfl_down_sync(0xffffffffu, num, o);
+        den += __shfl_down_sync(0xffffffffu, den, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { red[0][w] = num; red[1][w] = den; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int q = 0; q < 8; ++q) { a += red[0][q]; b += red[1][q]; }
+        atomicAdd(sums + 2 * J, a);
+        atomicAdd(sums + 2 * J + 1, b);
+    }
+}
+
+// (C Delta^2)(J) from the plane sums, then the widths that replace the
+// constant model's: Delta_YF = -2 C Delta^2 at GYF points, Delta_Y its
+// interpolation to GY points (the end planes take the nearest value).
+__global__ void k_dyn_widths(Dims d, const double* __restrict__ sums, const double* __restrict__ dy,
+                             const double* __restrict__ dyf, double* __restrict__ widths) {
+    const int ny = d.ny, nyp = d.nyp;
+    auto cd = [&](int j) {
+        j = j < 2 ? 2 : j > ny ? ny : j;
+        const double num = sums[2 * j], den = sums[2 * j + 1];
+        const double c = den > 0.0 ? -0.5 * num / den : 0.0;
+        return c > 0.0 ? c : 0.0;
+    };
+    for (int j = threadIdx.x; j < nyp; j += blockDim.x) {
+        widths[j] = j >= 1 ? -2.0 * cd(j) : 0.0;
+        double cg = 0.0;
+        if (j >= 3 && j <= ny) cg = (cd(j) * dyf[j - 1] + cd(j - 1) * dyf[j]) / (2.0 * dy[j]);
+        else if (j == 2 || j == ny + 1) cg = cd(j);
+        widths[nyp + j] = j >= 2 ? -2.0 * cg : 0.0;
+    }
+}
+
 // COURANT's velocity limit (courant.f:35-47) over physical rows 1..NY of the
 // fields the physical solves left (they are not band-limited, so the limit
 // is taken on them rather than on their transforms).  Non-negative doubles
@@ -557,6 +687,20 @@ cudaError_t launch_les_solve(const LesArgs& a, double* r, const double* nut, dou
                              cudaStream_t st) {
     dim3 grid(blocks(plane_pts(a.d)), a.d.nf);
     k_les_solve<<<grid, TB, 0, st>>>(a, r, nut, piv, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dyn_widths(const Dims& d, const double* sij, const double* u, const double2* cu, const double* dy,
+                              const double* dyf, double R, double* sums, double* widths, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(sums, 0, sizeof(double) * 2 * d.nyp, st);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(double) * ((size_t)NB * DZ_S * DX_S + (size_t)NQ * DZ_S * DX_T);
+    cudaFuncSetAttribute(k_dyn_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid((d.nx + DX_T - 1) / DX_T, (d.nz + DZ_T - 1) / DZ_T, d.ny - 1);
+    k_dyn_sums<<<grid, 256, smem, st>>>(d, sij, u, cu, dy, R, sums);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_dyn_widths<<<1, 256, 0, st>>>(d, sums, dy, dyf, widths);
     return cudaGetLastError();
 }
 

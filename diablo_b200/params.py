@@ -239,9 +239,10 @@ def validate(p: DiabloParams) -> None:
     if not (0 <= p.n_th <= MAX_TH):
         raise ValueError(f"N_TH must be in 0..{MAX_TH}")
     if p.les:
-        if p.les_model_type != 1:
-            # les.f:269-272 stops for the dynamic models
-            raise ValueError("LES_MODEL_TYPE must be 1 (constant Smagorinsky)")
+        if p.les_model_type not in (1, 2):
+            # 1: constant Smagorinsky (les.f); 2: the dynamic model of this
+            # library (the reference stops for 2 and 3, les.f:269-272)
+            raise ValueError("LES_MODEL_TYPE must be 1 (constant) or 2 (dynamic Smagorinsky)")
         if p.v_bc_ymin == 2 or p.v_bc_ymax == 2:
             # APPLY_BC_VEL_PHYS stops for V_BC = 2 (channel.f:2554, 2656)
             raise ValueError("LES needs V_BC_YMIN, V_BC_YMAX in 0, 1")

@@ -727,7 +727,109 @@ static double smag_width(orc_state* s, double dyj) {
     return -2.0 * (C_SMAG * C_SMAG) * pow(s->DX * beta_sgs * dyj * 2.0 * s->DZ * beta_sgs, 2.0 / 3.0);
 }
 
-/* les_chan (les.f:1-267, 280-336), LES_MODEL_TYPE = 1, NPROCY = NPROCZ = 1.
+/* The 5-point test filter of les_filter_chan (les.f:572-712) on one x-z
+ * plane of nq quantities q[nq][NZ][NX], periodic in x, then in z; tmp has
+ * the same size. */
+static void test_filter_plane(orc_state* s, double* q, double* tmp, int nq) {
+    const double Wm2 = 1.0 / 8.0, Wm1 = 1.0 / 4.0, W0 = 1.0 / 4.0, W1 = 1.0 / 4.0, W2 = 1.0 / 8.0;
+    const int NX = s->NX, NZ = s->NZ;
+    for (int f = 0; f < nq; ++f) {
+        double* A = q + (size_t)f * NZ * NX;
+        double* B = tmp + (size_t)f * NZ * NX;
+        for (int k = 0; k < NZ; ++k)
+            for (int i = 0; i < NX; ++i) {
+                const double* r = A + (size_t)k * NX;
+                B[(size_t)k * NX + i] = Wm2 * r[(i - 2 + NX) % NX] + Wm1 * r[(i - 1 + NX) % NX] + W0 * r[i] +
+                                        W1 * r[(i + 1) % NX] + W2 * r[(i + 2) % NX];
+            }
+        for (int k = 0; k < NZ; ++k)
+            for (int i = 0; i < NX; ++i)
+                A[(size_t)k * NX + i] = Wm2 * B[(size_t)((k - 2 + NZ) % NZ) * NX + i] +
+                                        Wm1 * B[(size_t)((k - 1 + NZ) % NZ) * NX + i] + W0 * B[(size_t)k * NX + i] +
+                                        W1 * B[(size_t)((k + 1) % NZ) * NX + i] + W2 * B[(size_t)((k + 2) % NZ) * NX + i];
+    }
+}
+
+/* Dynamic Smagorinsky coefficient, LES_MODEL_TYPE = 2.  The reference stops
+ * for this model type (les.f:269-272); this model is written for this
+ * library: the Germano identity with Lilly's least squares over each x-z
+ * plane, at GYF points J = 2..NY, with U2 and the GY strains S_12, S_23
+ * averaged to GYF:
+ *   L_ij = (u_i u_j)^ - u^_i u^_j
+ *   M_ij = R |S^| S^_ij - (|S| S_ij)^,   R = (Delta^/Delta)^2 = 9^(2/3)
+ *   (C Delta^2)(J) = max(0, -<L_ij M_ij> / (2 <M_ij M_ij>))
+ * where ^ is the test filter above, <.> the plane sum with the off-diagonal
+ * pairs counted twice, and |S|, |S^| have the mean shear removed as in
+ * les.f:113-137.  R reads the reference's label for this filter, alpha*beta
+ * = 9 (les.f:601), as the ratio of filtered cell volumes: the test filter
+ * widens x and z only.  DELTA_YF = -2 C Delta^2 at GYF points and DELTA_Y
+ * its interpolation to GY points, in the place of the constant model's
+ * -2 C_s^2 Delta^2 (les.f:196-217).  S1 holds |S| at GYF. */
+static void dynamic_widths(orc_state* s, const double* U1_bar, const double* U3_bar, double* DELTA_YF,
+                           double* DELTA_Y) {
+    const int NY = s->NY, NX = s->NX, NZ = s->NZ;
+    const double* DY = s->DY;
+    const double* DYF = s->DYF;
+    const double R = pow(9.0, 2.0 / 3.0);
+    double* CD = (double*)calloc(NY + 2, sizeof(double));
+    const size_t pl = (size_t)NX * NZ;
+#pragma omp parallel num_threads(nthreads())
+    {
+        double* q = (double*)malloc(sizeof(double) * 21 * pl);
+        double* tmp = (double*)malloc(sizeof(double) * 21 * pl);
+#pragma omp for schedule(dynamic)
+        for (int j = 2; j <= NY; ++j) {
+            for (int k = 0; k < NZ; ++k)
+                for (int i = 0; i < NX; ++i) {
+                    const double u1 = PH(s->U1, i, k, j), u3 = PH(s->U3, i, k, j);
+                    const double u2 = 0.5 * (PH(s->U2, i, k, j) + PH(s->U2, i, k, j + 1));
+                    const double s11 = PH(s->SIJ[0], i, k, j), s22 = PH(s->SIJ[1], i, k, j);
+                    const double s33 = PH(s->SIJ[2], i, k, j), s13 = PH(s->SIJ[4], i, k, j);
+                    const double s12 = 0.5 * (PH(s->SIJ[3], i, k, j) + PH(s->SIJ[3], i, k, j + 1));
+                    const double s23 = 0.5 * (PH(s->SIJ[5], i, k, j) + PH(s->SIJ[5], i, k, j + 1));
+                    const double sm = PH(s->S1, i, k, j);
+                    const double v[21] = {u1, u2, u3, u1 * u1, u2 * u2, u3 * u3, u1 * u2, u1 * u3, u2 * u3,
+                                          s11, s22, s33, s12, s13, s23,
+                                          sm * s11, sm * s22, sm * s33, sm * s12, sm * s13, sm * s23};
+                    for (int f = 0; f < 21; ++f) q[(size_t)f * pl + (size_t)k * NX + i] = v[f];
+                }
+            test_filter_plane(s, q, tmp, 21);
+            const double m1 = 0.5 * (U1_bar[j] - U1_bar[j - 1]) / DY[j] + 0.5 * (U1_bar[j + 1] - U1_bar[j]) / DY[j + 1];
+            const double m3 = 0.5 * (U3_bar[j] - U3_bar[j - 1]) / DY[j] + 0.5 * (U3_bar[j + 1] - U3_bar[j]) / DY[j + 1];
+            double num = 0.0, den = 0.0;
+            for (size_t e = 0; e < pl; ++e) {
+                double h[21];
+                for (int f = 0; f < 21; ++f) h[f] = q[(size_t)f * pl + e];
+                const double a12 = h[12] - 0.5 * m1, a23 = h[14] - 0.5 * m3;
+                const double sh = sqrt(2.0 * (h[9] * h[9]) + 4.0 * (a12 * a12) + 4.0 * (h[13] * h[13]) +
+                                       2.0 * (h[10] * h[10]) + 4.0 * (a23 * a23) + 2.0 * (h[11] * h[11]));
+                const double L11 = h[3] - h[0] * h[0], L22 = h[4] - h[1] * h[1], L33 = h[5] - h[2] * h[2];
+                const double L12 = h[6] - h[0] * h[1], L13 = h[7] - h[0] * h[2], L23 = h[8] - h[1] * h[2];
+                const double M11 = R * sh * h[9] - h[15], M22 = R * sh * h[10] - h[16], M33 = R * sh * h[11] - h[17];
+                const double M12 = R * sh * h[12] - h[18], M13 = R * sh * h[13] - h[19], M23 = R * sh * h[14] - h[20];
+                num += L11 * M11 + L22 * M22 + L33 * M33 + 2.0 * (L12 * M12 + L13 * M13 + L23 * M23);
+                den += M11 * M11 + M22 * M22 + M33 * M33 + 2.0 * (M12 * M12 + M13 * M13 + M23 * M23);
+            }
+            const double c = den > 0.0 ? -0.5 * num / den : 0.0;
+            CD[j] = c > 0.0 ? c : 0.0;
+        }
+        free(q);
+        free(tmp);
+    }
+    for (int j = 1; j <= NY + 1; ++j) {
+        const int jf = j < 2 ? 2 : j > NY ? NY : j;
+        DELTA_YF[j] = -2.0 * CD[jf];
+    }
+    for (int j = 2; j <= NY + 1; ++j) {
+        const double cg = (j >= 3 && j <= NY) ? (CD[j] * DYF[j - 1] + CD[j - 1] * DYF[j]) / (2.0 * DY[j])
+                        : CD[j <= 2 ? 2 : NY];
+        DELTA_Y[j] = -2.0 * cg;
+    }
+    free(CD);
+}
+
+/* les_chan (les.f:1-267, 280-336), LES_MODEL_TYPE = 1 (and 2, the dynamic
+ * coefficient above in place of C_s), NPROCY = NPROCZ = 1.
  * On exit U1..U3 are in physical space, NU_T is set and CF1..CF3 hold the
  * subgrid-stress divergence and the explicit cross terms. */
 static void les_chan(orc_state* s) {
@@ -805,6 +907,18 @@ static void les_chan(orc_state* s) {
                 PH(TEMP, i, k, j) = sqrt(2.0 * (g1 * g1) + 4.0 * (b4 * b4) + 4.0 * (g5 * g5) + 2.0 * (g2 * g2) +
                                          4.0 * (b6 * b6) + 2.0 * (g3 * g3));
             }
+    /* filter widths with -2 C^2 absorbed: constant (les.f:196-217) or
+     * dynamic (model type 2) */
+    double* DELTA_YF = (double*)calloc(NY + 2, sizeof(double));
+    double* DELTA_Y = (double*)calloc(NY + 2, sizeof(double));
+    if (s->p.les_model_type == 2) {
+        dynamic_widths(s, U1_bar, U3_bar, DELTA_YF, DELTA_Y);
+    } else {
+        for (int j = 1; j <= NY + 1; ++j) {
+            DELTA_YF[j] = smag_width(s, DYF[j]);
+            DELTA_Y[j] = smag_width(s, DY[j]);
+        }
+    }
     free(U1_bar);
     free(U3_bar);
     /* |S| S_ij: GYF components (les.f:165-177), Sij2 left to the implicit
@@ -826,12 +940,6 @@ static void les_chan(orc_state* s) {
                 PH(Sij4, i, k, j) = PH(TEMP, i, k, j) * (PH(Sij4, i, k, j) - 0.5 * (PH(U1, i, k, j) - PH(U1, i, k, j - 1)) / DY[j]);
                 PH(Sij6, i, k, j) = PH(TEMP, i, k, j) * (PH(Sij6, i, k, j) - 0.5 * (PH(U3, i, k, j) - PH(U3, i, k, j - 1)) / DY[j]);
             }
-    double* DELTA_YF = (double*)calloc(NY + 2, sizeof(double));
-    double* DELTA_Y = (double*)calloc(NY + 2, sizeof(double));
-    for (int j = 1; j <= NY + 1; ++j) {
-        DELTA_YF[j] = smag_width(s, DYF[j]);
-        DELTA_Y[j] = smag_width(s, DY[j]);
-    }
     /* NU_T = C_s^2 Delta^2 |S| at GY points (les.f:219-227); GHOST_LES_MPI
      * zeroes rows 1, 2, NY and NY+1 (mpi.f:494-507) */
 #pragma omp parallel for num_threads(nthreads())

@@ -1,21 +1,25 @@
-"""GPU parity of the constant-Smagorinsky LES branch against the oracle: the
+"""GPU parity of the LES branch against the oracle, for the constant
+Smagorinsky model (LES_MODEL_TYPE 1) and this library's dynamic model (2): the
 state after several RK3 steps and the eddy viscosity NU_T, through the
 C ABI, to the FP64 bar of the other parity tests (1e-10 relative L2, the
 small velocity components and the pressure measured against the velocity
 and pressure scales)."""
+import ctypes
+
+import numpy as np
 import pytest
 
 from diablo_b200 import grid as G, ics, params as P
-from diablo_b200.channel import Batch, Channel, DiabloError, DIABLO_ENOTSUP
+from diablo_b200.channel import Batch, Channel, DiabloError, DIABLO_ENOTSUP, load_library
 from oracle.oracle import Oracle
 from test_gpu_parity import TOL64, relerr, state_errors
 
 pytestmark = pytest.mark.gpu
 
 
-def les_channel(nx=32, ny=33, nz=24, n_th=1, neumann_top=False, variable_dt=False, create_new_flow=0):
+def les_channel(nx=32, ny=33, nz=24, n_th=1, neumann_top=False, variable_dt=False, create_new_flow=0, model=1):
     p = P.turbulent_channel(nx, ny, nz, re_tau=180.0, variable_dt=variable_dt)
-    p.les, p.les_model_type, p.create_new_flow = 1, 1, create_new_flow
+    p.les, p.les_model_type, p.create_new_flow = 1, model, create_new_flow
     p.n_th = n_th
     for n in range(1, n_th):
         p.pr[n], p.ri[n] = 1.0 + n, 0.0
@@ -52,19 +56,22 @@ def run(p, g, u, th, dt, steps, start_step=0):
     return err, plain, nut, o
 
 
-def test_les_channel_dirichlet():
+@pytest.mark.parametrize("model", [1, 2])
+def test_les_channel_dirichlet(model):
     """Closed channel, no-slip walls, one scalar: 4 steps with the model on."""
-    p, g, u, th = les_channel()
+    p, g, u, th = les_channel(model=model)
     err, plain, nut, o = run(p, g, u, th, 2e-4, 4)
     assert o.nu_t.max() > 0.0
     assert nut < TOL64, nut
     assert max(err.values()) < TOL64, (err, plain)
 
 
-def test_les_neumann_top_two_scalars_variable_dt():
+@pytest.mark.parametrize("model", [1, 2])
+def test_les_neumann_top_two_scalars_variable_dt(model):
     """Stress-free upper wall (APPLY_BC_LES rewrites row NY), a second scalar
-    with a Neumann lower wall (JSTART_TH = 1), CFL-adaptive dt, radix-3 x."""
-    p, g, u, th = les_channel(nx=48, ny=33, nz=24, n_th=2, neumann_top=True, variable_dt=True)
+    with a Neumann lower wall (JSTART_TH = 1), CFL-adaptive dt, radix-3 x;
+    NX = 48 is not a multiple of the dynamic model's 32-point tiles."""
+    p, g, u, th = les_channel(nx=48, ny=33, nz=24, n_th=2, neumann_top=True, variable_dt=True, model=model)
     err, plain, nut, _ = run(p, g, u, th, 2e-4, 3)
     assert nut < TOL64, nut
     assert max(err.values()) < TOL64, (err, plain)
@@ -81,6 +88,13 @@ def test_les_spin_up_switch():
 
 def test_les_rejected_configurations():
     p, g, _, _ = les_channel()
+    q = p.copy()
+    q.les_model_type = 3     # the reference stops here too (les.f:269-272)
+    L = load_library()
+    h = ctypes.c_void_p()
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (g.gy, g.gyf, g.dy, g.dyf)]
+    ptr = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert L.diablo_gpu_create(ctypes.byref(q), *[ptr(a) for a in arrs], ctypes.byref(h)) == DIABLO_ENOTSUP
     q = p.copy()
     q.precision = P.PREC_FP32SPLIT
     with pytest.raises(DiabloError) as e:

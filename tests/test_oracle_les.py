@@ -8,9 +8,9 @@ from diablo_b200 import grid as G, ics, params as P
 from oracle.oracle import Oracle
 
 
-def channel_case(les, create_new_flow=0, noise=0.5, neumann_top=False, nx=32, ny=33, nz=24, seed=3):
+def channel_case(les, create_new_flow=0, noise=0.5, neumann_top=False, nx=32, ny=33, nz=24, seed=3, model=1):
     p = P.turbulent_channel(nx, ny, nz, re_tau=180.0, variable_dt=False)
-    p.les, p.les_model_type, p.create_new_flow = les, 1, create_new_flow
+    p.les, p.les_model_type, p.create_new_flow = les, model, create_new_flow
     if neumann_top:
         p.u_bc_ymax = p.w_bc_ymax = 1
         p.u_bc_ymax_c1 = 0.1
@@ -97,12 +97,66 @@ def test_subgrid_model_dissipates_fluctuations(neumann_top):
 def test_validate_les_model_types():
     p = P.turbulent_channel(32, 33, 24)
     p.les = 1
-    p.les_model_type = 2
+    p.les_model_type = 3
     with pytest.raises(ValueError):
         P.validate(p)
+    p.les_model_type = 2
+    P.validate(p)
     p.les_model_type = 1
     p.v_bc_ymin = 2
     with pytest.raises(ValueError):
         P.validate(p)
     p.v_bc_ymin = 0
     P.validate(p)
+
+
+# --- dynamic Smagorinsky (LES_MODEL_TYPE 2, written for this library) -------
+
+def kh_dynamic(shift=0.0, seed=5):
+    p = P.kelvin_helmholtz(32, 33, 24)
+    p.les, p.les_model_type, p.create_new_flow = 1, 2, 0
+    P.validate(p)
+    g = G.channel_grid(G.uniform_gy(p.ny, -10.0, 10.0))
+    u, th = ics.shear_layer(p, g, seed=seed, amp=0.2)
+    u[0] += shift
+    o = Oracle(p, g, 0.01)
+    o.init_from_physical(u, th)
+    return p, o
+
+
+@pytest.mark.parametrize("model", [1, 2])
+def test_dynamic_model_rows_sign_and_finite(model):
+    p, o = channel_case(1, model=model)
+    o.step(2)
+    nt = o.nu_t
+    assert np.isfinite(nt).all() and nt.min() >= 0.0
+    for j in (0, 1, 2, p.ny, p.ny + 1):
+        assert not nt[j].any(), j
+    assert all(np.isfinite(x).all() for x in state(o))
+
+
+def test_dynamic_model_differs_from_constant():
+    _, a = channel_case(1, model=1)
+    _, b = channel_case(1, model=2)
+    a.rk_chan_1(1)
+    b.rk_chan_1(1)
+    assert np.abs(a.nu_t - b.nu_t).max() > 1e-3 * np.abs(a.nu_t).max()
+
+
+def test_dynamic_coefficient_is_galilean_invariant():
+    """A uniform streamwise velocity changes neither the Leonard stress L_ij
+    (the test filter keeps constants), the strain rates nor the mean-shear
+    removal, so NU_T of the first substage is the same."""
+    _, a = kh_dynamic(0.0)
+    _, b = kh_dynamic(0.7)
+    a.rk_chan_1(1)
+    b.rk_chan_1(1)
+    na, nb = a.nu_t, b.nu_t
+    assert na.max() > 0.0
+    assert np.abs(na - nb).max() <= 1e-9 * na.max()
+
+
+def test_dynamic_model_laminar_profile_has_no_eddy_viscosity():
+    _, o = channel_case(1, noise=0.0, model=2)
+    o.step(2)
+    assert o.nu_t.max() < 1e-14
