@@ -76,8 +76,9 @@ typedef struct diablo_params {
     double drhodx[DIABLO_MAX_TH], drhodz[DIABLO_MAX_TH];
     /* library options */
     int precision;                 /* DIABLO_PREC_* */
-    /* input_chan.dat LES_MODEL_TYPE (for/channel.f:1477); only 1, the
-     * constant-Smagorinsky model, is run (for/les.f:269-272 stops for 2, 3) */
+    /* input_chan.dat LES_MODEL_TYPE (for/channel.f:1477): 1 the constant
+     * Smagorinsky model of for/les.f; 2 a dynamic Smagorinsky model of this
+     * library (the reference stops for 2 and 3, for/les.f:269-272) */
     int les_model_type;
 } diablo_params;
 
