@@ -120,6 +120,9 @@ cudaError_t launch_dyn_widths(const Dims& d, const double* sij, const double* u,
 // COURANT's velocity minimum over physical rows 1..NY of U1..U3 (u: 3 fields).
 cudaError_t launch_les_cfl(const Dims& d, const double* u, const double* dy, double cfl, double dx, double dz,
                            double* dtmin, cudaStream_t st);
+// The learned closure's forward pass on device arrays (mlp.cu): x [n][11]
+// features in physical units -> y [n][6] stresses; mlp is a diablo_mlp handle.
+cudaError_t launch_mlp_forward(const void* mlp, const float* x, long long n, float* y, cudaStream_t st);
 // rows transformed together by the products kernel for a given NX
 int products_group(int nx);
 // Record the one-line message returned by diablo_gpu_last_error; returns code.

@@ -251,6 +251,42 @@ long long diablo_gpu_kernel_launches(void* handle);
 /* Short description of the last error on this thread. */
 const char* diablo_gpu_last_error(void);
 
+/* ------------------------------------------------------------------------ */
+/* Learned subgrid-stress closure.  The reference has no counterpart: it is   */
+/* this library's MLP from the 9 resolved velocity gradients du_i/dx_j        */
+/* (i-major), the wall distance in viscous units y+ and the filter width to   */
+/* the 6 stresses (tau_11, tau_22, tau_33, tau_12, tau_13, tau_23), through 3 */
+/* hidden layers of 64 GELU units.  Weights and activations are BF16 on the   */
+/* tensor cores with FP32 accumulation; parameters, gradients and the Adam    */
+/* state are FP32 on the device.                                              */
+/*                                                                            */
+/* Parameter vector (DIABLO_MLP_NPARAM floats): W1[64][11] b1[64] W2[64][64]  */
+/* b2[64] W3[64][64] b3[64] W4[6][64] b4[6] (the DIABLO_MLP_NTRAIN trained    */
+/* entries), then input means [11], input scales [11] and output scales [6]:  */
+/* the network maps (x - mean)/scale to tau / out_scale.                      */
+/* ------------------------------------------------------------------------ */
+#define DIABLO_MLP_NIN 11
+#define DIABLO_MLP_NHIDDEN 64
+#define DIABLO_MLP_NOUT 6
+#define DIABLO_MLP_NTRAIN 9478
+#define DIABLO_MLP_NPARAM 9506
+int diablo_mlp_create(void** mlp);
+int diablo_mlp_destroy(void* mlp);
+/* Set all parameters (scales must be non-zero); resets the Adam state. */
+int diablo_mlp_set_params(void* mlp, const float* params);
+int diablo_mlp_get_params(void* mlp, float* params);
+/* x: host [n][11] features; y: host [n][6] stresses. */
+int diablo_mlp_forward(void* mlp, const float* x, long long n, float* y);
+/* Loss sum_samples sum_outputs (y/out_scale - t/out_scale)^2 / (2n) and its
+ * gradient with respect to the DIABLO_MLP_NTRAIN trained parameters. */
+int diablo_mlp_gradient(void* mlp, const float* x, const float* t, long long n, double* loss, float* grad);
+/* steps Adam steps (beta 0.9, 0.999, eps 1e-8, learning rate lr) on
+ * consecutive mini-batches of `batch` samples, cycling through the n
+ * samples as given (the caller shuffles); losses[s] (may be NULL) receives
+ * each step's mini-batch loss before its update. */
+int diablo_mlp_train(void* mlp, const float* x, const float* t, long long n, int batch, int steps, float lr,
+                     double* losses);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,104 @@
+"""FP64 restatement of the learned subgrid-stress closure (the MLP of
+diablo_b200/csrc/mlp.cu): forward pass, loss, analytic gradient and one Adam
+step, in numpy.
+
+TEST INFRASTRUCTURE ONLY: the checker of the GPU kernels in tests/ (the
+forward values and the gradients they compute), never imported by the
+diablo_b200 package.  The reference has no such model, so this oracle is
+checked against finite differences of itself (tests/test_oracle_mlp.py).
+
+Parameter vector layout (float, as the C ABI): W1[64][11] b1[64] W2[64][64]
+b2[64] W3[64][64] b3[64] W4[6][64] b4[6] | in_mean[11] in_scale[11]
+out_scale[6].  GELU is the exact 0.5 z (1 + erf(z / sqrt 2)).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+NIN, NH, NOUT = 11, 64, 6
+SHAPES = [("W1", (NH, NIN)), ("b1", (NH,)), ("W2", (NH, NH)), ("b2", (NH,)), ("W3", (NH, NH)), ("b3", (NH,)),
+          ("W4", (NOUT, NH)), ("b4", (NOUT,))]
+NTRAIN = sum(int(np.prod(s)) for _, s in SHAPES)
+NPARAM = NTRAIN + NIN + NIN + NOUT
+
+_erf = np.vectorize(math.erf, otypes=[np.float64])
+
+
+def unpack(p: np.ndarray) -> dict:
+    p = np.asarray(p, dtype=np.float64)
+    out, o = {}, 0
+    for name, shape in SHAPES:
+        n = int(np.prod(shape))
+        out[name] = p[o:o + n].reshape(shape)
+        o += n
+    out["mean"] = p[o:o + NIN]
+    out["scale"] = p[o + NIN:o + 2 * NIN]
+    out["oscale"] = p[o + 2 * NIN:o + 2 * NIN + NOUT]
+    return out
+
+
+def bf16(a: np.ndarray) -> np.ndarray:
+    """Round to bfloat16 (round to nearest even on the float32 bits), as
+    __float2bfloat16_rn does; returned as float64."""
+    f = np.asarray(a, dtype=np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def gelu(z):
+    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+
+
+def gelu_d(z):
+    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+
+
+def forward(p: np.ndarray, x: np.ndarray, emulate_bf16: bool = False, keep: bool = False):
+    """Stresses (physical units) for features x [n][11].  With emulate_bf16
+    the weights, the normalised inputs and the hidden activations are rounded
+    to bfloat16 as the tensor-core kernels see them."""
+    q = unpack(p)
+    r = bf16 if emulate_bf16 else (lambda a: a)
+    h = r((np.asarray(x, dtype=np.float64) - q["mean"]) / q["scale"])
+    hs, zs = [h], []
+    for l in (1, 2, 3):
+        z = h @ r(q[f"W{l}"]).T + q[f"b{l}"]
+        zs.append(z)
+        h = r(gelu(z))
+        hs.append(h)
+    y = h @ r(q["W4"]).T + q["b4"]
+    if keep:
+        return y, hs, zs
+    return y * q["oscale"]
+
+
+def loss_grad(p: np.ndarray, x: np.ndarray, t: np.ndarray):
+    """Loss sum (y - t/out_scale)^2 / (2n) over samples and outputs (y the
+    normalised output) and its gradient with respect to the trained
+    parameters, FP64."""
+    q = unpack(p)
+    n = x.shape[0]
+    y, hs, zs = forward(p, x, keep=True)
+    e = y - np.asarray(t, dtype=np.float64) / q["oscale"]
+    loss = 0.5 * float(np.sum(e * e)) / n
+    d = e / n
+    grads = {"W4": d.T @ hs[3], "b4": d.sum(axis=0)}
+    g = d @ q["W4"]
+    for l in (3, 2, 1):
+        dl = g * gelu_d(zs[l - 1])
+        grads[f"W{l}"] = dl.T @ hs[l - 1]
+        grads[f"b{l}"] = dl.sum(axis=0)
+        g = dl @ q[f"W{l}"]
+    return loss, np.concatenate([grads[name].reshape(-1) for name, _ in SHAPES])
+
+
+def adam_step(p, grad, m1, m2, step, lr, b1=0.9, b2=0.999, eps=1e-8):
+    """One Adam update of the trained parameters (step counts from 1)."""
+    p = np.array(p, dtype=np.float64)
+    m1 = b1 * m1 + (1 - b1) * grad
+    m2 = b2 * m2 + (1 - b2) * grad * grad
+    p[:NTRAIN] -= lr * (m1 / (1 - b1 ** step)) / (np.sqrt(m2 / (1 - b2 ** step)) + eps)
+    return p, m1, m2
