@@ -35,6 +35,7 @@ EXPORTS = [
     "diablo_gpu_get_stream", "diablo_gpu_set_profiling", "diablo_gpu_kernel_times",
     "diablo_gpu_rem_div_chan_noalloc", "diablo_gpu_autotune", "diablo_gpu_batch_create",
     "diablo_gpu_batch_step", "diablo_gpu_batch_destroy", "diablo_gpu_filter_chan", "diablo_gpu_download_nu_t",
+    "diablo_gpu_sgs_samples",
 ]
 KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
 
@@ -84,6 +85,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_batch_destroy.argtypes = [vp]
     L.diablo_gpu_filter_chan.argtypes = [vp, ip]
     L.diablo_gpu_download_nu_t.argtypes = [vp, dp]
+    L.diablo_gpu_sgs_samples.argtypes = [vp, ip, ip, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                         ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     _lib = L
     return L
 
@@ -198,6 +201,20 @@ class Channel:
         buf = np.zeros(physical_shape(self.p))
         _check(self.L.diablo_gpu_download_nu_t(self._h, _dp(buf)), "diablo_gpu_download_nu_t")
         return buf[:, : self.p.nz, : self.p.nx].copy()
+
+    def sgs_samples(self, width: int = 3, stride: int = 1):
+        """Closure training samples of the current state: features [n][11]
+        and targets [n][6] of a width x width x-z top-hat filter."""
+        p = self.p
+        n = (p.ny - 2) * (-(-p.nx // stride)) * (-(-p.nz // stride))
+        x = np.zeros((n, 11), dtype=np.float32)
+        t = np.zeros((n, 6), dtype=np.float32)
+        cnt = ctypes.c_longlong()
+        fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        _check(self.L.diablo_gpu_sgs_samples(self._h, width, stride, fp(x), fp(t), n, ctypes.byref(cnt)),
+               "diablo_gpu_sgs_samples")
+        assert cnt.value == n
+        return x, t
 
     # --- routines of the reference ------------------------------------------
     def rk_chan_1(self, rk_step: int) -> None:

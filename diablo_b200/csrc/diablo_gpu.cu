@@ -886,6 +886,41 @@ int diablo_gpu_download_nu_t(void* handle, double* nu_t) {
     return DIABLO_OK;
 }
 
+static int ensure_work(Handle* h);
+
+int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float* t, long long capacity,
+                           long long* n) {
+    Handle* h = (Handle*)handle;
+    if (!h || !n) return fail(DIABLO_EINVAL, "null pointer argument");
+    const Dims& d = h->d;
+    if (width < 1 || width % 2 == 0 || width > d.nx || width > d.nz)
+        return fail(DIABLO_EINVAL, "filter width must be odd and at most NX, NZ");
+    if (stride < 1) return fail(DIABLO_EINVAL, "stride must be >= 1");
+    const long long ns = (long long)(d.ny - 2) * ((d.nx + stride - 1) / stride) * ((d.nz + stride - 1) / stride);
+    *n = ns;
+    if (!x || !t || capacity < ns) return fail(DIABLO_EINVAL, "sample arrays too small (the count is in *n)");
+    int rc = ensure_work(h);
+    if (rc) return rc;
+    const size_t pf = (size_t)d.nyp * d.nz * d.nx;
+    CK(launch_zinv<double>(d, h->cu, h->s_field, h->xb, h->x_field, 3, 0, d.nyp, h->pz, h->twz_d, h->st));
+    for (int f = 0; f < 3; ++f)
+        CK(launch_xinv(d, (const double2*)h->xb + (size_t)f * h->x_field, h->pw + (size_t)f * pf, 0, d.nyp, h->pm,
+                       h->twm_d, h->twn_d, h->st));
+    float *dx_ = nullptr, *dt_ = nullptr;
+    cudaError_t e = cudaMalloc((void**)&dx_, sizeof(float) * 11 * (size_t)ns);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&dt_, sizeof(float) * 6 * (size_t)ns);
+    if (e == cudaSuccess)
+        e = launch_sgs_samples(d, h->pw, h->d_gyf, h->d_dyf, h->dx, h->dz, h->p.nu, width, stride, dx_, dt_, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(x, dx_, sizeof(float) * 11 * (size_t)ns, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t, dt_, sizeof(float) * 6 * (size_t)ns, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    cudaFree(dx_);
+    cudaFree(dt_);
+    h->launches += 5;
+    if (e != cudaSuccess) return fail(DIABLO_ECUDA, std::string("closure samples: ") + cudaGetErrorString(e));
+    return DIABLO_OK;
+}
+
 int diablo_gpu_rk_chan_2(void* handle) {
     (void)handle;
     return fail(DIABLO_ENOTSUP, "RK_CHAN_2 is not supported (the reference stops here too)");

@@ -117,6 +117,10 @@ cudaError_t launch_les_solve(const LesArgs& a, double* r, const double* nut, dou
 // widths[NY+2..] = Delta_Y.  sij: the six physical strain fields, u: U1..U3.
 cudaError_t launch_dyn_widths(const Dims& d, const double* sij, const double* u, const double2* cu, const double* dy,
                               const double* dyf, double R, double* sums, double* widths, cudaStream_t st);
+// Closure samples (features [n][11], targets [n][6]) of a w x w x-z top-hat
+// filter at GYF points J = 2..NY-1 and every stride-th x and z point.
+cudaError_t launch_sgs_samples(const Dims& d, const double* u, const double* gyf, const double* dyf, double dx,
+                               double dz, double nu, int w, int stride, float* x, float* t, cudaStream_t st);
 // COURANT's velocity minimum over physical rows 1..NY of U1..U3 (u: 3 fields).
 cudaError_t launch_les_cfl(const Dims& d, const double* u, const double* dy, double cfl, double dx, double dz,
                            double* dtmin, cudaStream_t st);

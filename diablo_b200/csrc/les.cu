@@ -592,6 +592,63 @@ __global__ void k_dyn_widths(Dims d, const double* __restrict__ sums, const doub
     }
 }
 
+// ---------------------------------------------------------------------------
+// Samples for the learned closure: from physical U1..U3, at GYF points
+// J = 2..NY-1 and every `stride`-th x and z point, the features and targets
+// of a w x w top-hat filter in x and z (periodic; w odd), one thread per
+// sample.  U2 is averaged to GYF before filtering.  Features: the 9
+// gradients d(ubar_i)/dx_j (i-major; centred differences over one cell in x
+// and z, over GYF(J+-1) in y), y+ = (distance to the nearer of GYF(1),
+// GYF(NY)) / NU and Delta = (w DX DYF(J) w DZ)^(1/3).  Targets: tau_ij =
+// bar(u_i u_j) - ubar_i ubar_j in the order 11, 22, 33, 12, 13, 23.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TB) k_sgs_samples(Dims d, const double* __restrict__ u, const double* __restrict__ gyf,
+                                                    const double* __restrict__ dyf, double dx, double dz, double nu,
+                                                    int w, int stride, float* __restrict__ x, float* __restrict__ t) {
+    const int nx = d.nx, nz = d.nz, ny = d.ny;
+    const int nxs = (nx + stride - 1) / stride, nzs = (nz + stride - 1) / stride;
+    const long long ns = (long long)(ny - 2) * nzs * nxs;
+    const long long s = (long long)blockIdx.x * TB + threadIdx.x;
+    if (s >= ns) return;
+    const int ii = (int)(s % nxs), kk = (int)((s / nxs) % nzs), J = 2 + (int)(s / ((long long)nxs * nzs));
+    const int i = ii * stride, k = kk * stride;
+    const size_t pp = plane_pts(d), pf = pp * d.nyp;
+    const int hw = (w - 1) / 2;
+    const double inv = 1.0 / ((double)w * w);
+    auto raw = [&](int c, int j, int ia, int ka) -> double {
+        ia = ((ia % nx) + nx) % nx;
+        ka = ((ka % nz) + nz) % nz;
+        const size_t o = (size_t)j * pp + (size_t)ka * nx + ia;
+        return c == 1 ? 0.5 * (u[pf + o] + u[pf + o + pp]) : u[(size_t)c * pf + o];
+    };
+    auto bar = [&](int c, int j, int ic, int kc) {
+        double a = 0.0;
+        for (int dk = -hw; dk <= hw; ++dk)
+            for (int di = -hw; di <= hw; ++di) a += raw(c, j, ic + di, kc + dk);
+        return a * inv;
+    };
+    float* xo = x + s * 11;
+    float* to = t + s * 6;
+    const double hy = gyf[J + 1] - gyf[J - 1];
+    for (int c = 0; c < 3; ++c) {
+        xo[3 * c + 0] = (float)((bar(c, J, i + 1, k) - bar(c, J, i - 1, k)) / (2.0 * dx));
+        xo[3 * c + 1] = (float)((bar(c, J + 1, i, k) - bar(c, J - 1, i, k)) / hy);
+        xo[3 * c + 2] = (float)((bar(c, J, i, k + 1) - bar(c, J, i, k - 1)) / (2.0 * dz));
+    }
+    const double dwall = fmin(gyf[J] - gyf[1], gyf[ny] - gyf[J]);
+    xo[9] = (float)(dwall / nu);
+    xo[10] = (float)cbrt((double)w * dx * dyf[J] * (double)w * dz);
+    double ub[3] = {bar(0, J, i, k), bar(1, J, i, k), bar(2, J, i, k)};
+    double pr[6] = {0, 0, 0, 0, 0, 0};
+    for (int dk = -hw; dk <= hw; ++dk)
+        for (int di = -hw; di <= hw; ++di) {
+            const double a = raw(0, J, i + di, k + dk), b = raw(1, J, i + di, k + dk), c = raw(2, J, i + di, k + dk);
+            pr[0] += a * a; pr[1] += b * b; pr[2] += c * c; pr[3] += a * b; pr[4] += a * c; pr[5] += b * c;
+        }
+    const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+    for (int q = 0; q < 6; ++q) to[q] = (float)(pr[q] * inv - ub[pa[q]] * ub[pb[q]]);
+}
+
 // COURANT's velocity limit (courant.f:35-47) over physical rows 1..NY of the
 // fields the physical solves left (they are not band-limited, so the limit
 // is taken on them rather than on their transforms).  Non-negative doubles
@@ -701,6 +758,15 @@ cudaError_t launch_dyn_widths(const Dims& d, const double* sij, const double* u,
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_dyn_widths<<<1, 256, 0, st>>>(d, sums, dy, dyf, widths);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sgs_samples(const Dims& d, const double* u, const double* gyf, const double* dyf, double dx,
+                               double dz, double nu, int w, int stride, float* x, float* t, cudaStream_t st) {
+    const int nxs = (d.nx + stride - 1) / stride, nzs = (d.nz + stride - 1) / stride;
+    const long long ns = (long long)(d.ny - 2) * nzs * nxs;
+    if (ns <= 0) return cudaSuccess;
+    k_sgs_samples<<<(unsigned)((ns + TB - 1) / TB), TB, 0, st>>>(d, u, gyf, dyf, dx, dz, nu, w, stride, x, t);
     return cudaGetLastError();
 }
 

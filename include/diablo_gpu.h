@@ -286,6 +286,16 @@ int diablo_mlp_gradient(void* mlp, const float* x, const float* t, long long n, 
  * each step's mini-batch loss before its update. */
 int diablo_mlp_train(void* mlp, const float* x, const float* t, long long n, int batch, int steps, float lr,
                      double* losses);
+/* Training samples from a channel instance's current state (the reference
+ * has no counterpart): a width x width top-hat filter in x and z (periodic,
+ * width odd) of the velocity, at GYF points J = 2..NY-1 and every stride-th
+ * x and z point, J-major then z then x.  x receives [n][11] features
+ * (d ubar_i/dx_j i-major, y+, Delta; see DIABLO_MLP_NIN), t [n][6] targets
+ * tau_ij = bar(u_i u_j) - ubar_i ubar_j (11, 22, 33, 12, 13, 23), with
+ * n = (NY-2) ceil(NX/stride) ceil(NZ/stride) written to *n; arrays shorter
+ * than that (capacity samples) give DIABLO_EINVAL with *n set. */
+int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float* t, long long capacity,
+                           long long* n);
 
 #ifdef __cplusplus
 }
