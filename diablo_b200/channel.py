@@ -35,7 +35,7 @@ EXPORTS = [
     "diablo_gpu_get_stream", "diablo_gpu_set_profiling", "diablo_gpu_kernel_times",
     "diablo_gpu_rem_div_chan_noalloc", "diablo_gpu_autotune", "diablo_gpu_batch_create",
     "diablo_gpu_batch_step", "diablo_gpu_batch_destroy", "diablo_gpu_filter_chan", "diablo_gpu_download_nu_t",
-    "diablo_gpu_sgs_samples",
+    "diablo_gpu_sgs_samples", "diablo_gpu_set_sgs_mlp",
 ]
 KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
 
@@ -85,6 +85,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_batch_destroy.argtypes = [vp]
     L.diablo_gpu_filter_chan.argtypes = [vp, ip]
     L.diablo_gpu_download_nu_t.argtypes = [vp, dp]
+    L.diablo_gpu_set_sgs_mlp.argtypes = [vp, vp]
     L.diablo_gpu_sgs_samples.argtypes = [vp, ip, ip, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
                                          ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     _lib = L
@@ -201,6 +202,13 @@ class Channel:
         buf = np.zeros(physical_shape(self.p))
         _check(self.L.diablo_gpu_download_nu_t(self._h, _dp(buf)), "diablo_gpu_download_nu_t")
         return buf[:, : self.p.nz, : self.p.nx].copy()
+
+    def set_sgs_mlp(self, mlp) -> None:
+        """Attach a closure network (diablo_b200.mlp.SgsMlp) for
+        LES_MODEL_TYPE 4, or detach it with None."""
+        self._mlp = mlp
+        _check(self.L.diablo_gpu_set_sgs_mlp(self._h, mlp.handle if mlp is not None else None),
+               "diablo_gpu_set_sgs_mlp")
 
     def sgs_samples(self, width: int = 3, stride: int = 1):
         """Closure training samples of the current state: features [n][11]

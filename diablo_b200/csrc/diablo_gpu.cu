@@ -69,6 +69,8 @@ struct Handle {
     // Delta_YF, Delta_Y ([2][nyp])
     double *nut = nullptr, *lu = nullptr, *la = nullptr, *lb = nullptr, *d_delta = nullptr;
     double* d_dyn = nullptr;      // dynamic model: [2][nyp] plane sums, [2][nyp] widths
+    void* mlp = nullptr;          // learned closure (LES_MODEL_TYPE 4), owned by the caller
+    float *mlp_x = nullptr, *mlp_t = nullptr;   // its features [n][11] and stresses [n][6]
     double2 *ls = nullptr, *lr = nullptr;
     void* lx = nullptr;
     bool nut_set = false;         // NU_T has been computed at least once
@@ -136,7 +138,8 @@ void free_handle(Handle* h) {
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
                     h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_tabs, h->d_phitab,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
-                    h->twz_f, h->nut, h->lu, h->la, h->lb, h->d_delta, h->ls, h->lr, h->lx, h->d_dyn};
+                    h->twz_f, h->nut, h->lu, h->la, h->lb, h->d_delta, h->ls, h->lr, h->lx, h->d_dyn,
+                    h->mlp_x, h->mlp_t};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (h->st) cudaStreamDestroy(h->st);
@@ -272,8 +275,8 @@ int validate(const diablo_params* p) {
     if (p->les) {
         // 1: constant Smagorinsky (les.f); 2: this library's dynamic model; the
         // reference stops for 2 and 3 (les.f:269-272)
-        if (p->les_model_type != 1 && p->les_model_type != 2)
-            return fail(DIABLO_ENOTSUP, "LES_MODEL_TYPE must be 1 (constant) or 2 (dynamic Smagorinsky)");
+        if (p->les_model_type != 1 && p->les_model_type != 2 && p->les_model_type != 4)
+            return fail(DIABLO_ENOTSUP, "LES_MODEL_TYPE must be 1 (constant), 2 (dynamic) or 4 (learned closure)");
         if (p->precision != DIABLO_PREC_FP64) return fail(DIABLO_ENOTSUP, "the LES branch runs in FP64 only");
     }
     auto bc01 = [](int t) { return t == 0 || t == 1; };
@@ -708,15 +711,36 @@ static int les_substage(Handle* h, int rk_step, int time_step, double time, doub
     const int r = rk_step - 1;
     const size_t pf = (size_t)d.nyp * d.nz * d.nx;
     const int nyp = d.nyp;
+    // LES_MODEL_TYPE 4 runs the learned closure when one is attached and
+    // falls back to the dynamic model otherwise
+    const bool use_mlp = p.les_model_type == 4 && h->mlp;
+    const bool dyn = p.les_model_type == 2 || (p.les_model_type == 4 && !h->mlp);
     // filter widths with -2 C^2 absorbed: the constant model's, or the
     // dynamic model's of this substage
-    const double* delta_yf = p.les_model_type == 2 ? h->d_dyn + 2 * nyp : h->d_delta;
+    const double* delta_yf = dyn ? h->d_dyn + 2 * nyp : h->d_delta;
     const double* delta_y = delta_yf + nyp;
     CnArgs a = substage_args(h, rk_step, time, h_bar, beta_bar, zeta_bar);
     ProfScope ps(h, DIABLO_KERNEL_OTHER);
     CK(launch_les_pre(a, h->d_k2, h->lr, h->st));
     h->launches += 1;
-    if (sgs) {
+    if (sgs && use_mlp) {
+        // the learned closure: ghost cells as les_chan sets them, features of
+        // the resolved field at GYF rows 2..NY-1, the network's stresses, and
+        // their divergence into CF (explicit; NU_T stays zero)
+        dim3 grid((d.nkxp + 127) / 128, d.nkzt);
+        k_apply_bc_vel<<<grid, 128, 0, h->st>>>(d, h->cu, h->d_dy, h->d_dyf, p);
+        CK(cudaGetLastError());
+        CK(launch_les_bc(d, h->cu, p, h->st));
+        CK(les_to_phys(h, h->cu, 3, h->lu, 0, nyp));
+        const long long n = (long long)(d.ny - 2) * d.nz * d.nx;
+        CK(launch_sgs_samples(d, h->lu, h->d_gyf, h->d_dyf, h->dx, h->dz, p.nu, 1, 1, h->mlp_x, nullptr, h->st));
+        CK(launch_mlp_forward(h->mlp, h->mlp_x, n, h->mlp_t, h->st));
+        CK(launch_mlp_tau_fields(d, h->mlp_t, h->d_dy, h->d_dyf, h->lb, h->st));
+        CK(launch_phys_bc_vel(d, h->lu, h->d_dy, h->d_dyf, p, h->st));
+        CK(les_to_fourier(h, h->lb, 6, h->ls, 0, nyp));
+        CK(launch_mlp_tau_cf(d, h->ls, h->cf, h->d_kx, h->d_kz, h->d_dy, h->d_dyf, h->st));
+        h->launches += 8;
+    } else if (sgs) {
         // les_chan: ghost cells (APPLY_BC_VEL_MPI, APPLY_BC_LES), strain rates
         dim3 grid((d.nkxp + 127) / 128, d.nkzt);
         k_apply_bc_vel<<<grid, 128, 0, h->st>>>(d, h->cu, h->d_dy, h->d_dyf, p);
@@ -726,7 +750,7 @@ static int les_substage(Handle* h, int rk_step, int time_step, double time, doub
         h->launches += 3;
         CK(les_to_phys(h, h->ls, 6, h->la, 0, nyp));
         CK(les_to_phys(h, h->cu, 3, h->lu, 0, nyp));
-        if (p.les_model_type == 2) {
+        if (dyn) {
             CK(launch_dyn_widths(d, h->la, h->lu, h->cu, h->d_dy, h->d_dyf, std::pow(9.0, 2.0 / 3.0), h->d_dyn,
                                  h->d_dyn + 2 * nyp, h->st));
             h->launches += 2;
@@ -918,6 +942,25 @@ int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float*
     cudaFree(dt_);
     h->launches += 5;
     if (e != cudaSuccess) return fail(DIABLO_ECUDA, std::string("closure samples: ") + cudaGetErrorString(e));
+    return DIABLO_OK;
+}
+
+int diablo_gpu_set_sgs_mlp(void* handle, void* mlp) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    if (!h->p.les) return fail(DIABLO_EINVAL, "the closure needs an LES instance");
+    if (mlp && !h->mlp_x) {
+        const size_t n = (size_t)(h->d.ny - 2) * h->d.nz * h->d.nx;
+        cudaError_t e = cudaMalloc((void**)&h->mlp_x, sizeof(float) * 11 * n);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&h->mlp_t, sizeof(float) * 6 * n);
+        if (e != cudaSuccess) {
+            cudaFree(h->mlp_x);
+            cudaFree(h->mlp_t);
+            h->mlp_x = h->mlp_t = nullptr;
+            return fail(DIABLO_ENOMEM, std::string("closure buffers: ") + cudaGetErrorString(e));
+        }
+    }
+    h->mlp = mlp;
     return DIABLO_OK;
 }
 

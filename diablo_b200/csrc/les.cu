@@ -628,7 +628,6 @@ __global__ void __launch_bounds__(TB) k_sgs_samples(Dims d, const double* __rest
         return a * inv;
     };
     float* xo = x + s * 11;
-    float* to = t + s * 6;
     const double hy = gyf[J + 1] - gyf[J - 1];
     for (int c = 0; c < 3; ++c) {
         xo[3 * c + 0] = (float)((bar(c, J, i + 1, k) - bar(c, J, i - 1, k)) / (2.0 * dx));
@@ -638,6 +637,8 @@ __global__ void __launch_bounds__(TB) k_sgs_samples(Dims d, const double* __rest
     const double dwall = fmin(gyf[J] - gyf[1], gyf[ny] - gyf[J]);
     xo[9] = (float)(dwall / nu);
     xo[10] = (float)cbrt((double)w * dx * dyf[J] * (double)w * dz);
+    if (!t) return;
+    float* to = t + s * 6;
     double ub[3] = {bar(0, J, i, k), bar(1, J, i, k), bar(2, J, i, k)};
     double pr[6] = {0, 0, 0, 0, 0, 0};
     for (int dk = -hw; dk <= hw; ++dk)
@@ -647,6 +648,54 @@ __global__ void __launch_bounds__(TB) k_sgs_samples(Dims d, const double* __rest
         }
     const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
     for (int q = 0; q < 6; ++q) to[q] = (float)(pr[q] * inv - ub[pa[q]] * ub[pb[q]]);
+}
+
+// The closure's stresses at GYF points J = 2..NY-1 (tau [n][6] in the
+// sampler's order, every x and z point) into physical fields: tau_11,
+// tau_22, tau_33, tau_13 at GYF points; tau_12, tau_23 interpolated to GY
+// points J = 3..NY-1 with the weights of the GY interpolation of channel.f
+// (DYF(J-1), DYF(J)); all other rows zero.  out: 6 fields [J][z][x].
+__global__ void __launch_bounds__(TB) k_mlp_tau_fields(Dims d, const float* __restrict__ tau,
+                                                       const double* __restrict__ dy, const double* __restrict__ dyf,
+                                                       double* __restrict__ out) {
+    const size_t pp = plane_pts(d), pf = pp * d.nyp;
+    const size_t g = (size_t)blockIdx.x * TB + threadIdx.x;
+    if (g >= pf) return;
+    const int J = (int)(g / pp), ny = d.ny;
+    const size_t col = g % pp;
+    auto T = [&](int q, int j) { return (double)tau[((size_t)(j - 2) * pp + col) * 6 + q]; };
+    const bool f = J >= 2 && J <= ny - 1;
+    out[g] = f ? T(0, J) : 0.0;              // 11
+    out[pf + g] = f ? T(1, J) : 0.0;         // 22
+    out[2 * pf + g] = f ? T(2, J) : 0.0;     // 33
+    out[3 * pf + g] = f ? T(4, J) : 0.0;     // 13
+    const bool gy = J >= 3 && J <= ny - 1;
+    const double w0 = gy ? dyf[J - 1] : 0.0, w1 = gy ? dyf[J] : 0.0, h2 = 2.0 * dy[J];
+    out[4 * pf + g] = gy ? (T(3, J) * w0 + T(3, J - 1) * w1) / h2 : 0.0;   // 12 at GY
+    out[5 * pf + g] = gy ? (T(5, J) * w0 + T(5, J - 1) * w1) / h2 : 0.0;   // 23 at GY
+}
+
+// CF_i -= d tau_ij / dx_j for the closure's stresses (all explicit): tau
+// holds the forward transforms of k_mlp_tau_fields' six fields.
+__global__ void __launch_bounds__(TB) k_mlp_tau_cf(Dims d, const double2* __restrict__ tau, double2* __restrict__ cf,
+                                                   const double* __restrict__ kxw, const double* __restrict__ kzw,
+                                                   const double* __restrict__ dy, const double* __restrict__ dyf) {
+    int J, m, kx;
+    if (!spec_index(d, (size_t)blockIdx.x * TB + threadIdx.x, J, m, kx)) return;
+    const int ny = d.ny;
+    if (J < 2 || J > ny) return;
+    const size_t ps = d.splane(), fs = ps * d.nyp;
+    const size_t o = (size_t)J * ps + (size_t)m * d.ldx + kx;
+    const double KX = kxw[kx], KZ = kzw[m];
+    auto T = [&](int q, int j) { return tau[(size_t)q * fs + o + (size_t)(j - J) * ps]; };
+    if (J <= ny - 1) {
+        double2* f1 = cf + o;
+        double2* f3 = cf + 2 * fs + o;
+        *f1 = *f1 - ik(KX, T(0, J)) - (T(4, J + 1) - T(4, J)) / dyf[J] - ik(KZ, T(3, J));
+        *f3 = *f3 - ik(KX, T(3, J)) - (T(5, J + 1) - T(5, J)) / dyf[J] - ik(KZ, T(2, J));
+    }
+    double2* f2 = cf + fs + o;
+    *f2 = *f2 - ik(KX, T(4, J)) - (T(1, J) - T(1, J - 1)) / dy[J] - ik(KZ, T(5, J));
 }
 
 // COURANT's velocity limit (courant.f:35-47) over physical rows 1..NY of the
@@ -767,6 +816,18 @@ cudaError_t launch_sgs_samples(const Dims& d, const double* u, const double* gyf
     const long long ns = (long long)(d.ny - 2) * nzs * nxs;
     if (ns <= 0) return cudaSuccess;
     k_sgs_samples<<<(unsigned)((ns + TB - 1) / TB), TB, 0, st>>>(d, u, gyf, dyf, dx, dz, nu, w, stride, x, t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_tau_fields(const Dims& d, const float* tau, const double* dy, const double* dyf, double* out,
+                                  cudaStream_t st) {
+    k_mlp_tau_fields<<<blocks(plane_pts(d) * d.nyp), TB, 0, st>>>(d, tau, dy, dyf, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_tau_cf(const Dims& d, const double2* tau, double2* cf, const double* kx, const double* kz,
+                              const double* dy, const double* dyf, cudaStream_t st) {
+    k_mlp_tau_cf<<<blocks(spec_items(d)), TB, 0, st>>>(d, tau, cf, kx, kz, dy, dyf);
     return cudaGetLastError();
 }
 

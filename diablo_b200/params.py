@@ -239,10 +239,11 @@ def validate(p: DiabloParams) -> None:
     if not (0 <= p.n_th <= MAX_TH):
         raise ValueError(f"N_TH must be in 0..{MAX_TH}")
     if p.les:
-        if p.les_model_type not in (1, 2):
+        if p.les_model_type not in (1, 2, 4):
             # 1: constant Smagorinsky (les.f); 2: the dynamic model of this
-            # library (the reference stops for 2 and 3, les.f:269-272)
-            raise ValueError("LES_MODEL_TYPE must be 1 (constant) or 2 (dynamic Smagorinsky)")
+            # library (the reference stops for 2 and 3, les.f:269-272); 4: the
+            # learned closure of this library
+            raise ValueError("LES_MODEL_TYPE must be 1 (constant), 2 (dynamic) or 4 (learned closure)")
         if p.v_bc_ymin == 2 or p.v_bc_ymax == 2:
             # APPLY_BC_VEL_PHYS stops for V_BC = 2 (channel.f:2554, 2656)
             raise ValueError("LES needs V_BC_YMIN, V_BC_YMAX in 0, 1")

@@ -78,7 +78,8 @@ typedef struct diablo_params {
     int precision;                 /* DIABLO_PREC_* */
     /* input_chan.dat LES_MODEL_TYPE (for/channel.f:1477): 1 the constant
      * Smagorinsky model of for/les.f; 2 a dynamic Smagorinsky model of this
-     * library (the reference stops for 2 and 3, for/les.f:269-272) */
+     * library (the reference stops for 2 and 3, for/les.f:269-272); 4 the
+     * learned closure (diablo_gpu_set_sgs_mlp), the dynamic model without one */
     int les_model_type;
 } diablo_params;
 
@@ -296,6 +297,15 @@ int diablo_mlp_train(void* mlp, const float* x, const float* t, long long n, int
  * than that (capacity samples) give DIABLO_EINVAL with *n set. */
 int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float* t, long long capacity,
                            long long* n);
+/* Attach a closure network to an LES instance (NULL detaches; the caller
+ * keeps ownership and must not change its parameters while a substage that
+ * uses it runs).  With LES_MODEL_TYPE 4, each LES substage then computes the
+ * features of the resolved field (width 1, every point of rows 2..NY-1), the
+ * network's stresses, tau_12 and tau_23 interpolated to GY points, and
+ * CF_i -= d tau_ij / dx_j explicitly, in place of the eddy-viscosity model
+ * (NU_T stays zero); without a network type 4 runs the dynamic model.  The
+ * reference has no counterpart. */
+int diablo_gpu_set_sgs_mlp(void* handle, void* mlp);
 
 #ifdef __cplusplus
 }

@@ -11,6 +11,7 @@
 
 #include <complex.h>
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -119,6 +120,7 @@ struct orc_state {
      * KAPPA_T (channel.f:314-322 copies it for every scalar); Sij<->CSij and
      * TEMP<->CTEMP share one buffer each as header_les:31-37 equivalences them */
     double *NU_T, *SIJ[6], *TEMP;
+    float* MLP;           /* learned closure parameters (LES_MODEL_TYPE 4), or NULL */
     fftplan px_plan, pz_plan;
 };
 
@@ -217,7 +219,8 @@ void orc_destroy(orc_state* s) {
                       s->U1, s->U2, s->U3, s->P, s->R1, s->R2, s->R3, s->F1, s->F2,
                       s->F3, s->S1, s->TH, s->CTH, s->FTH, s->CFTH, s->RTH, s->CRTH,
                       s->NU_T, s->TEMP, s->SIJ[0], s->SIJ[1], s->SIJ[2], s->SIJ[3], s->SIJ[4],
-                      s->SIJ[5]};
+                      s->SIJ[5], NULL};
+    free(s->MLP);
     for (size_t q = 0; q < sizeof(bufs) / sizeof(bufs[0]); ++q) free(bufs[q]);
     plan_free(&s->px_plan);
     plan_free(&s->pz_plan);
@@ -828,6 +831,148 @@ static void dynamic_widths(orc_state* s, const double* U1_bar, const double* U3_
     free(CD);
 }
 
+/* The learned closure (LES_MODEL_TYPE 4), which the reference does not
+ * have: the features of the resolved field at GYF rows J = 2..NY-1 (the
+ * velocity gradients by centred differences, U2 averaged to GYF, y+ and the
+ * grid filter width), the MLP of the GPU library with its weights,
+ * normalised inputs and hidden activations rounded to bfloat16 as its
+ * tensor cores see them, tau_12 and tau_23 interpolated to GY points, and
+ * CF_i -= d tau_ij / dx_j, all explicit. */
+#define MLP_NIN 11
+#define MLP_NH 64
+#define MLP_NOUT 6
+static float bf16r(double v) {
+    float f = (float)v;
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+void orc_set_mlp(orc_state* s, const float* params) {
+    const size_t n = (size_t)MLP_NH * MLP_NIN + MLP_NH + 2 * ((size_t)MLP_NH * MLP_NH + MLP_NH) +
+                     (size_t)MLP_NOUT * MLP_NH + MLP_NOUT + 2 * MLP_NIN + MLP_NOUT;
+    free(s->MLP);
+    s->MLP = NULL;
+    if (!params) return;
+    s->MLP = (float*)malloc(sizeof(float) * n);
+    memcpy(s->MLP, params, sizeof(float) * n);
+}
+
+static void mlp_forward(const float* P, const float* xf, float* y) {
+    const float* W1 = P;
+    const float* b1 = W1 + MLP_NH * MLP_NIN;
+    const float* W2 = b1 + MLP_NH;
+    const float* b2 = W2 + MLP_NH * MLP_NH;
+    const float* W3 = b2 + MLP_NH;
+    const float* b3 = W3 + MLP_NH * MLP_NH;
+    const float* W4 = b3 + MLP_NH;
+    const float* b4 = W4 + MLP_NOUT * MLP_NH;
+    const float* mean = b4 + MLP_NOUT;
+    const float* scale = mean + MLP_NIN;
+    const float* osc = scale + MLP_NIN;
+    double h[MLP_NH], g[MLP_NH], x[MLP_NIN];
+    for (int k = 0; k < MLP_NIN; ++k) x[k] = bf16r((xf[k] - mean[k]) / scale[k]);
+    for (int o = 0; o < MLP_NH; ++o) {
+        double z = b1[o];
+        for (int k = 0; k < MLP_NIN; ++k) z += (double)bf16r(W1[o * MLP_NIN + k]) * x[k];
+        h[o] = bf16r((float)(0.5 * z * (1.0 + erf(z / sqrt(2.0)))));
+    }
+    const float* Ws[2] = {W2, W3};
+    const float* bs[2] = {b2, b3};
+    for (int l = 0; l < 2; ++l) {
+        for (int o = 0; o < MLP_NH; ++o) {
+            double z = bs[l][o];
+            for (int k = 0; k < MLP_NH; ++k) z += (double)bf16r(Ws[l][o * MLP_NH + k]) * h[k];
+            g[o] = bf16r((float)(0.5 * z * (1.0 + erf(z / sqrt(2.0)))));
+        }
+        memcpy(h, g, sizeof(h));
+    }
+    for (int o = 0; o < MLP_NOUT; ++o) {
+        double z = b4[o];
+        for (int k = 0; k < MLP_NH; ++k) z += (double)bf16r(W4[o * MLP_NH + k]) * h[k];
+        y[o] = (float)z * osc[o];
+    }
+}
+
+static void les_mlp(orc_state* s) {
+    const int NY = s->NY, NX = s->NX, NZ = s->NZ, NXP = s->NXP, TNKZ = s->TNKZ;
+    const double* DY = s->DY;
+    const double* DYF = s->DYF;
+    const double* GYF = s->GYF;
+    double *U1 = s->U1, *U2 = s->U2, *U3 = s->U3;
+    double *CF1 = s->F1, *CF2 = s->F2, *CF3 = s->F3;
+    const cplx CI = I;
+    orc_apply_bc_vel(s);
+    apply_bc_les(s);
+    orc_fft_xz_to_physical(s, U1, U1, 0, NY + 1);
+    orc_fft_xz_to_physical(s, U2, U2, 0, NY + 1);
+    orc_fft_xz_to_physical(s, U3, U3, 0, NY + 1);
+    double* T[6];
+    for (int q = 0; q < 6; ++q) {
+        T[q] = s->SIJ[q];
+        memset(T[q], 0, sizeof(double) * s->nreal);
+    }
+    const size_t pl = (size_t)NX * NZ;
+    float* tau = (float*)calloc((size_t)(NY + 2) * pl * 6, sizeof(float));
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY - 1; ++j)
+        for (int k = 0; k < NZ; ++k)
+            for (int i = 0; i < NX; ++i) {
+                const int ip = (i + 1) % NX, im = (i - 1 + NX) % NX, kp = (k + 1) % NZ, km = (k - 1 + NZ) % NZ;
+                double x[MLP_NIN];
+                const double* Us[3] = {U1, U2, U3};
+                const double hy = GYF[j + 1] - GYF[j - 1];
+                for (int c = 0; c < 3; ++c) {
+                    const double* u = Us[c];
+#define UU(ii, kk, jj) (c == 1 ? 0.5 * (PH(u, ii, kk, jj) + PH(u, ii, kk, (jj) + 1)) : PH(u, ii, kk, jj))
+                    x[3 * c + 0] = (UU(ip, k, j) - UU(im, k, j)) / (2.0 * s->DX);
+                    x[3 * c + 1] = (UU(i, k, j + 1) - UU(i, k, j - 1)) / hy;
+                    x[3 * c + 2] = (UU(i, kp, j) - UU(i, km, j)) / (2.0 * s->DZ);
+#undef UU
+                }
+                x[9] = fmin(GYF[j] - GYF[1], GYF[NY] - GYF[j]) / s->p.nu;
+                x[10] = cbrt(s->DX * DYF[j] * s->DZ);
+                float xf[MLP_NIN];
+                for (int q = 0; q < MLP_NIN; ++q) xf[q] = (float)x[q];
+                mlp_forward(s->MLP, xf, tau + (((size_t)j * NZ + k) * NX + i) * 6);
+            }
+    /* 11, 22, 33, 13 at GYF rows 2..NY-1; 12, 23 at GY rows 3..NY-1 */
+#define TAU(q, i, k, j) ((double)tau[(((size_t)(j) * NZ + (k)) * NX + (i)) * 6 + (q)])
+    for (int j = 2; j <= NY - 1; ++j)
+        for (int k = 0; k < NZ; ++k)
+            for (int i = 0; i < NX; ++i) {
+                PH(T[0], i, k, j) = TAU(0, i, k, j);
+                PH(T[1], i, k, j) = TAU(1, i, k, j);
+                PH(T[2], i, k, j) = TAU(2, i, k, j);
+                PH(T[3], i, k, j) = TAU(4, i, k, j);
+                if (j >= 3) {
+                    PH(T[4], i, k, j) = (TAU(3, i, k, j) * DYF[j - 1] + TAU(3, i, k, j - 1) * DYF[j]) / (2.0 * DY[j]);
+                    PH(T[5], i, k, j) = (TAU(5, i, k, j) * DYF[j - 1] + TAU(5, i, k, j - 1) * DYF[j]) / (2.0 * DY[j]);
+                }
+            }
+#undef TAU
+    free(tau);
+    for (int q = 0; q < 6; ++q) orc_fft_xz_to_fourier(s, T[q], T[q], 0, NY + 1);
+#pragma omp parallel for num_threads(nthreads())
+    for (int j = 2; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                if (j <= NY - 1) {
+                    CX(CF1, i, k, j) = CX(CF1, i, k, j) - CI * s->KX[i] * CX(T[0], i, k, j) -
+                                       (CX(T[4], i, k, j + 1) - CX(T[4], i, k, j)) / DYF[j] -
+                                       CI * s->KZ[k] * CX(T[3], i, k, j);
+                    CX(CF3, i, k, j) = CX(CF3, i, k, j) - CI * s->KX[i] * CX(T[3], i, k, j) -
+                                       (CX(T[5], i, k, j + 1) - CX(T[5], i, k, j)) / DYF[j] -
+                                       CI * s->KZ[k] * CX(T[2], i, k, j);
+                }
+                CX(CF2, i, k, j) = CX(CF2, i, k, j) - CI * s->KX[i] * CX(T[4], i, k, j) -
+                                   (CX(T[1], i, k, j) - CX(T[1], i, k, j - 1)) / DY[j] -
+                                   CI * s->KZ[k] * CX(T[5], i, k, j);
+            }
+}
+
 /* les_chan (les.f:1-267, 280-336), LES_MODEL_TYPE = 1 (and 2, the dynamic
  * coefficient above in place of C_s), NPROCY = NPROCZ = 1.
  * On exit U1..U3 are in physical space, NU_T is set and CF1..CF3 hold the
@@ -844,6 +989,10 @@ static void les_chan(orc_state* s) {
     double *Sij1 = s->SIJ[0], *Sij2 = s->SIJ[1], *Sij3 = s->SIJ[2];
     double *Sij4 = s->SIJ[3], *Sij5 = s->SIJ[4], *Sij6 = s->SIJ[5];
     const cplx CI = I;
+    if (s->p.les_model_type == 4 && s->MLP) {
+        les_mlp(s);
+        return;
+    }
     /* ghost cells (les.f:64-77): APPLY_BC_VEL_MPI, then APPLY_BC_LES */
     orc_apply_bc_vel(s);
     apply_bc_les(s);
@@ -911,7 +1060,7 @@ static void les_chan(orc_state* s) {
      * dynamic (model type 2) */
     double* DELTA_YF = (double*)calloc(NY + 2, sizeof(double));
     double* DELTA_Y = (double*)calloc(NY + 2, sizeof(double));
-    if (s->p.les_model_type == 2) {
+    if (s->p.les_model_type == 2 || s->p.les_model_type == 4) {   /* 4 without a network: dynamic */
         dynamic_widths(s, U1_bar, U3_bar, DELTA_YF, DELTA_Y);
     } else {
         for (int j = 1; j <= NY + 1; ++j) {

@@ -75,6 +75,9 @@ void orc_step(orc_state* s);
 void orc_filter_chan(orc_state* s, int n);
 /* Statistics of SAVE_STATS_CHAN (DIABLO_STAT_* profiles, NY+2 each). */
 void orc_stats(orc_state* s, double* profiles);
+/* Parameters of the learned closure (LES_MODEL_TYPE 4), in the layout of the
+ * GPU library's diablo_mlp_set_params; NULL removes it. */
+void orc_set_mlp(orc_state* s, const float* params);
 /* Plain complex DFT of length n (interleaved), sign -1 or +1, unnormalised;
  * exposed for the transform-convention tests. */
 int orc_cdft(int n, double* data, int sign);

@@ -59,6 +59,7 @@ def lib() -> ctypes.CDLL:
                      "orc_apply_bc_scalar", "orc_step"):
             getattr(L, name).argtypes = [vp]
         L.orc_stats.argtypes = [vp, dp]
+        L.orc_set_mlp.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
         L.orc_cdft.restype = ip
         L.orc_cdft.argtypes = [ip, dp, ip]
         _lib = L
@@ -190,6 +191,14 @@ class Oracle:
 
     def filter_chan(self, n: int = 1) -> None:
         lib().orc_filter_chan(self._h, n)
+
+    def set_mlp(self, params) -> None:
+        """The learned closure's parameters (LES_MODEL_TYPE 4), or None."""
+        if params is None:
+            lib().orc_set_mlp(self._h, None)
+            return
+        self._mlp = np.ascontiguousarray(params, dtype=np.float32)
+        lib().orc_set_mlp(self._h, self._mlp.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
 
     def stats(self) -> np.ndarray:
         out = np.zeros((17, self.p.ny + 2))

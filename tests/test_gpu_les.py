@@ -104,3 +104,61 @@ def test_les_rejected_configurations():
         with pytest.raises(DiabloError) as e:
             Batch([c])
         assert e.value.code == DIABLO_ENOTSUP
+
+
+# --- the learned closure (LES_MODEL_TYPE 4) ----------------------------------
+
+def closure_params(seed=21, out=1e-2):
+    """A seeded network whose inputs are normalised by the features' typical
+    sizes in this flow and whose stresses are O(out)."""
+    from diablo_b200 import mlp as ML
+    mean = np.zeros(11)
+    scale = np.concatenate([np.full(9, 20.0), [60.0, 0.1]])
+    return ML.init_params(seed, mean, scale, np.full(6, out))
+
+
+def run_closure(p, g, u, th, dt, steps, params):
+    from diablo_b200.mlp import SgsMlp
+    o = Oracle(p, g, dt)
+    o.init_from_physical(u, th)
+    if params is not None:
+        o.set_mlp(params)
+    c = Channel(p, g, dt)
+    c.upload([x.copy() for x in o.cu], o.cp.copy(), o.cth.copy())
+    m = SgsMlp(params) if params is not None else None
+    with c:
+        if m is not None:
+            c.set_sgs_mlp(m)
+        for _ in range(steps):
+            o.step()
+            c.step()
+        err = state_errors(p, c, o, scaled=True)
+        plain = state_errors(p, c, o)
+        s = c.download()
+    if m is not None:
+        m.close()
+    return err, plain, s, o
+
+
+def test_learned_closure_matches_oracle():
+    """Closure stresses from the same BF16 network on both sides (the
+    oracle rounds weights, inputs and activations to bfloat16 as the tensor
+    cores do, and accumulates in FP64 where the GPU uses FP32): the states
+    after 3 steps agree to 1e-7, set by those accumulations and by the
+    rare activations that round to different bfloat16 neighbours."""
+    p, g, u, th = les_channel(model=4)
+    err, plain, s, o = run_closure(p, g, u, th, 2e-4, 3, closure_params())
+    assert max(err.values()) < 1e-7, (err, plain)
+    # the closure acted: the state differs from the run without any model
+    q = p.copy()
+    q.les = 0
+    o0 = Oracle(q, g, 2e-4)
+    o0.init_from_physical(u, th)
+    o0.step(3)
+    assert relerr(o.cu[0], o0.cu[0]) > 1e-9
+
+
+def test_learned_closure_falls_back_to_dynamic_model():
+    p, g, u, th = les_channel(model=4)
+    err, plain, _, _ = run_closure(p, g, u, th, 2e-4, 3, None)
+    assert max(err.values()) < TOL64, (err, plain)
