@@ -1,0 +1,161 @@
+"""Training and a-priori evaluation of the learned subgrid-stress closure.
+
+The closure (diablo_b200.mlp) is trained on snapshots of this solver's own
+DNS: every `every` steps the state is filtered by a `width` x `width` top-hat
+in x and z on the GPU (Channel.sgs_samples), which gives the resolved
+velocity gradients, y+ and the filter width as features and the subfilter
+stresses tau_ij = bar(u_i u_j) - ubar_i ubar_j as targets.  Snapshots are
+split 80/20 with a seeded permutation; the network is trained by the
+library's own kernels (diablo_mlp_train) on the training snapshots.
+
+The method without the network is an eddy viscosity: tau^d_ij = -2 C Delta^2
+|S| S_ij for the deviatoric stresses.  Its a-priori error is bounded below
+by the best coefficient for each y-plane fitted by least squares to the
+training snapshots' stresses -- the best any such model, the dynamic one
+included, can do at a plane -- and that fit is the baseline the network is
+compared with on the held-out snapshots.
+"""
+from __future__ import annotations
+
+import time as _time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .channel import Channel
+from .mlp import NIN, NOUT, SgsMlp, init_params, normalisation
+
+_PAIRS = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+
+
+@dataclass
+class Snapshots:
+    x: np.ndarray            # [n][11] features
+    t: np.ndarray            # [n][6] subfilter stresses
+    snap: np.ndarray         # [n] snapshot index of each sample
+    per_snapshot: int
+    seconds: float = 0.0
+
+
+def dns_snapshots(p, grid, dt, u, th, count: int, every: int, warmup: int = 0, width: int = 3,
+                  stride: int = 1) -> Snapshots:
+    """Run the DNS on the GPU and collect `count` filtered snapshots, one
+    every `every` steps after `warmup` steps."""
+    t0 = _time.perf_counter()
+    xs, ts = [], []
+    with Channel(p, grid, dt) as c:
+        c.init_from_physical(u, th)
+        c.step(warmup)
+        for _ in range(count):
+            c.step(every)
+            x, t = c.sgs_samples(width, stride)
+            xs.append(x)
+            ts.append(t)
+    m = xs[0].shape[0]
+    snap = np.repeat(np.arange(count), m)
+    return Snapshots(np.concatenate(xs), np.concatenate(ts), snap, m, _time.perf_counter() - t0)
+
+
+def split(count: int, seed: int, frac: float = 0.8):
+    """Seeded split of snapshot indices into training and held-out sets."""
+    perm = np.random.default_rng(seed).permutation(count)
+    k = int(round(frac * count))
+    return np.sort(perm[:k]), np.sort(perm[k:])
+
+
+def deviatoric(t: np.ndarray) -> np.ndarray:
+    d = np.array(t, dtype=np.float64, copy=True)
+    tr = (d[:, 0] + d[:, 1] + d[:, 2]) / 3.0
+    d[:, :3] -= tr[:, None]
+    return d
+
+
+def _norm2(a: np.ndarray) -> np.ndarray:
+    """Squared tensor norm with the off-diagonal pairs counted twice."""
+    return np.sum(a[:, :3] ** 2, axis=1) + 2.0 * np.sum(a[:, 3:] ** 2, axis=1)
+
+
+def eddy_viscosity_basis(x: np.ndarray) -> np.ndarray:
+    """m_ij = -2 Delta^2 |S| S_ij from the features (S_ij the symmetric part
+    of the velocity gradient, |S| = sqrt(2 S_ij S_ij))."""
+    g = np.asarray(x[:, :9], dtype=np.float64).reshape(-1, 3, 3)
+    s = 0.5 * (g + g.transpose(0, 2, 1))
+    sv = np.stack([s[:, a, b] for a, b in _PAIRS], axis=1)
+    smag = np.sqrt(2.0 * _norm2(sv))
+    delta = np.asarray(x[:, 10], dtype=np.float64)
+    return -2.0 * (delta ** 2 * smag)[:, None] * sv
+
+
+def plane_coefficients(x: np.ndarray, t: np.ndarray) -> dict:
+    """Least-squares C for each plane (keyed by its y+ feature) from samples."""
+    m = eddy_viscosity_basis(x)
+    d = deviatoric(t)
+    num = np.sum(d[:, :3] * m[:, :3], axis=1) + 2.0 * np.sum(d[:, 3:] * m[:, 3:], axis=1)
+    den = _norm2(m)
+    key = np.round(np.asarray(x[:, 9], dtype=np.float64), 6)
+    out = {}
+    for k in np.unique(key):
+        sel = key == k
+        out[k] = float(num[sel].sum() / den[sel].sum()) if den[sel].sum() > 0 else 0.0
+    return out
+
+
+def eddy_viscosity_predict(x: np.ndarray, coef: dict) -> np.ndarray:
+    key = np.round(np.asarray(x[:, 9], dtype=np.float64), 6)
+    c = np.array([coef.get(k, 0.0) for k in key])
+    return c[:, None] * eddy_viscosity_basis(x)
+
+
+def relative_error(pred: np.ndarray, true: np.ndarray) -> float:
+    """Tensor-norm relative L2 error over all samples."""
+    return float(np.sqrt(_norm2(pred - true).sum() / _norm2(true).sum()))
+
+
+@dataclass
+class ClosureReport:
+    train_samples: int
+    test_samples: int
+    train_seconds: float
+    losses: np.ndarray
+    mlp_test_error: float             # full tau, held-out snapshots
+    mlp_test_error_deviatoric: float
+    eddy_viscosity_test_error: float  # deviatoric, best per-plane coefficient
+    params: np.ndarray = field(repr=False, default=None)
+
+    def summary(self) -> dict:
+        return {"train_samples": self.train_samples, "test_samples": self.test_samples,
+                "train_seconds": self.train_seconds, "final_loss": float(self.losses[-1]),
+                "first_loss": float(self.losses[0]),
+                "mlp_test_error": self.mlp_test_error,
+                "mlp_test_error_deviatoric": self.mlp_test_error_deviatoric,
+                "eddy_viscosity_best_plane_fit_test_error": self.eddy_viscosity_test_error}
+
+
+def train_and_evaluate(data: Snapshots, seed: int, steps: int, batch: int = 1024, lr: float = 2e-3,
+                       frac: float = 0.8) -> ClosureReport:
+    """Train on the training snapshots (seeded split and shuffle) and compare
+    the network with the best per-plane eddy viscosity on the held-out ones."""
+    count = int(data.snap.max()) + 1
+    tr, te = split(count, seed, frac)
+    mtr = np.isin(data.snap, tr)
+    xtr, ttr = data.x[mtr], data.t[mtr]
+    xte, tte = data.x[~mtr], data.t[~mtr]
+    perm = np.random.default_rng(seed + 1).permutation(xtr.shape[0])
+    xtr, ttr = xtr[perm], ttr[perm]
+    mean, scale, osc = normalisation(xtr.astype(np.float64), ttr.astype(np.float64))
+    t0 = _time.perf_counter()
+    with SgsMlp(init_params(seed, mean, scale, osc)) as m:
+        losses = m.train(xtr, ttr, batch, steps, lr)
+        train_seconds = _time.perf_counter() - t0
+        pred = m.forward(xte).astype(np.float64)
+        params = m.params()
+    coef = plane_coefficients(xtr, ttr)
+    ev = eddy_viscosity_predict(xte, coef)
+    dte = deviatoric(tte)
+    return ClosureReport(xtr.shape[0], xte.shape[0], train_seconds, losses,
+                         relative_error(pred, tte.astype(np.float64)),
+                         relative_error(deviatoric(pred), dte),
+                         relative_error(ev, dte), params)
+
+
+assert NIN == 11 and NOUT == 6
