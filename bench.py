@@ -63,7 +63,10 @@ def parse_args():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-les", action="store_true")
-    ap.add_argument("--only", choices=["les"], default=None,
+    ap.add_argument("--no-closure", action="store_true")
+    ap.add_argument("--closure-snapshots", type=int, default=2000)
+    ap.add_argument("--closure-steps", type=int, default=20000)
+    ap.add_argument("--only", choices=["les", "closure"], default=None,
                     help="run one leg alone and print its JSON (for profiling captures)")
     ap.add_argument("--error-steps", type=int, default=500,
                     help="steps after which FP32-split is compared with FP64 (besides 100)")
@@ -307,26 +310,40 @@ def les_rates(w, u, th, steps: int, warmup: int, torch, cpu: bool) -> dict:
     from diablo_b200.params import PREC_FP64
     from diablo_b200.channel import Channel
 
-    out = {"workload": "same grid and initial fields, LES=1, LES_MODEL_TYPE=1 (C_s=0.13), "
-                       "CREATE_NEW_FLOW=F, FP64"}
-    for les in (0, 1):
+    from diablo_b200.mlp import SgsMlp
+
+    out = {"workload": "same grid and initial fields, LES=1, CREATE_NEW_FLOW=F, FP64; les: LES_MODEL_TYPE=1 "
+                       "(C_s=0.13), les_dynamic: 2, les_closure: 4 with a seeded untrained network (the cost "
+                       "does not depend on the weights)"}
+    for key, les, model in (("dns", 0, 1), ("les", 1, 1), ("les_dynamic", 1, 2), ("les_closure", 1, 4)):
         p = w.p.copy()
         p.precision = PREC_FP64
-        p.les, p.les_model_type, p.create_new_flow = les, 1, 0
+        p.les, p.les_model_type, p.create_new_flow = les, model, 0
         c = Channel(p, w.grid, w.dt)
+        m = None
+        if model == 4:
+            m = SgsMlp(seed=7)
+            c.set_sgs_mlp(m)
         c.init_from_physical(u, th)
         c.step(warmup)
         n0 = c.kernel_launches()
         ms = timed_steps(c, steps, torch)
         launches = c.kernel_launches() - n0
-        key = "les" if les else "dns"
         out[f"{key}_steps_per_s"] = steps / (ms / 1e3)
         out[f"{key}_ms_per_step"] = ms / steps
         out[f"{key}_gpu_launches_per_step"] = launches / steps
-        if les:
+        if key == "les":
             out["nu_t_max"] = float(c.download_nu_t().max())
         c.close()
+        if m is not None:
+            m.close()
     out["les_cost_vs_dns"] = out["les_ms_per_step"] / out["dns_ms_per_step"]
+    out["les_dynamic_cost_vs_dns"] = out["les_dynamic_ms_per_step"] / out["dns_ms_per_step"]
+    out["les_closure_cost_vs_dns"] = out["les_closure_ms_per_step"] / out["dns_ms_per_step"]
+    # closure inference: MLP flops per resolved point, 2 (11*64 + 2*64*64 + 64*6), over (NY-2) NX NZ points
+    # per substage
+    fl = 2 * (11 * 64 + 2 * 64 * 64 + 64 * 6) * (w.p.ny - 2) * w.p.nx * w.p.nz * 3
+    out["closure_network_gflop_per_step"] = fl / 1e9
     if cpu:
         from diablo_b200 import workloads
         from oracle.oracle import Oracle
@@ -350,6 +367,28 @@ def les_rates(w, u, th, steps: int, warmup: int, torch, cpu: bool) -> dict:
     return out
 
 
+def closure_rates(snapshots: int, steps: int, seed: int = 41) -> dict:
+    """The learned closure's training on this solver's DNS: Kelvin-Helmholtz
+    layer 64x65x64 (amp 0.2 seeded noise), `snapshots` snapshots one every 3
+    steps, 3x3 x-z top-hat, every 4th x and z point, seeded 80/20 split by
+    snapshot, `steps` Adam steps of 4096 samples; a-priori errors on the
+    held-out snapshots against the best per-plane eddy viscosity."""
+    from diablo_b200 import closure, grid as G, ics, params as P
+
+    p = P.kelvin_helmholtz(64, 65, 64)
+    g = G.channel_grid(G.uniform_gy(p.ny, -10.0, 10.0))
+    u, th = ics.shear_layer(p, g, seed=seed, amp=0.2)
+    data = closure.dns_snapshots(p, g, 0.01, u, th, count=snapshots, every=3, warmup=10, width=3, stride=4)
+    rep = closure.train_and_evaluate(data, seed=seed + 1, steps=steps, batch=4096, lr=2e-3)
+    out = rep.summary()
+    flop_per_sample = 3 * 2 * (11 * 64 + 2 * 64 * 64 + 64 * 6)     # forward + backward
+    out.update({"snapshots": snapshots, "snapshot_seconds": data.seconds, "adam_steps": steps, "batch": 4096,
+                "train_samples_per_s": steps * 4096 / rep.train_seconds,
+                "train_tflops": steps * 4096 * flop_per_sample / rep.train_seconds / 1e12,
+                "workload": "KH 64x65x64 DNS, amp 0.2, 3x3 top-hat, stride 4, seeded 80/20 split by snapshot"})
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from diablo_b200 import build, workloads
@@ -365,6 +404,14 @@ def run_ours(args, rank, world, local_rank):
                                 device_id=torch.device("cuda", local_rank))
     nx, ny, nz = (int(v) for v in args.grid.split(","))
     w = workloads.precision(nx, ny, nz)
+    if args.only == "closure":
+        out = closure_rates(args.closure_snapshots, args.closure_steps) if rank == 0 else None
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"closure": out}), flush=True)
+        return
     if args.only == "les":
         u, th = w.initial_fields()
         out = les_rates(w, u, th, args.steps, args.warmup, torch, cpu=False)
@@ -437,6 +484,10 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_batched:
         batched = batched_rates(max(3, min(args.steps, 20)))
 
+    closure_line = None
+    if not args.no_closure and rank == 0:
+        closure_line = closure_rates(args.closure_snapshots, args.closure_steps)
+
     les = None
     if not args.no_les:
         les = les_rates(w, u, th, max(3, min(args.steps, 20)), 3, torch,
@@ -476,7 +527,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(), "fp64": fp64,
         "fp32_split_speedup_vs_fp64": (value / world) / fp64["steps_per_s"] if fp64 else None,
-        "kernel_ms_per_step": kernel_ms, "batched": batched, "les": les,
+        "kernel_ms_per_step": kernel_ms, "batched": batched, "les": les, "closure": closure_line,
     }
     print(json.dumps(line), flush=True)
 

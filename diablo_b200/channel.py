@@ -87,7 +87,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_download_nu_t.argtypes = [vp, dp]
     L.diablo_gpu_set_sgs_mlp.argtypes = [vp, vp]
     L.diablo_gpu_sgs_samples.argtypes = [vp, ip, ip, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
-                                         ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+                                         ctypes.POINTER(ctypes.c_float), ctypes.c_longlong,
+                                         ctypes.POINTER(ctypes.c_longlong)]
     _lib = L
     return L
 
@@ -211,18 +212,20 @@ class Channel:
                "diablo_gpu_set_sgs_mlp")
 
     def sgs_samples(self, width: int = 3, stride: int = 1):
-        """Closure training samples of the current state: features [n][11]
-        and targets [n][6] of a width x width x-z top-hat filter."""
+        """Closure training samples of the current state for a width x width
+        x-z top-hat filter: dimensionless features [n][11], dimensionless
+        targets [n][6] and the stress scales [n] (tau = target * scale)."""
         p = self.p
         n = (p.ny - 2) * (-(-p.nx // stride)) * (-(-p.nz // stride))
         x = np.zeros((n, 11), dtype=np.float32)
         t = np.zeros((n, 6), dtype=np.float32)
+        s = np.zeros(n, dtype=np.float32)
         cnt = ctypes.c_longlong()
         fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-        _check(self.L.diablo_gpu_sgs_samples(self._h, width, stride, fp(x), fp(t), n, ctypes.byref(cnt)),
+        _check(self.L.diablo_gpu_sgs_samples(self._h, width, stride, fp(x), fp(t), fp(s), n, ctypes.byref(cnt)),
                "diablo_gpu_sgs_samples")
         assert cnt.value == n
-        return x, t
+        return x, t, s
 
     # --- routines of the reference ------------------------------------------
     def rk_chan_1(self, rk_step: int) -> None:

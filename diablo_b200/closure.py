@@ -3,15 +3,21 @@
 The closure (diablo_b200.mlp) is trained on snapshots of this solver's own
 DNS: every `every` steps the state is filtered by a `width` x `width` top-hat
 in x and z on the GPU (Channel.sgs_samples), which gives the resolved
-velocity gradients, y+ and the filter width as features and the subfilter
-stresses tau_ij = bar(u_i u_j) - ubar_i ubar_j as targets.  Snapshots are
+velocity gradients (divided by their norm G), y+ and the filter width Delta
+as features and the subfilter stresses tau_ij = bar(u_i u_j) - ubar_i
+ubar_j divided by Delta^2 G^2 as targets; this dimensionless form lets
+snapshots of a decaying flow weigh alike.  Snapshots are
 split 80/20 with a seeded permutation; the network is trained by the
-library's own kernels (diablo_mlp_train) on the training snapshots.
+library's own kernels (diablo_mlp_train) on the training snapshots, whose
+samples are drawn with probabilities proportional to s^2 = (Delta^2 G^2)^2
+so that the dimensionless loss weighs samples as the error of the
+dimensional stresses does (otherwise the quiescent regions, where tau/s is
+noise over a small G^2, would dominate it).
 
 The method without the network is an eddy viscosity: tau^d_ij = -2 C Delta^2
 |S| S_ij for the deviatoric stresses.  Its a-priori error is bounded below
 by the best coefficient for each y-plane fitted by least squares to the
-training snapshots' stresses -- the best any such model, the dynamic one
+training snapshots' (dimensional) stresses -- the best any such model, the dynamic one
 included, can do at a plane -- and that fit is the baseline the network is
 compared with on the held-out snapshots.
 """
@@ -30,8 +36,9 @@ _PAIRS = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
 
 @dataclass
 class Snapshots:
-    x: np.ndarray            # [n][11] features
-    t: np.ndarray            # [n][6] subfilter stresses
+    x: np.ndarray            # [n][11] dimensionless features
+    t: np.ndarray            # [n][6] dimensionless subfilter stresses
+    s: np.ndarray            # [n] stress scales Delta^2 G^2
     snap: np.ndarray         # [n] snapshot index of each sample
     per_snapshot: int
     seconds: float = 0.0
@@ -42,18 +49,20 @@ def dns_snapshots(p, grid, dt, u, th, count: int, every: int, warmup: int = 0, w
     """Run the DNS on the GPU and collect `count` filtered snapshots, one
     every `every` steps after `warmup` steps."""
     t0 = _time.perf_counter()
-    xs, ts = [], []
+    xs, ts, ss = [], [], []
     with Channel(p, grid, dt) as c:
         c.init_from_physical(u, th)
         c.step(warmup)
         for _ in range(count):
             c.step(every)
-            x, t = c.sgs_samples(width, stride)
+            x, t, s = c.sgs_samples(width, stride)
             xs.append(x)
             ts.append(t)
+            ss.append(s)
     m = xs[0].shape[0]
     snap = np.repeat(np.arange(count), m)
-    return Snapshots(np.concatenate(xs), np.concatenate(ts), snap, m, _time.perf_counter() - t0)
+    return Snapshots(np.concatenate(xs), np.concatenate(ts), np.concatenate(ss), snap, m,
+                     _time.perf_counter() - t0)
 
 
 def split(count: int, seed: int, frac: float = 0.8):
@@ -76,22 +85,24 @@ def _norm2(a: np.ndarray) -> np.ndarray:
 
 
 def eddy_viscosity_basis(x: np.ndarray) -> np.ndarray:
-    """m_ij = -2 Delta^2 |S| S_ij from the features (S_ij the symmetric part
-    of the velocity gradient, |S| = sqrt(2 S_ij S_ij))."""
+    """m_ij = -2 Delta^2 |S| S_ij / (Delta^2 G^2) from the dimensionless
+    features (S_ij the symmetric part of the gradient g_ij / G, |S| =
+    sqrt(2 S_ij S_ij)): the eddy viscosity's stresses in the targets' form."""
     g = np.asarray(x[:, :9], dtype=np.float64).reshape(-1, 3, 3)
     s = 0.5 * (g + g.transpose(0, 2, 1))
     sv = np.stack([s[:, a, b] for a, b in _PAIRS], axis=1)
     smag = np.sqrt(2.0 * _norm2(sv))
-    delta = np.asarray(x[:, 10], dtype=np.float64)
-    return -2.0 * (delta ** 2 * smag)[:, None] * sv
+    return -2.0 * smag[:, None] * sv
 
 
-def plane_coefficients(x: np.ndarray, t: np.ndarray) -> dict:
-    """Least-squares C for each plane (keyed by its y+ feature) from samples."""
+def plane_coefficients(x: np.ndarray, t: np.ndarray, s: np.ndarray) -> dict:
+    """Least-squares C for each plane (keyed by its y+ feature) from samples,
+    minimising the error of the dimensional stresses (weights s^2)."""
     m = eddy_viscosity_basis(x)
     d = deviatoric(t)
-    num = np.sum(d[:, :3] * m[:, :3], axis=1) + 2.0 * np.sum(d[:, 3:] * m[:, 3:], axis=1)
-    den = _norm2(m)
+    w = np.asarray(s, dtype=np.float64) ** 2
+    num = w * (np.sum(d[:, :3] * m[:, :3], axis=1) + 2.0 * np.sum(d[:, 3:] * m[:, 3:], axis=1))
+    den = w * _norm2(m)
     key = np.round(np.asarray(x[:, 9], dtype=np.float64), 6)
     out = {}
     for k in np.unique(key):
@@ -106,9 +117,11 @@ def eddy_viscosity_predict(x: np.ndarray, coef: dict) -> np.ndarray:
     return c[:, None] * eddy_viscosity_basis(x)
 
 
-def relative_error(pred: np.ndarray, true: np.ndarray) -> float:
-    """Tensor-norm relative L2 error over all samples."""
-    return float(np.sqrt(_norm2(pred - true).sum() / _norm2(true).sum()))
+def relative_error(pred: np.ndarray, true: np.ndarray, s: np.ndarray) -> float:
+    """Tensor-norm relative L2 error over all samples of the dimensional
+    stresses (dimensionless values times the scales s)."""
+    s = np.asarray(s, dtype=np.float64)[:, None]
+    return float(np.sqrt(_norm2((pred - true) * s).sum() / _norm2(true * s).sum()))
 
 
 @dataclass
@@ -132,30 +145,39 @@ class ClosureReport:
 
 
 def train_and_evaluate(data: Snapshots, seed: int, steps: int, batch: int = 1024, lr: float = 2e-3,
-                       frac: float = 0.8) -> ClosureReport:
+                       frac: float = 0.8, max_stats: int = 2_000_000) -> ClosureReport:
     """Train on the training snapshots (seeded split and shuffle) and compare
-    the network with the best per-plane eddy viscosity on the held-out ones."""
+    the network with the best per-plane eddy viscosity on the held-out ones.
+    The normalisation, the per-plane coefficients and the held-out errors use
+    seeded subsamples of at most max_stats samples (training uses all)."""
     count = int(data.snap.max()) + 1
     tr, te = split(count, seed, frac)
     mtr = np.isin(data.snap, tr)
-    xtr, ttr = data.x[mtr], data.t[mtr]
-    xte, tte = data.x[~mtr], data.t[~mtr]
-    perm = np.random.default_rng(seed + 1).permutation(xtr.shape[0])
-    xtr, ttr = xtr[perm], ttr[perm]
-    mean, scale, osc = normalisation(xtr.astype(np.float64), ttr.astype(np.float64))
+    xtr, ttr, strn = data.x[mtr], data.t[mtr], data.s[mtr]
+    xte, tte, ste = data.x[~mtr], data.t[~mtr], data.s[~mtr]
+    w = strn.astype(np.float64) ** 2
+    draw = np.random.default_rng(seed + 1).choice(xtr.shape[0], xtr.shape[0], replace=True, p=w / w.sum())
+    xtr, ttr, strn = xtr[draw], ttr[draw], strn[draw]
+    rng = np.random.default_rng(seed + 2)
+    sub = lambda n: slice(None) if n <= max_stats else np.sort(rng.choice(n, max_stats, replace=False))
+    st = sub(xtr.shape[0])
+    se = sub(xte.shape[0])
+    mean, scale, osc = normalisation(xtr[st].astype(np.float64), ttr[st].astype(np.float64))
     t0 = _time.perf_counter()
     with SgsMlp(init_params(seed, mean, scale, osc)) as m:
         losses = m.train(xtr, ttr, batch, steps, lr)
         train_seconds = _time.perf_counter() - t0
-        pred = m.forward(xte).astype(np.float64)
+        pred = m.forward(xte[se]).astype(np.float64)
         params = m.params()
-    coef = plane_coefficients(xtr, ttr)
-    ev = eddy_viscosity_predict(xte, coef)
-    dte = deviatoric(tte)
+    coef = plane_coefficients(xtr[st], ttr[st], strn[st])
+    ev = eddy_viscosity_predict(xte[se], coef)
+    tsel = tte[se].astype(np.float64)
+    ssel = ste[se]
+    dte = deviatoric(tsel)
     return ClosureReport(xtr.shape[0], xte.shape[0], train_seconds, losses,
-                         relative_error(pred, tte.astype(np.float64)),
-                         relative_error(deviatoric(pred), dte),
-                         relative_error(ev, dte), params)
+                         relative_error(pred, tsel, ssel),
+                         relative_error(deviatoric(pred), dte, ssel),
+                         relative_error(ev, dte, ssel), params)
 
 
 assert NIN == 11 and NOUT == 6

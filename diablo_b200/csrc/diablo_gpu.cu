@@ -70,7 +70,7 @@ struct Handle {
     double *nut = nullptr, *lu = nullptr, *la = nullptr, *lb = nullptr, *d_delta = nullptr;
     double* d_dyn = nullptr;      // dynamic model: [2][nyp] plane sums, [2][nyp] widths
     void* mlp = nullptr;          // learned closure (LES_MODEL_TYPE 4), owned by the caller
-    float *mlp_x = nullptr, *mlp_t = nullptr;   // its features [n][11] and stresses [n][6]
+    float *mlp_x = nullptr, *mlp_t = nullptr, *mlp_s = nullptr;   // its features [n][11], outputs [n][6], scales [n]
     double2 *ls = nullptr, *lr = nullptr;
     void* lx = nullptr;
     bool nut_set = false;         // NU_T has been computed at least once
@@ -139,7 +139,7 @@ void free_handle(Handle* h) {
                     h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_tabs, h->d_phitab,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
                     h->twz_f, h->nut, h->lu, h->la, h->lb, h->d_delta, h->ls, h->lr, h->lx, h->d_dyn,
-                    h->mlp_x, h->mlp_t};
+                    h->mlp_x, h->mlp_t, h->mlp_s};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (h->st) cudaStreamDestroy(h->st);
@@ -733,9 +733,10 @@ static int les_substage(Handle* h, int rk_step, int time_step, double time, doub
         CK(launch_les_bc(d, h->cu, p, h->st));
         CK(les_to_phys(h, h->cu, 3, h->lu, 0, nyp));
         const long long n = (long long)(d.ny - 2) * d.nz * d.nx;
-        CK(launch_sgs_samples(d, h->lu, h->d_gyf, h->d_dyf, h->dx, h->dz, p.nu, 1, 1, h->mlp_x, nullptr, h->st));
+        CK(launch_sgs_samples(d, h->lu, h->d_gyf, h->d_dyf, h->dx, h->dz, p.nu, 1, 1, h->mlp_x, nullptr, h->mlp_s,
+                              h->st));
         CK(launch_mlp_forward(h->mlp, h->mlp_x, n, h->mlp_t, h->st));
-        CK(launch_mlp_tau_fields(d, h->mlp_t, h->d_dy, h->d_dyf, h->lb, h->st));
+        CK(launch_mlp_tau_fields(d, h->mlp_t, h->mlp_s, h->d_dy, h->d_dyf, h->lb, h->st));
         CK(launch_phys_bc_vel(d, h->lu, h->d_dy, h->d_dyf, p, h->st));
         CK(les_to_fourier(h, h->lb, 6, h->ls, 0, nyp));
         CK(launch_mlp_tau_cf(d, h->ls, h->cf, h->d_kx, h->d_kz, h->d_dy, h->d_dyf, h->st));
@@ -912,8 +913,8 @@ int diablo_gpu_download_nu_t(void* handle, double* nu_t) {
 
 static int ensure_work(Handle* h);
 
-int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float* t, long long capacity,
-                           long long* n) {
+int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float* t, float* scale,
+                           long long capacity, long long* n) {
     Handle* h = (Handle*)handle;
     if (!h || !n) return fail(DIABLO_EINVAL, "null pointer argument");
     const Dims& d = h->d;
@@ -922,7 +923,7 @@ int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float*
     if (stride < 1) return fail(DIABLO_EINVAL, "stride must be >= 1");
     const long long ns = (long long)(d.ny - 2) * ((d.nx + stride - 1) / stride) * ((d.nz + stride - 1) / stride);
     *n = ns;
-    if (!x || !t || capacity < ns) return fail(DIABLO_EINVAL, "sample arrays too small (the count is in *n)");
+    if (!x || !t || !scale || capacity < ns) return fail(DIABLO_EINVAL, "sample arrays too small (the count is in *n)");
     int rc = ensure_work(h);
     if (rc) return rc;
     const size_t pf = (size_t)d.nyp * d.nz * d.nx;
@@ -930,16 +931,20 @@ int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float*
     for (int f = 0; f < 3; ++f)
         CK(launch_xinv(d, (const double2*)h->xb + (size_t)f * h->x_field, h->pw + (size_t)f * pf, 0, d.nyp, h->pm,
                        h->twm_d, h->twn_d, h->st));
-    float *dx_ = nullptr, *dt_ = nullptr;
+    float *dx_ = nullptr, *dt_ = nullptr, *ds_ = nullptr;
     cudaError_t e = cudaMalloc((void**)&dx_, sizeof(float) * 11 * (size_t)ns);
     if (e == cudaSuccess) e = cudaMalloc((void**)&dt_, sizeof(float) * 6 * (size_t)ns);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&ds_, sizeof(float) * (size_t)ns);
     if (e == cudaSuccess)
-        e = launch_sgs_samples(d, h->pw, h->d_gyf, h->d_dyf, h->dx, h->dz, h->p.nu, width, stride, dx_, dt_, h->st);
+        e = launch_sgs_samples(d, h->pw, h->d_gyf, h->d_dyf, h->dx, h->dz, h->p.nu, width, stride, dx_, dt_, ds_,
+                               h->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(x, dx_, sizeof(float) * 11 * (size_t)ns, cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(t, dt_, sizeof(float) * 6 * (size_t)ns, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(scale, ds_, sizeof(float) * (size_t)ns, cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
     cudaFree(dx_);
     cudaFree(dt_);
+    cudaFree(ds_);
     h->launches += 5;
     if (e != cudaSuccess) return fail(DIABLO_ECUDA, std::string("closure samples: ") + cudaGetErrorString(e));
     return DIABLO_OK;
@@ -953,10 +958,12 @@ int diablo_gpu_set_sgs_mlp(void* handle, void* mlp) {
         const size_t n = (size_t)(h->d.ny - 2) * h->d.nz * h->d.nx;
         cudaError_t e = cudaMalloc((void**)&h->mlp_x, sizeof(float) * 11 * n);
         if (e == cudaSuccess) e = cudaMalloc((void**)&h->mlp_t, sizeof(float) * 6 * n);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&h->mlp_s, sizeof(float) * n);
         if (e != cudaSuccess) {
             cudaFree(h->mlp_x);
             cudaFree(h->mlp_t);
-            h->mlp_x = h->mlp_t = nullptr;
+            cudaFree(h->mlp_s);
+            h->mlp_x = h->mlp_t = h->mlp_s = nullptr;
             return fail(DIABLO_ENOMEM, std::string("closure buffers: ") + cudaGetErrorString(e));
         }
     }

@@ -117,14 +117,15 @@ cudaError_t launch_les_solve(const LesArgs& a, double* r, const double* nut, dou
 // widths[NY+2..] = Delta_Y.  sij: the six physical strain fields, u: U1..U3.
 cudaError_t launch_dyn_widths(const Dims& d, const double* sij, const double* u, const double2* cu, const double* dy,
                               const double* dyf, double R, double* sums, double* widths, cudaStream_t st);
-// Closure samples (features [n][11], targets [n][6]) of a w x w x-z top-hat
+// Closure samples (features [n][11], targets [n][6], scales [n]; t may be
+// null) of a w x w x-z top-hat
 // filter at GYF points J = 2..NY-1 and every stride-th x and z point.
 cudaError_t launch_sgs_samples(const Dims& d, const double* u, const double* gyf, const double* dyf, double dx,
-                               double dz, double nu, int w, int stride, float* x, float* t, cudaStream_t st);
+                               double dz, double nu, int w, int stride, float* x, float* t, float* sc, cudaStream_t st);
 // The closure's stresses ([n][6] at GYF rows 2..NY-1) to six physical fields
 // (11, 22, 33, 13 at GYF; 12, 23 at GY), and their divergence into CF.
-cudaError_t launch_mlp_tau_fields(const Dims& d, const float* tau, const double* dy, const double* dyf, double* out,
-                                  cudaStream_t st);
+cudaError_t launch_mlp_tau_fields(const Dims& d, const float* tau, const float* sc, const double* dy, const double* dyf,
+                                  double* out, cudaStream_t st);
 cudaError_t launch_mlp_tau_cf(const Dims& d, const double2* tau, double2* cf, const double* kx, const double* kz,
                               const double* dy, const double* dyf, cudaStream_t st);
 // COURANT's velocity minimum over physical rows 1..NY of U1..U3 (u: 3 fields).

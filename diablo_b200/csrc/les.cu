@@ -596,15 +596,18 @@ __global__ void k_dyn_widths(Dims d, const double* __restrict__ sums, const doub
 // Samples for the learned closure: from physical U1..U3, at GYF points
 // J = 2..NY-1 and every `stride`-th x and z point, the features and targets
 // of a w x w top-hat filter in x and z (periodic; w odd), one thread per
-// sample.  U2 is averaged to GYF before filtering.  Features: the 9
-// gradients d(ubar_i)/dx_j (i-major; centred differences over one cell in x
-// and z, over GYF(J+-1) in y), y+ = (distance to the nearer of GYF(1),
-// GYF(NY)) / NU and Delta = (w DX DYF(J) w DZ)^(1/3).  Targets: tau_ij =
-// bar(u_i u_j) - ubar_i ubar_j in the order 11, 22, 33, 12, 13, 23.
+// sample.  U2 is averaged to GYF before filtering.  The gradients
+// g_ij = d(ubar_i)/dx_j (i-major; centred differences over one cell in x and
+// z, over GYF(J+-1) in y) enter in dimensionless form: features g_ij / G
+// with G = |g|, then y+ = (distance to the nearer of GYF(1), GYF(NY)) / NU
+// and Delta = (w DX DYF(J) w DZ)^(1/3); the stress scale is s = Delta^2 G^2.
+// Targets (when t is given): tau_ij / s, tau_ij = bar(u_i u_j) - ubar_i
+// ubar_j in the order 11, 22, 33, 12, 13, 23 (zero where s = 0).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(TB) k_sgs_samples(Dims d, const double* __restrict__ u, const double* __restrict__ gyf,
                                                     const double* __restrict__ dyf, double dx, double dz, double nu,
-                                                    int w, int stride, float* __restrict__ x, float* __restrict__ t) {
+                                                    int w, int stride, float* __restrict__ x, float* __restrict__ t,
+                                                    float* __restrict__ sc) {
     const int nx = d.nx, nz = d.nz, ny = d.ny;
     const int nxs = (nx + stride - 1) / stride, nzs = (nz + stride - 1) / stride;
     const long long ns = (long long)(ny - 2) * nzs * nxs;
@@ -629,14 +632,21 @@ __global__ void __launch_bounds__(TB) k_sgs_samples(Dims d, const double* __rest
     };
     float* xo = x + s * 11;
     const double hy = gyf[J + 1] - gyf[J - 1];
+    double gr[9], g2 = 0.0;
     for (int c = 0; c < 3; ++c) {
-        xo[3 * c + 0] = (float)((bar(c, J, i + 1, k) - bar(c, J, i - 1, k)) / (2.0 * dx));
-        xo[3 * c + 1] = (float)((bar(c, J + 1, i, k) - bar(c, J - 1, i, k)) / hy);
-        xo[3 * c + 2] = (float)((bar(c, J, i, k + 1) - bar(c, J, i, k - 1)) / (2.0 * dz));
+        gr[3 * c + 0] = (bar(c, J, i + 1, k) - bar(c, J, i - 1, k)) / (2.0 * dx);
+        gr[3 * c + 1] = (bar(c, J + 1, i, k) - bar(c, J - 1, i, k)) / hy;
+        gr[3 * c + 2] = (bar(c, J, i, k + 1) - bar(c, J, i, k - 1)) / (2.0 * dz);
     }
+    for (int q = 0; q < 9; ++q) g2 += gr[q] * gr[q];
+    const double G = sqrt(g2), ig = G > 0.0 ? 1.0 / G : 0.0;
+    for (int q = 0; q < 9; ++q) xo[q] = (float)(gr[q] * ig);
     const double dwall = fmin(gyf[J] - gyf[1], gyf[ny] - gyf[J]);
+    const double delta = cbrt((double)w * dx * dyf[J] * (double)w * dz);
     xo[9] = (float)(dwall / nu);
-    xo[10] = (float)cbrt((double)w * dx * dyf[J] * (double)w * dz);
+    xo[10] = (float)delta;
+    const double scale = delta * delta * g2;
+    sc[s] = (float)scale;
     if (!t) return;
     float* to = t + s * 6;
     double ub[3] = {bar(0, J, i, k), bar(1, J, i, k), bar(2, J, i, k)};
@@ -647,23 +657,28 @@ __global__ void __launch_bounds__(TB) k_sgs_samples(Dims d, const double* __rest
             pr[0] += a * a; pr[1] += b * b; pr[2] += c * c; pr[3] += a * b; pr[4] += a * c; pr[5] += b * c;
         }
     const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
-    for (int q = 0; q < 6; ++q) to[q] = (float)(pr[q] * inv - ub[pa[q]] * ub[pb[q]]);
+    const double is = scale > 0.0 ? 1.0 / scale : 0.0;
+    for (int q = 0; q < 6; ++q) to[q] = (float)((pr[q] * inv - ub[pa[q]] * ub[pb[q]]) * is);
 }
 
-// The closure's stresses at GYF points J = 2..NY-1 (tau [n][6] in the
-// sampler's order, every x and z point) into physical fields: tau_11,
+// The closure's stresses at GYF points J = 2..NY-1 (the network's
+// dimensionless output y [n][6] in the sampler's order times the sample's
+// scale s, every x and z point) into physical fields: tau_11,
 // tau_22, tau_33, tau_13 at GYF points; tau_12, tau_23 interpolated to GY
 // points J = 3..NY-1 with the weights of the GY interpolation of channel.f
 // (DYF(J-1), DYF(J)); all other rows zero.  out: 6 fields [J][z][x].
 __global__ void __launch_bounds__(TB) k_mlp_tau_fields(Dims d, const float* __restrict__ tau,
-                                                       const double* __restrict__ dy, const double* __restrict__ dyf,
-                                                       double* __restrict__ out) {
+                                                       const float* __restrict__ sc, const double* __restrict__ dy,
+                                                       const double* __restrict__ dyf, double* __restrict__ out) {
     const size_t pp = plane_pts(d), pf = pp * d.nyp;
     const size_t g = (size_t)blockIdx.x * TB + threadIdx.x;
     if (g >= pf) return;
     const int J = (int)(g / pp), ny = d.ny;
     const size_t col = g % pp;
-    auto T = [&](int q, int j) { return (double)tau[((size_t)(j - 2) * pp + col) * 6 + q]; };
+    auto T = [&](int q, int j) {
+        const size_t e = (size_t)(j - 2) * pp + col;
+        return (double)(tau[e * 6 + q] * sc[e]);
+    };
     const bool f = J >= 2 && J <= ny - 1;
     out[g] = f ? T(0, J) : 0.0;              // 11
     out[pf + g] = f ? T(1, J) : 0.0;         // 22
@@ -811,17 +826,17 @@ cudaError_t launch_dyn_widths(const Dims& d, const double* sij, const double* u,
 }
 
 cudaError_t launch_sgs_samples(const Dims& d, const double* u, const double* gyf, const double* dyf, double dx,
-                               double dz, double nu, int w, int stride, float* x, float* t, cudaStream_t st) {
+                               double dz, double nu, int w, int stride, float* x, float* t, float* sc, cudaStream_t st) {
     const int nxs = (d.nx + stride - 1) / stride, nzs = (d.nz + stride - 1) / stride;
     const long long ns = (long long)(d.ny - 2) * nzs * nxs;
     if (ns <= 0) return cudaSuccess;
-    k_sgs_samples<<<(unsigned)((ns + TB - 1) / TB), TB, 0, st>>>(d, u, gyf, dyf, dx, dz, nu, w, stride, x, t);
+    k_sgs_samples<<<(unsigned)((ns + TB - 1) / TB), TB, 0, st>>>(d, u, gyf, dyf, dx, dz, nu, w, stride, x, t, sc);
     return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_tau_fields(const Dims& d, const float* tau, const double* dy, const double* dyf, double* out,
-                                  cudaStream_t st) {
-    k_mlp_tau_fields<<<blocks(plane_pts(d) * d.nyp), TB, 0, st>>>(d, tau, dy, dyf, out);
+cudaError_t launch_mlp_tau_fields(const Dims& d, const float* tau, const float* sc, const double* dy, const double* dyf,
+                                  double* out, cudaStream_t st) {
+    k_mlp_tau_fields<<<blocks(plane_pts(d) * d.nyp), TB, 0, st>>>(d, tau, sc, dy, dyf, out);
     return cudaGetLastError();
 }
 

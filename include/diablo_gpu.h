@@ -255,8 +255,9 @@ const char* diablo_gpu_last_error(void);
 /* ------------------------------------------------------------------------ */
 /* Learned subgrid-stress closure.  The reference has no counterpart: it is   */
 /* this library's MLP from the 9 resolved velocity gradients du_i/dx_j        */
-/* (i-major), the wall distance in viscous units y+ and the filter width to   */
-/* the 6 stresses (tau_11, tau_22, tau_33, tau_12, tau_13, tau_23), through 3 */
+/* (i-major, divided by their norm G), the wall distance in viscous units y+  */
+/* and the filter width Delta to the 6 stresses (tau_11, tau_22, tau_33,      */
+/* tau_12, tau_13, tau_23) divided by Delta^2 G^2, through 3                  */
 /* hidden layers of 64 GELU units.  Weights and activations are BF16 on the   */
 /* tensor cores with FP32 accumulation; parameters, gradients and the Adam    */
 /* state are FP32 on the device.                                              */
@@ -276,7 +277,8 @@ int diablo_mlp_destroy(void* mlp);
 /* Set all parameters (scales must be non-zero); resets the Adam state. */
 int diablo_mlp_set_params(void* mlp, const float* params);
 int diablo_mlp_get_params(void* mlp, float* params);
-/* x: host [n][11] features; y: host [n][6] stresses. */
+/* x: host [n][11] features; y: host [n][6] outputs (dimensionless stresses
+ * in the closure's use). */
 int diablo_mlp_forward(void* mlp, const float* x, long long n, float* y);
 /* Loss sum_samples sum_outputs (y/out_scale - t/out_scale)^2 / (2n) and its
  * gradient with respect to the DIABLO_MLP_NTRAIN trained parameters. */
@@ -290,18 +292,22 @@ int diablo_mlp_train(void* mlp, const float* x, const float* t, long long n, int
 /* Training samples from a channel instance's current state (the reference
  * has no counterpart): a width x width top-hat filter in x and z (periodic,
  * width odd) of the velocity, at GYF points J = 2..NY-1 and every stride-th
- * x and z point, J-major then z then x.  x receives [n][11] features
- * (d ubar_i/dx_j i-major, y+, Delta; see DIABLO_MLP_NIN), t [n][6] targets
- * tau_ij = bar(u_i u_j) - ubar_i ubar_j (11, 22, 33, 12, 13, 23), with
- * n = (NY-2) ceil(NX/stride) ceil(NZ/stride) written to *n; arrays shorter
- * than that (capacity samples) give DIABLO_EINVAL with *n set. */
-int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float* t, long long capacity,
-                           long long* n);
+ * x and z point, J-major then z then x.  With g_ij = d ubar_i/dx_j
+ * (i-major), G = |g| and Delta = (width DX DYF(J) width DZ)^(1/3):
+ * x receives [n][11] features (g_ij / G, y+, Delta), scale [n] the stress
+ * scale s = Delta^2 G^2 and t [n][6] the targets tau_ij / s, tau_ij =
+ * bar(u_i u_j) - ubar_i ubar_j (11, 22, 33, 12, 13, 23); the closure's
+ * network works in this dimensionless form.  n = (NY-2) ceil(NX/stride)
+ * ceil(NZ/stride) is written to *n; arrays shorter than that (capacity
+ * samples) give DIABLO_EINVAL with *n set. */
+int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float* t, float* scale,
+                           long long capacity, long long* n);
 /* Attach a closure network to an LES instance (NULL detaches; the caller
  * keeps ownership and must not change its parameters while a substage that
  * uses it runs).  With LES_MODEL_TYPE 4, each LES substage then computes the
- * features of the resolved field (width 1, every point of rows 2..NY-1), the
- * network's stresses, tau_12 and tau_23 interpolated to GY points, and
+ * features of the resolved field (width 1, every point of rows 2..NY-1, as
+ * diablo_gpu_sgs_samples), the network's outputs times Delta^2 G^2 as the
+ * stresses, tau_12 and tau_23 interpolated to GY points, and
  * CF_i -= d tau_ij / dx_j explicitly, in place of the eddy-viscosity model
  * (NU_T stays zero); without a network type 4 runs the dynamic model.  The
  * reference has no counterpart. */

@@ -833,8 +833,9 @@ static void dynamic_widths(orc_state* s, const double* U1_bar, const double* U3_
 
 /* The learned closure (LES_MODEL_TYPE 4), which the reference does not
  * have: the features of the resolved field at GYF rows J = 2..NY-1 (the
- * velocity gradients by centred differences, U2 averaged to GYF, y+ and the
- * grid filter width), the MLP of the GPU library with its weights,
+ * velocity gradients by centred differences, U2 averaged to GYF, divided by
+ * their norm G; y+ and the grid filter width Delta), the MLP of the GPU
+ * library, whose outputs times Delta^2 G^2 are the stresses, with its weights,
  * normalised inputs and hidden activations rounded to bfloat16 as its
  * tensor cores see them, tau_12 and tau_23 interpolated to GY points, and
  * CF_i -= d tau_ij / dx_j, all explicit. */
@@ -932,11 +933,18 @@ static void les_mlp(orc_state* s) {
                     x[3 * c + 2] = (UU(i, kp, j) - UU(i, km, j)) / (2.0 * s->DZ);
 #undef UU
                 }
+                double g2 = 0.0;
+                for (int q = 0; q < 9; ++q) g2 += x[q] * x[q];
+                const double G = sqrt(g2), ig = G > 0.0 ? 1.0 / G : 0.0;
+                for (int q = 0; q < 9; ++q) x[q] *= ig;
                 x[9] = fmin(GYF[j] - GYF[1], GYF[NY] - GYF[j]) / s->p.nu;
                 x[10] = cbrt(s->DX * DYF[j] * s->DZ);
+                const float sc = (float)(x[10] * x[10] * g2);
                 float xf[MLP_NIN];
                 for (int q = 0; q < MLP_NIN; ++q) xf[q] = (float)x[q];
-                mlp_forward(s->MLP, xf, tau + (((size_t)j * NZ + k) * NX + i) * 6);
+                float* y = tau + (((size_t)j * NZ + k) * NX + i) * 6;
+                mlp_forward(s->MLP, xf, y);
+                for (int q = 0; q < 6; ++q) y[q] = y[q] * sc;
             }
     /* 11, 22, 33, 13 at GYF rows 2..NY-1; 12, 23 at GY rows 3..NY-1 */
 #define TAU(q, i, k, j) ((double)tau[(((size_t)(j) * NZ + (k)) * NX + (i)) * 6 + (q)])

@@ -12,7 +12,8 @@ import numpy as np
 
 def samples(u1, u2, u3, gyf, dyf, dx, dz, nu, w, stride):
     """u1, u2, u3: physical fields [NY+2][NZ][NX] (U2 at GY points).
-    Returns features [n][11] and targets [n][6] in FP64, n = (NY-2) *
+    Returns the dimensionless features [n][11] (g_ij/G, y+, Delta), targets
+    [n][6] (tau_ij / s) and scales s = Delta^2 G^2 [n] in FP64, n = (NY-2) *
     ceil(NX/stride) * ceil(NZ/stride), J-major then z then x."""
     ny = u1.shape[0] - 2
     u2f = np.zeros_like(u2)
@@ -45,4 +46,9 @@ def samples(u1, u2, u3, gyf, dyf, dx, dz, nu, w, stride):
     sl = (slice(None), slice(None, None, stride), slice(None, None, stride))
     x = np.stack([f[sl].reshape(-1) for f in feats], axis=1)
     t = np.stack([a[js][sl].reshape(-1) for a in tau], axis=1)
-    return x, t
+    g2 = np.sum(x[:, :9] ** 2, axis=1)
+    G = np.sqrt(g2)
+    x[:, :9] = np.where(G[:, None] > 0, x[:, :9] / np.where(G > 0, G, 1.0)[:, None], 0.0)
+    s = x[:, 10] ** 2 * g2
+    t = np.where(s[:, None] > 0, t / np.where(s > 0, s, 1.0)[:, None], 0.0)
+    return x, t, s

@@ -108,12 +108,13 @@ def test_les_rejected_configurations():
 
 # --- the learned closure (LES_MODEL_TYPE 4) ----------------------------------
 
-def closure_params(seed=21, out=1e-2):
+def closure_params(seed=21, out=1e-3):
     """A seeded network whose inputs are normalised by the features' typical
-    sizes in this flow and whose stresses are O(out)."""
+    sizes (the gradients enter divided by their norm) and whose
+    dimensionless stresses are O(out)."""
     from diablo_b200 import mlp as ML
     mean = np.zeros(11)
-    scale = np.concatenate([np.full(9, 20.0), [60.0, 0.1]])
+    scale = np.concatenate([np.full(9, 0.3), [60.0, 0.1]])
     return ML.init_params(seed, mean, scale, np.full(6, out))
 
 
@@ -143,19 +144,24 @@ def run_closure(p, g, u, th, dt, steps, params):
 def test_learned_closure_matches_oracle():
     """Closure stresses from the same BF16 network on both sides (the
     oracle rounds weights, inputs and activations to bfloat16 as the tensor
-    cores do, and accumulates in FP64 where the GPU uses FP32): the states
-    after 3 steps agree to 1e-7, set by those accumulations and by the
-    rare activations that round to different bfloat16 neighbours."""
+    cores do, and accumulates in FP64 where the GPU uses FP32).  After 3
+    steps the velocity agrees to 1e-9; CF and CP, which carry the stresses
+    directly (CP through phi/h), to 5e-7 -- the size of the few activations
+    that round to different bfloat16 neighbours -- while the closure itself
+    changes CF by far more than that."""
     p, g, u, th = les_channel(model=4)
     err, plain, s, o = run_closure(p, g, u, th, 2e-4, 3, closure_params())
-    assert max(err.values()) < 1e-7, (err, plain)
-    # the closure acted: the state differs from the run without any model
+    for k in ("cu1", "cu2", "cu3", "cth1"):
+        assert err[k] < 1e-9, (err, plain)
+    assert max(err.values()) < 5e-7, (err, plain)
+    # the closure's own effect, from the run without any model
     q = p.copy()
     q.les = 0
     o0 = Oracle(q, g, 2e-4)
     o0.init_from_physical(u, th)
     o0.step(3)
-    assert relerr(o.cu[0], o0.cu[0]) > 1e-9
+    effect = max(relerr(o.cf[c][2:p.ny + 1], o0.cf[c][2:p.ny + 1]) for c in range(3))
+    assert effect > 200 * max(err[k] for k in ("cf1", "cf2", "cf3")), (effect, err)
 
 
 def test_learned_closure_falls_back_to_dynamic_model():

@@ -2,7 +2,8 @@
 restatement (oracle/sgs_oracle.py) on the same state: the GPU's physical
 fields come from its own transforms, the oracle's from the CPU oracle's
 FFT_XZ_TO_PHYSICAL of the downloaded state, so the comparison covers both.
-Outputs are float32: per column, agreement to 1e-5 of the column's scale."""
+Outputs are float32: per column, agreement to 1e-5 of the column's scale
+(the targets, divided by the small scale Delta^2 G^2, to 1e-4)."""
 import numpy as np
 import pytest
 
@@ -25,18 +26,19 @@ def test_samples_match_oracle(width, stride):
     with Channel(p, g, 2e-4) as c:
         c.upload([x.copy() for x in o.cu], o.cp.copy(), o.cth.copy())
         c.step(2)
-        x, t = c.sgs_samples(width, stride)
+        x, t, sc = c.sgs_samples(width, stride)
         s = c.download()
     phys = []
     for k in range(3):
         v = new_physical(p)
         o.fft_xz_to_physical(s["cu"][k].copy(), v, 0, p.ny + 1)
         phys.append(v[:, : p.nz, : p.nx].copy())
-    xo, to = sgs_oracle.samples(*phys, g.gyf, g.dyf, p.lx / p.nx, p.lz / p.nz, p.nu, width, stride)
-    assert x.shape == xo.shape and t.shape == to.shape
-    for a, b in ((x, xo), (t, to)):
+    xo, to, so = sgs_oracle.samples(*phys, g.gyf, g.dyf, p.lx / p.nx, p.lz / p.nz, p.nu, width, stride)
+    assert x.shape == xo.shape and t.shape == to.shape and sc.shape == so.shape
+    for a, b in ((x, xo), (t, to), (sc[:, None], so[:, None])):
         scale = np.abs(b).max(axis=0)
         scale[scale == 0] = 1.0
-        assert (np.abs(a - b).max(axis=0) <= 1e-5 * scale).all(), np.abs(a - b).max(axis=0) / scale
+        tol = 1e-4 if a is t else 1e-5
+        assert (np.abs(a - b).max(axis=0) <= tol * scale).all(), np.abs(a - b).max(axis=0) / scale
     if width > 1:
         assert np.abs(t[:, 0]).max() > 0          # the filter leaves a subfilter stress
