@@ -24,6 +24,9 @@ LIB_PATH = os.path.join(_HERE, "libdiablo_gpu.so")
 DIABLO_OK, DIABLO_EINVAL, DIABLO_ERADIX, DIABLO_ECUDA, DIABLO_ENOTSUP, DIABLO_ENAN, DIABLO_ENOMEM, DIABLO_ETIMEOUT = (
     0, -1, -2, -3, -4, -5, -6, -7)
 NSTATS = 17
+# DIABLO_STAT_* rows of diablo_gpu_stats
+STAT_INDEX = {"ume": 0, "vme": 1, "wme": 2, "urms": 3, "vrms": 4, "wrms": 5, "uv": 6, "uw": 7, "wv": 8,
+              "dudy": 9, "dwdy": 10, "cp": 11, "shear": 12, "thme": 13, "dthdy": 14, "thrms": 15, "thv": 16}
 
 # C entry points declared in include/diablo_gpu.h
 EXPORTS = [

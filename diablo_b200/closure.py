@@ -181,3 +181,82 @@ def train_and_evaluate(data: Snapshots, seed: int, steps: int, batch: int = 1024
 
 
 assert NIN == 11 and NOUT == 6
+
+
+# --- a-posteriori comparison ---------------------------------------------------
+
+def coarsen(p_fine, a: np.ndarray, p_coarse) -> np.ndarray:
+    """Spectral truncation of a Fortran-layout Fourier array to the modes a
+    coarser x-z grid keeps (same y grid); the coefficients are normalised by
+    NX NZ on both grids, so they carry over unchanged."""
+    from .layout import new_fourier
+    out = new_fourier(p_coarse)
+    nkx, nkz = p_coarse.nx // 3, p_coarse.nz // 3
+    tf, tc = 2 * (p_fine.nz // 3), 2 * nkz
+    out[:, : nkz + 1, : nkx + 1] = a[:, : nkz + 1, : nkx + 1]
+    for k in range(1, nkz + 1):
+        out[:, tc + 1 - k, : nkx + 1] = a[:, tf + 1 - k, : nkx + 1]
+    return out
+
+
+def _profiles(stats: np.ndarray) -> dict:
+    from .channel import STAT_INDEX
+    return {k: stats[STAT_INDEX[k]] for k in ("ume", "urms", "vrms", "wrms", "uv")}
+
+
+def a_posteriori(p, grid, dt, u, th, steps: int, params: np.ndarray, factor: int = 3) -> dict:
+    """DNS on p's grid and LES on the grid coarsened `factor` times in x and
+    z, from the DNS's initial state truncated to the LES modes, `steps`
+    steps each; mean-velocity and Reynolds-stress profiles of each LES (no
+    model, the dynamic model, the closure with `params`) against the
+    filtered DNS (the final DNS state truncated the same way) as relative L2
+    errors over the planes."""
+    from .mlp import SgsMlp
+
+    q = p.copy()
+    q.nx, q.nz = p.nx // factor, p.nz // factor
+    q.les, q.create_new_flow = 1, 0
+    with Channel(p, grid, dt) as c:
+        c.init_from_physical(u, th)
+        s0 = c.download()
+        t0 = _time.perf_counter()
+        c.step(steps)
+        c.synchronize()
+        dns_seconds = _time.perf_counter() - t0
+        s1 = c.download()
+
+    def coarse_channel(s, model):
+        r = q.copy()
+        if model == 0:
+            r.les = 0
+        else:
+            r.les_model_type = model
+        ch = Channel(r, grid, dt)
+        ch.upload([coarsen(p, s["cu"][k], q) for k in range(3)], coarsen(p, s["cp"], q),
+                  np.stack([coarsen(p, s["cth"][n], q) for n in range(p.n_th)]) if p.n_th else None)
+        return ch
+
+    with coarse_channel(s1, 0) as ref:
+        target = _profiles(ref.stats())
+    out = {"dns_grid": [p.nx, p.ny, p.nz], "les_grid": [q.nx, q.ny, q.nz], "steps": steps, "dt": dt,
+           "dns_seconds": dns_seconds}
+    for name, model in (("no_model", 0), ("dynamic", 2), ("closure", 4)):
+        ch = coarse_channel(s0, model)
+        m = None
+        if model == 4:
+            m = SgsMlp(params)
+            ch.set_sgs_mlp(m)
+        t0 = _time.perf_counter()
+        ch.step(steps)
+        ch.synchronize()
+        el = _time.perf_counter() - t0
+        prof = _profiles(ch.stats())
+        ch.close()
+        if m is not None:
+            m.close()
+        err = {}
+        for k, ref_prof in target.items():
+            d = np.linalg.norm(prof[k] - ref_prof)
+            err[k] = float(d / max(np.linalg.norm(ref_prof), 1e-300)) if np.isfinite(d) else float("inf")
+        out[name] = {"profile_errors": err, "seconds": el}
+    return out
