@@ -633,10 +633,26 @@ __global__ void __launch_bounds__(TB) k_sgs_samples(Dims d, const double* __rest
     float* xo = x + s * 11;
     const double hy = gyf[J + 1] - gyf[J - 1];
     double gr[9], g2 = 0.0;
-    for (int c = 0; c < 3; ++c) {
-        gr[3 * c + 0] = (bar(c, J, i + 1, k) - bar(c, J, i - 1, k)) / (2.0 * dx);
-        gr[3 * c + 1] = (bar(c, J + 1, i, k) - bar(c, J - 1, i, k)) / hy;
-        gr[3 * c + 2] = (bar(c, J, i, k + 1) - bar(c, J, i, k - 1)) / (2.0 * dz);
+    if (w == 1) {
+        // unfiltered (the LES features): neighbours once, no modulo per access
+        const int ip = i + 1 < nx ? i + 1 : 0, im = i > 0 ? i - 1 : nx - 1;
+        const int kp = k + 1 < nz ? k + 1 : 0, km = k > 0 ? k - 1 : nz - 1;
+        const size_t o = (size_t)J * pp + (size_t)k * nx + i;
+        const size_t oxp = (size_t)J * pp + (size_t)k * nx + ip, oxm = (size_t)J * pp + (size_t)k * nx + im;
+        const size_t ozp = (size_t)J * pp + (size_t)kp * nx + i, ozm = (size_t)J * pp + (size_t)km * nx + i;
+        const double r2x = 0.5 / dx, r2z = 0.5 / dz, rhy = 1.0 / hy;
+        for (int c = 0; c < 3; ++c) {
+            auto at = [&](size_t q) { return c == 1 ? 0.5 * (u[pf + q] + u[pf + q + pp]) : u[(size_t)c * pf + q]; };
+            gr[3 * c + 0] = (at(oxp) - at(oxm)) * r2x;
+            gr[3 * c + 1] = (at(o + pp) - at(o - pp)) * rhy;
+            gr[3 * c + 2] = (at(ozp) - at(ozm)) * r2z;
+        }
+    } else {
+        for (int c = 0; c < 3; ++c) {
+            gr[3 * c + 0] = (bar(c, J, i + 1, k) - bar(c, J, i - 1, k)) / (2.0 * dx);
+            gr[3 * c + 1] = (bar(c, J + 1, i, k) - bar(c, J - 1, i, k)) / hy;
+            gr[3 * c + 2] = (bar(c, J, i, k + 1) - bar(c, J, i, k - 1)) / (2.0 * dz);
+        }
     }
     for (int q = 0; q < 9; ++q) g2 += gr[q] * gr[q];
     const double G = sqrt(g2), ig = G > 0.0 ? 1.0 / G : 0.0;

@@ -4,8 +4,8 @@
 // The reference has no such model; this is the library's own.
 //
 // Arithmetic: weights and activations in BF16 on the tensor cores
-// (mma.sync m16n8k16, BF16 x BF16 -> FP32), accumulation, biases, GELU,
-// losses, gradients and the Adam state in FP32.  Each warp owns a tile of
+// (mma.sync m16n8k16, BF16 x BF16 -> FP32), accumulation, biases, GELU (tanh
+// form), losses, gradients and the Adam state in FP32.  Each warp owns a tile of
 // 16 samples.  Every product is a 16 x 8 x 16 tile read from shared memory
 // with one of four fragment loaders, so the forward pass (H W^T), the
 // backward pass (delta W) and the weight gradients (delta^T H) share them.
@@ -84,9 +84,25 @@ __device__ __forceinline__ void ldb_row(uint32_t (&b)[2], const uint16_t* s, int
     b[1] = pack2(s[(2 * t + 8) * ld + g], s[(2 * t + 9) * ld + g]);
 }
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))),
+// with tanh u = 1 - 2 / (exp(2u) + 1) on the clamped argument (|u| <= 9,
+// where tanh is 1 to FP32 precision) from the fast exponential; and its
+// derivative for the backward pass.
+__device__ __forceinline__ float tanh_c(float u) {
+    u = fminf(fmaxf(u, -9.0f), 9.0f);
+    return 1.0f - __fdividef(2.0f, __expf(2.0f * u) + 1.0f);
+}
+__device__ __forceinline__ float gelu(float z) {
+    return 0.5f * z * (1.0f + tanh_c(0.79788456080286536f * (z + 0.044715f * z * z * z)));
+}
 __device__ __forceinline__ float gelu_d(float z) {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+    const float t = tanh_c(0.79788456080286536f * (z + 0.044715f * z * z * z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * 0.79788456080286536f * (1.0f + 0.134145f * z * z);
+}
+// two floats to a packed BF16 pair (round to nearest even), low half first
+__device__ __forceinline__ uint32_t bf2(float lo, float hi) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&h);
 }
 
 struct MlpDev {
@@ -181,35 +197,94 @@ __device__ void forward_tile(const uint16_t* sw, const float* sb, const WarpTile
     for (int q = 0; q < 4; ++q) y[q] = acc[q];
 }
 
-constexpr size_t fwd_smem() {
-    return sizeof(uint16_t) * (SWN + NW * (TS * LD1 + 3 * TS * LDW)) + sizeof(float) * (3 * NH + 8);
+constexpr size_t fwd_smem() { return sizeof(uint16_t) * SWN + sizeof(float) * (3 * NH + 8); }
+
+// Inference: activations stay in registers.  The m16n8 accumulators of n
+// tiles 2kt and 2kt+1 hold exactly the m16k16 A fragment of k tile kt of the
+// next layer, so a layer's GELU output is packed to BF16 in place and fed to
+// the next layer's mma without touching shared memory; only the weights
+// (B fragments) are read from it.  The inputs are read straight from
+// global memory into the first layer's A fragment.  8 warps per block,
+// grid-stride over 16-sample tiles.
+constexpr int FW = 8;   // warps per inference block
+
+__device__ __forceinline__ void gelu_pack(const float (&acc)[NH / 8][4], uint32_t (&a)[NH / 16][4]) {
+#pragma unroll
+    for (int kt = 0; kt < NH / 16; ++kt) {
+        a[kt][0] = bf2(gelu(acc[2 * kt][0]), gelu(acc[2 * kt][1]));
+        a[kt][1] = bf2(gelu(acc[2 * kt][2]), gelu(acc[2 * kt][3]));
+        a[kt][2] = bf2(gelu(acc[2 * kt + 1][0]), gelu(acc[2 * kt + 1][1]));
+        a[kt][3] = bf2(gelu(acc[2 * kt + 1][2]), gelu(acc[2 * kt + 1][3]));
+    }
 }
 
-__global__ void __launch_bounds__(32 * NW) k_mlp_forward(MlpDev m, const float* __restrict__ x, long long n,
+__global__ void __launch_bounds__(32 * FW) k_mlp_forward(MlpDev m, const float* __restrict__ x, long long n,
                                                           float* __restrict__ y) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint16_t* sw = reinterpret_cast<uint16_t*>(smem);
-    uint16_t* tiles = sw + SWN;
-    float* sb = reinterpret_cast<float*>(tiles + NW * (TS * LD1 + 3 * TS * LDW));
+    float* sb = reinterpret_cast<float*>(sw + SWN);
+    __shared__ float s_mean[NIN], s_scale[NIN], s_out[NOUT];
     load_weights(m, sw, sb);
+    if (threadIdx.x < NIN) {
+        s_mean[threadIdx.x] = m.p[OMEAN + threadIdx.x];
+        s_scale[threadIdx.x] = m.p[OSCALE + threadIdx.x];
+    }
+    if (threadIdx.x < NOUT) s_out[threadIdx.x] = m.p[OOUT + threadIdx.x];
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    WarpTiles w;
-    w.x = tiles + warp * (TS * LD1 + 3 * TS * LDW);
-    for (int l = 0; l < 3; ++l) { w.h[l] = w.x + TS * LD1 + l * TS * LDW; w.z[l] = nullptr; }
     const long long ntile = (n + TS - 1) / TS;
-    for (long long tile = (long long)blockIdx.x * NW + warp; tile < ntile; tile += (long long)gridDim.x * NW) {
+    for (long long tile = (long long)blockIdx.x * FW + warp; tile < ntile; tile += (long long)gridDim.x * FW) {
         const long long s0 = tile * TS;
-        load_inputs(m, x, n, s0, w.x, lane);
-        __syncwarp();
-        float o[4];
-        forward_tile(sw, sb, w, o, g, t);
+        // layer-1 A fragment: normalised inputs of rows g, g+8, columns 2t..2t+1, 2t+8..2t+9
+        auto xin = [&](int r, int c) -> uint16_t {
+            if (c >= NIN || s0 + r >= n) return 0;
+            return bf((x[(s0 + r) * NIN + c] - s_mean[c]) / s_scale[c]);
+        };
+        uint32_t a1[4];
+        a1[0] = pack2(xin(g, 2 * t), xin(g, 2 * t + 1));
+        a1[1] = pack2(xin(g + 8, 2 * t), xin(g + 8, 2 * t + 1));
+        a1[2] = pack2(xin(g, 2 * t + 8), xin(g, 2 * t + 9));
+        a1[3] = pack2(xin(g + 8, 2 * t + 8), xin(g + 8, 2 * t + 9));
+        float acc[NH / 8][4];
+#pragma unroll
+        for (int nt = 0; nt < NH / 8; ++nt) {
+            const float b0 = sb[nt * 8 + 2 * t], b1 = sb[nt * 8 + 2 * t + 1];
+            acc[nt][0] = b0; acc[nt][1] = b1; acc[nt][2] = b0; acc[nt][3] = b1;
+            uint32_t b[2];
+            ldb_col(b, sw + SW1 + nt * 8 * LD1, LD1, g, t);
+            mma(acc[nt], a1, b);
+        }
+        uint32_t a[NH / 16][4];
+#pragma unroll
+        for (int l = 1; l < 3; ++l) {
+            gelu_pack(acc, a);
+            const uint16_t* W = sw + (l == 1 ? SW2 : SW3);
+            const float* bias = sb + l * NH;
+#pragma unroll
+            for (int nt = 0; nt < NH / 8; ++nt) {
+                const float b0 = bias[nt * 8 + 2 * t], b1 = bias[nt * 8 + 2 * t + 1];
+                acc[nt][0] = b0; acc[nt][1] = b1; acc[nt][2] = b0; acc[nt][3] = b1;
+#pragma unroll
+                for (int kt = 0; kt < NH / 16; ++kt) {
+                    uint32_t b[2];
+                    ldb_col(b, W + nt * 8 * LDW + kt * 16, LDW, g, t);
+                    mma(acc[nt], a[kt], b);
+                }
+            }
+        }
+        gelu_pack(acc, a);
+        float o[4] = {sb[3 * NH + 2 * t], sb[3 * NH + 2 * t + 1], sb[3 * NH + 2 * t], sb[3 * NH + 2 * t + 1]};
+#pragma unroll
+        for (int kt = 0; kt < NH / 16; ++kt) {
+            uint32_t b[2];
+            ldb_col(b, sw + SW4 + kt * 16, LDW, g, t);
+            mma(o, a[kt], b);
+        }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int r = g + (q >> 1) * 8, c = 2 * t + (q & 1);
-            if (c < NOUT && s0 + r < n) y[(s0 + r) * NOUT + c] = o[q] * m.p[OOUT + c];
+            if (c < NOUT && s0 + r < n) y[(s0 + r) * NOUT + c] = o[q] * s_out[c];
         }
-        __syncwarp();
     }
 }
 
@@ -465,10 +540,10 @@ cudaError_t launch_mlp_forward(const void* mlp, const float* x, long long n, flo
     const size_t smem = fwd_smem();
     cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const long long tiles = (n + TS - 1) / TS;
-    long long nb = (tiles + NW - 1) / NW;
-    if (nb > 148 * 8) nb = 148 * 8;
+    long long nb = (tiles + FW - 1) / FW;
+    if (nb > 148 * 4) nb = 148 * 4;
     if (nb < 1) return cudaSuccess;
-    k_mlp_forward<<<(unsigned)nb, 32 * NW, smem, st>>>(md, x, n, y);
+    k_mlp_forward<<<(unsigned)nb, 32 * FW, smem, st>>>(md, x, n, y);
     return cudaGetLastError();
 }
 

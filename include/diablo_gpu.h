@@ -257,8 +257,8 @@ const char* diablo_gpu_last_error(void);
 /* this library's MLP from the 9 resolved velocity gradients du_i/dx_j        */
 /* (i-major, divided by their norm G), the wall distance in viscous units y+  */
 /* and the filter width Delta to the 6 stresses (tau_11, tau_22, tau_33,      */
-/* tau_12, tau_13, tau_23) divided by Delta^2 G^2, through 3                  */
-/* hidden layers of 64 GELU units.  Weights and activations are BF16 on the   */
+/* tau_12, tau_13, tau_23) divided by Delta^2 G^2, through 3 hidden layers   */
+/* of 64 GELU units (tanh form).  Weights and activations are BF16 on the     */
 /* tensor cores with FP32 accumulation; parameters, gradients and the Adam    */
 /* state are FP32 on the device.                                              */
 /*                                                                            */

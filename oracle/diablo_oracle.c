@@ -861,6 +861,11 @@ void orc_set_mlp(orc_state* s, const float* params) {
     memcpy(s->MLP, params, sizeof(float) * n);
 }
 
+/* GELU in its tanh form, as the GPU library evaluates it */
+static double mlp_gelu(double z) {
+    return 0.5 * z * (1.0 + tanh(sqrt(2.0 / (4.0 * atan(1.0))) * (z + 0.044715 * z * z * z)));
+}
+
 static void mlp_forward(const float* P, const float* xf, float* y) {
     const float* W1 = P;
     const float* b1 = W1 + MLP_NH * MLP_NIN;
@@ -878,7 +883,7 @@ static void mlp_forward(const float* P, const float* xf, float* y) {
     for (int o = 0; o < MLP_NH; ++o) {
         double z = b1[o];
         for (int k = 0; k < MLP_NIN; ++k) z += (double)bf16r(W1[o * MLP_NIN + k]) * x[k];
-        h[o] = bf16r((float)(0.5 * z * (1.0 + erf(z / sqrt(2.0)))));
+        h[o] = bf16r((float)mlp_gelu(z));
     }
     const float* Ws[2] = {W2, W3};
     const float* bs[2] = {b2, b3};
@@ -886,7 +891,7 @@ static void mlp_forward(const float* P, const float* xf, float* y) {
         for (int o = 0; o < MLP_NH; ++o) {
             double z = bs[l][o];
             for (int k = 0; k < MLP_NH; ++k) z += (double)bf16r(Ws[l][o * MLP_NH + k]) * h[k];
-            g[o] = bf16r((float)(0.5 * z * (1.0 + erf(z / sqrt(2.0)))));
+            g[o] = bf16r((float)mlp_gelu(z));
         }
         memcpy(h, g, sizeof(h));
     }

@@ -9,7 +9,8 @@ checked against finite differences of itself (tests/test_oracle_mlp.py).
 
 Parameter vector layout (float, as the C ABI): W1[64][11] b1[64] W2[64][64]
 b2[64] W3[64][64] b3[64] W4[6][64] b4[6] | in_mean[11] in_scale[11]
-out_scale[6].  GELU is the exact 0.5 z (1 + erf(z / sqrt 2)).
+out_scale[6].  GELU is its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z +
+0.044715 z^3))).
 """
 from __future__ import annotations
 
@@ -23,7 +24,7 @@ SHAPES = [("W1", (NH, NIN)), ("b1", (NH,)), ("W2", (NH, NH)), ("b2", (NH,)), ("W
 NTRAIN = sum(int(np.prod(s)) for _, s in SHAPES)
 NPARAM = NTRAIN + NIN + NIN + NOUT
 
-_erf = np.vectorize(math.erf, otypes=[np.float64])
+_C = math.sqrt(2.0 / math.pi)
 
 
 def unpack(p: np.ndarray) -> dict:
@@ -49,11 +50,12 @@ def bf16(a: np.ndarray) -> np.ndarray:
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    return 0.5 * z * (1.0 + np.tanh(_C * (z + 0.044715 * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(_C * (z + 0.044715 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _C * (1.0 + 3 * 0.044715 * z * z)
 
 
 def forward(p: np.ndarray, x: np.ndarray, emulate_bf16: bool = False, keep: bool = False):
