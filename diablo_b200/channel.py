@@ -24,6 +24,10 @@ LIB_PATH = os.path.join(_HERE, "libdiablo_gpu.so")
 DIABLO_OK, DIABLO_EINVAL, DIABLO_ERADIX, DIABLO_ECUDA, DIABLO_ENOTSUP, DIABLO_ENAN, DIABLO_ENOMEM, DIABLO_ETIMEOUT = (
     0, -1, -2, -3, -4, -5, -6, -7)
 NSTATS = 17
+# profiles of diablo_gpu_mean_stats: chan rows, then per scalar the SCAL rows
+MEAN_NAMES = ["ume", "vme", "wme", "urms", "vrms", "wrms", "uv", "uw", "wv", "dudy", "dwdy", "cp", "shear",
+              "omega_x", "omega_y", "omega_z"]
+SCAL_NAMES = ["thme", "dthdy", "thrms", "thv", "pe_diss"]
 # DIABLO_STAT_* rows of diablo_gpu_stats
 STAT_INDEX = {"ume": 0, "vme": 1, "wme": 2, "urms": 3, "vrms": 4, "wrms": 5, "uv": 6, "uw": 7, "wv": 8,
               "dudy": 9, "dwdy": 10, "cp": 11, "shear": 12, "thme": 13, "dthdy": 14, "thrms": 15, "thv": 16}
@@ -38,6 +42,7 @@ EXPORTS = [
     "diablo_gpu_get_stream", "diablo_gpu_set_profiling", "diablo_gpu_kernel_times",
     "diablo_gpu_rem_div_chan_noalloc", "diablo_gpu_autotune", "diablo_gpu_batch_create",
     "diablo_gpu_batch_step", "diablo_gpu_batch_destroy", "diablo_gpu_filter_chan", "diablo_gpu_download_nu_t",
+    "diablo_gpu_mean_stats",
     "diablo_gpu_sgs_samples", "diablo_gpu_set_sgs_mlp",
 ]
 KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
@@ -75,6 +80,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_download_phi.argtypes = [vp, dp]
     L.diablo_gpu_courant.argtypes = [vp, dp, dp]
     L.diablo_gpu_stats.argtypes = [vp, dp]
+    L.diablo_gpu_mean_stats.argtypes = [vp, dp, dp, dp]
     L.diablo_gpu_kernel_launches.argtypes = [vp]
     L.diablo_gpu_kernel_launches.restype = ctypes.c_longlong
     L.diablo_gpu_last_error.restype = ctypes.c_char_p
@@ -274,6 +280,23 @@ class Channel:
     def stats(self) -> np.ndarray:
         out = np.zeros((NSTATS, self.p.ny + 2))
         _check(self.L.diablo_gpu_stats(self._h, _dp(out)), "diablo_gpu_stats")
+        return out
+
+    def mean_stats(self) -> dict:
+        """Every mean.h5 / tke.h5 profile of SAVE_STATS_CHAN (NY+2 values
+        each): MEAN_NAMES, SCAL_NAMES with the scalar's two-digit number
+        (thme01, ...), and epsilon (rows 2..NY-1)."""
+        p = self.p
+        ny2 = p.ny + 2
+        chan = np.zeros((len(MEAN_NAMES), ny2))
+        scal = np.zeros((max(p.n_th, 1), len(SCAL_NAMES), ny2))
+        eps = np.zeros(ny2)
+        _check(self.L.diablo_gpu_mean_stats(self._h, _dp(chan), _dp(scal), _dp(eps)), "diablo_gpu_mean_stats")
+        out = {name: chan[k] for k, name in enumerate(MEAN_NAMES)}
+        for n in range(p.n_th):
+            for k, name in enumerate(SCAL_NAMES):
+                out[f"{name}{n + 1:02d}"] = scal[n, k]
+        out["epsilon"] = eps
         return out
 
     def fft_xz_to_fourier(self, v: np.ndarray, vv: np.ndarray, jmin: int, jmax: int) -> None:

@@ -56,6 +56,7 @@ struct Handle {
     double* pw = nullptr;         // 4 physical fields (POISSON_P_CHAN, statistics), allocated on first use
     double* d_me = nullptr;       // [4][nyp] mean profiles for the statistics
     double* d_sums = nullptr;     // [9][nyp] plane sums of the statistics
+    double* d_msums = nullptr;    // [4 + 3 N_TH][nyp] plane sums of the mean.h5 / tke.h5 profiles, then [nyp] 1/(GY(j+1)-GY(j-1))
     double* bcv = nullptr;        // [nf][nyp] BC-row values of the (0,0) mode
     double* d_tabs = nullptr;     // [nf][part_table_doubles] CN partition factors
     double* d_phitab = nullptr;   // [column][phi_table_doubles/column] phi partition factors
@@ -136,7 +137,7 @@ void free_handle(Handle* h) {
     if (!h) return;
     for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
-                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_tabs, h->d_phitab,
+                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_msums, h->d_tabs, h->d_phitab,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
                     h->twz_f, h->nut, h->lu, h->la, h->lb, h->d_delta, h->ls, h->lr, h->lx, h->d_dyn,
                     h->mlp_x, h->mlp_t, h->mlp_s};
@@ -1204,6 +1205,121 @@ int diablo_gpu_stats(void* handle, double* profiles) {
     if (d.nth > 0) {
         O(DIABLO_STAT_THME, 0) = thme[0];
         O(DIABLO_STAT_THME, nyp - 1) = thme[nyp - 1];
+    }
+    return DIABLO_OK;
+}
+
+// The remaining profiles of SAVE_STATS_CHAN's mean.h5 and tke.h5
+// (save_stats.f:270-347, 452-536, 937-1135): the base statistics above,
+// then each Fourier field of k_stats_spec goes to physical space on its own
+// and k_plane_terms adds its plane sums.  Physical U1..U3 stay in pw[0..2]
+// from the base statistics; pw[3] takes one field at a time.
+int diablo_gpu_mean_stats(void* handle, double* chan, double* scal, double* epsilon) {
+    Handle* h = (Handle*)handle;
+    if (!h || !chan || (h->d.nth > 0 && !scal)) return fail(DIABLO_EINVAL, "null pointer argument");
+    const Dims& d = h->d;
+    const size_t nyp = (size_t)d.nyp, pf = nyp * d.nz * d.nx;
+    std::vector<double> base((size_t)DIABLO_NSTATS * nyp);
+    int rc = diablo_gpu_stats(handle, base.data());
+    if (rc) return rc;
+    const int nsum = 4 + 3 * d.nth;
+    if (!h->d_msums) {
+        cudaError_t e = cudaMalloc((void**)&h->d_msums, sizeof(double) * (nsum + 1) * nyp);
+        if (e != cudaSuccess) {
+            h->d_msums = nullptr;
+            return fail(DIABLO_ENOMEM, std::string("statistics sums: ") + cudaGetErrorString(e));
+        }
+        std::vector<double> rg(nyp, 0.0);
+        for (int j = 1; j <= d.ny; ++j) rg[j] = 1.0 / (h->gy[j + 1] - h->gy[j - 1]);
+        CK(cudaMemcpy(h->d_msums + (size_t)nsum * nyp, rg.data(), sizeof(double) * nyp, cudaMemcpyHostToDevice));
+    }
+    ProfScope ps(h, DIABLO_KERNEL_OTHER);
+    double* acc = h->d_msums;
+    const double* rg = h->d_msums + (size_t)nsum * nyp;
+    double *U1 = h->pw, *U2 = h->pw + pf, *U3 = h->pw + 2 * pf, *F = h->pw + 3 * pf;
+    const double* ume = h->d_me;
+    const double* vme = h->d_me + nyp;
+    const double* wme = h->d_me + 2 * nyp;
+    double* thm = h->d_me + 3 * nyp;
+    // Fourier field `kind` (of CU, or of scalar cs) -> F on planes 1..NY
+    auto field = [&](int kind, const double2* cs) -> cudaError_t {
+        cudaError_t e = launch_stats_spec(d, kind, h->cu, cs, h->api_s, h->d_kx, h->d_kz, h->d_dyf, h->d_gyf, h->st);
+        if (e == cudaSuccess)
+            e = launch_zinv<double>(d, h->api_s, h->s_field, h->xb, h->x_field, 1, 1, d.ny, h->pz, h->twz_d, h->st);
+        if (e == cudaSuccess) e = launch_xinv(d, h->xb, F, 1, d.ny, h->pm, h->twm_d, h->twn_d, h->st);
+        h->launches += 3;
+        return e;
+    };
+    auto term = [&](int mode, const double* f, const double* u, const double* m, const double* m2, int jlo, int jhi,
+                    int slot, int init) -> cudaError_t {
+        h->launches += 1;
+        return launch_plane_terms(d, mode, f, u, m, m2, h->d_dy, h->d_dyf, rg, jlo, jhi, acc + (size_t)slot * nyp,
+                                  init, h->st);
+    };
+    // rms vorticity, planes 1..NY
+    for (int c = 0; c < 3; ++c) {
+        CK(field(c, nullptr));
+        CK(term(0, F, nullptr, nullptr, nullptr, 1, d.ny, c, 1));
+    }
+    // pseudo-dissipation, planes 2..NY-1, in tkebudget_chan's order of terms
+    const int e0 = 2, e1 = d.ny - 1;
+    CK(field(3, nullptr)); CK(term(1, F, nullptr, nullptr, nullptr, e0, e1, 3, 1));     // du/dx
+    CK(field(4, nullptr)); CK(term(0, F, nullptr, nullptr, nullptr, e0, e1, 3, 0));     // dv/dx
+    CK(term(2, nullptr, U1, ume, nullptr, e0, e1, 3, 0));                               // du/dy
+    CK(field(5, nullptr)); CK(term(1, F, nullptr, nullptr, nullptr, e0, e1, 3, 0));     // dw/dx
+    CK(field(6, nullptr)); CK(term(1, F, nullptr, nullptr, nullptr, e0, e1, 3, 0));     // du/dz
+    CK(term(3, nullptr, U2, vme, nullptr, e0, e1, 3, 0));                               // dv/dy
+    CK(term(2, nullptr, U3, wme, nullptr, e0, e1, 3, 0));                               // dw/dy
+    CK(field(7, nullptr)); CK(term(0, F, nullptr, nullptr, nullptr, e0, e1, 3, 0));     // dv/dz
+    CK(field(8, nullptr)); CK(term(1, F, nullptr, nullptr, nullptr, e0, e1, 3, 0));     // dw/dz
+    // scalars: TH - THME, its flux with V, and |grad TH|^2
+    std::vector<double> thme((size_t)d.nth * nyp);
+    for (int n = 0; n < d.nth; ++n) {
+        const double2* cs = h->cu + (size_t)(3 + n) * h->s_field;
+        std::vector<double2> c00(nyp);
+        CK(cudaMemcpy2DAsync(c00.data(), sizeof(double2), cs, sizeof(double2) * h->s_plane, sizeof(double2), nyp,
+                             cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        for (size_t j = 0; j < nyp; ++j) thme[(size_t)n * nyp + j] = c00[j].x;
+        CK(cudaMemcpyAsync(thm, thme.data() + (size_t)n * nyp, sizeof(double) * nyp, cudaMemcpyHostToDevice, h->st));
+        CK(launch_zinv<double>(d, cs, h->s_field, h->xb, h->x_field, 1, 0, d.nyp, h->pz, h->twz_d, h->st));
+        CK(launch_xinv(d, h->xb, F, 0, d.nyp, h->pm, h->twm_d, h->twn_d, h->st));
+        h->launches += 2;
+        const int s0 = 4 + 3 * n;
+        CK(term(4, F, nullptr, thm, nullptr, 1, d.ny, s0, 1));
+        CK(term(5, F, U2, thm, vme, 1, d.ny, s0 + 1, 1));
+        for (int k = 0; k < 3; ++k) {
+            CK(field(9 + k, cs));
+            CK(term(0, F, nullptr, nullptr, nullptr, 1, d.ny, s0 + 2, k == 0));
+        }
+    }
+    std::vector<double> sums((size_t)nsum * nyp);
+    CK(cudaMemcpyAsync(sums.data(), acc, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    auto S = [&](int k, int j) { return sums[(size_t)k * nyp + j]; };
+    for (size_t q = 0; q < (size_t)DIABLO_NMEAN * nyp; ++q) chan[q] = 0.0;
+    for (int s = 0; s < DIABLO_STAT_THME; ++s)
+        for (size_t j = 0; j < nyp; ++j) chan[(size_t)s * nyp + j] = base[(size_t)s * nyp + j];
+    const double nxz = (double)d.nx * (double)d.nz;       // DBLE(NX)*DBLE(NZ)
+    const double nxzi = (double)(d.nx * d.nz);            // DBLE(NX*NZ)
+    const double nn = (double)((float)d.nz * (float)d.nx);  // FLOAT(NZ)*FLOAT(NX)
+    for (int c = 0; c < 3; ++c)
+        for (int j = 1; j <= d.ny; ++j) chan[(size_t)(DIABLO_MEAN_OMEGA_X + c) * nyp + j] = std::sqrt(S(c, j) / nxz);
+    if (epsilon) {
+        for (size_t j = 0; j < nyp; ++j) epsilon[j] = 0.0;
+        for (int j = e0; j <= e1; ++j) epsilon[j] = h->p.nu * S(3, j) / nxzi;
+    }
+    for (int n = 0; n < d.nth; ++n) {
+        double* o = scal + (size_t)n * DIABLO_NSCAL * nyp;
+        const double* tm = thme.data() + (size_t)n * nyp;
+        for (size_t q = 0; q < (size_t)DIABLO_NSCAL * nyp; ++q) o[q] = 0.0;
+        for (size_t j = 0; j < nyp; ++j) o[DIABLO_SCAL_THME * nyp + j] = tm[j];
+        for (int j = 1; j <= d.ny; ++j) {
+            o[DIABLO_SCAL_DTHDY * nyp + j] = (tm[j] - tm[j - 1]) / (h->gyf[j] - h->gyf[j - 1]);
+            o[DIABLO_SCAL_THRMS * nyp + j] = std::sqrt(S(4 + 3 * n, j) / nn);
+            o[DIABLO_SCAL_THV * nyp + j] = S(5 + 3 * n, j) / nn;
+            o[DIABLO_SCAL_PE_DISS * nyp + j] = S(6 + 3 * n, j) / nxzi;
+        }
     }
     return DIABLO_OK;
 }

@@ -85,6 +85,15 @@ cudaError_t launch_poisson_column(const PoissonArgs& a, cudaStream_t st);
 cudaError_t launch_stats_planes(const Dims& d, const double* u1, const double* u2, const double* u3,
                                 const double* th, const double* me, const double* dy, const double* dyf, double* out,
                                 cudaStream_t st);
+// One Fourier field of the vorticity / dissipation / scalar-gradient
+// statistics on rows 1..NY (kinds 0..11, see k_stats_spec).
+cudaError_t launch_stats_spec(const Dims& d, int kind, const double2* cu, const double2* cs, double2* out,
+                              const double* kx, const double* kz, const double* dyf, const double* gyf,
+                              cudaStream_t st);
+// acc[j] (+)= plane sum of one statistics term (modes 0..5), planes jlo..jhi.
+cudaError_t launch_plane_terms(const Dims& d, int mode, const double* f, const double* u, const double* m,
+                               const double* m2, const double* dy, const double* dyf, const double* rg, int jlo,
+                               int jhi, double* acc, int init, cudaStream_t st);
 // filter_chan (filter.f:1-98) on one scalar field of the S layout; fnx, fnz
 // are NX and NZ as the reference's FLOAT() gives them.
 cudaError_t launch_filter_chan(const Dims& d, double2* cth, const double* kx, const double* kz, double lx,

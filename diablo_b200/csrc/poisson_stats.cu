@@ -190,6 +190,119 @@ __global__ void __launch_bounds__(256) k_stats_planes(Dims d, const double* __re
     if (threadIdx.x < 9) out[threadIdx.x * nyp + j] = red[threadIdx.x][0];
 }
 
+// One Fourier field of the remaining SAVE_STATS_CHAN profiles on rows
+// J = 1..NY (zero on rows 0 and NY+1), from CU (after APPLY_BC_VEL) or from
+// one scalar CS:
+//  kind 0: omega_x = (CU3(j+1)-CU3(j-1))/(2 DYF(j)) - ikz (CU2(j+1)+CU2(j))/2
+//       1: omega_y = ikz CU1 - ikx CU3                     (save_stats.f:270-322)
+//       2: omega_z = ikx (CU2(j+1)+CU2(j))/2 - (CU1(j+1)-CU1(j-1))/(2 DYF(j))
+//    3..5: ikx CU1, ikx CU2, ikx CU3   6..8: ikz CU1, ikz CU2, ikz CU3
+//          (the gradients of tkebudget_chan, save_stats.f:957-1135)
+//   9..11: ikx CS, (CS(j+1)-CS(j-1))/(GYF(j+1)-GYF(j-1)), ikz CS
+//          (the scalar gradient of pe_diss, save_stats.f:465-474)
+__global__ void k_stats_spec(Dims d, int kind, const double2* __restrict__ cu, const double2* __restrict__ cs,
+                             double2* __restrict__ out, const double* __restrict__ kx, const double* __restrict__ kz,
+                             const double* __restrict__ dyf, const double* __restrict__ gyf) {
+    const size_t ps = d.splane();
+    const size_t fs = ps * d.nyp;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < fs; e += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(e / ps);
+        const size_t col = e % ps;
+        const int m = (int)(col / d.ldx), i = (int)(col % d.ldx);
+        double2 v = make_double2(0.0, 0.0);
+        if (j >= 1 && j <= d.ny && m < d.nkzt && i < d.nkxp) {
+            const double2* u1 = cu + col;
+            const double2* u2 = cu + fs + col;
+            const double2* u3 = cu + 2 * fs + col;
+            const double KX = kx[i], KZ = kz[m];
+            auto ddy = [&](const double2* f) {
+                const double2 a = f[(j + 1) * ps], b = f[(j - 1) * ps];
+                return make_double2((a.x - b.x) / (2. * dyf[j]), (a.y - b.y) / (2. * dyf[j]));
+            };
+            auto avg2 = [&]() {
+                const double2 a = u2[(j + 1) * ps], b = u2[j * ps];
+                return make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
+            };
+            switch (kind) {
+                case 0: { const double2 a = ddy(u3), b = ikd(KZ, avg2());
+                          v = make_double2(a.x - b.x, a.y - b.y); } break;
+                case 1: { const double2 a = ikd(KZ, u1[j * ps]), b = ikd(KX, u3[j * ps]);
+                          v = make_double2(a.x - b.x, a.y - b.y); } break;
+                case 2: { const double2 a = ikd(KX, avg2()), b = ddy(u1);
+                          v = make_double2(a.x - b.x, a.y - b.y); } break;
+                case 3: v = ikd(KX, u1[j * ps]); break;
+                case 4: v = ikd(KX, u2[j * ps]); break;
+                case 5: v = ikd(KX, u3[j * ps]); break;
+                case 6: v = ikd(KZ, u1[j * ps]); break;
+                case 7: v = ikd(KZ, u2[j * ps]); break;
+                case 8: v = ikd(KZ, u3[j * ps]); break;
+                case 9: v = ikd(KX, cs[col + j * ps]); break;
+                case 10: { const double2 a = cs[col + (j + 1) * ps], b = cs[col + (j - 1) * ps];
+                           const double g = gyf[j + 1] - gyf[j - 1];
+                           v = make_double2((a.x - b.x) / g, (a.y - b.y) / g); } break;
+                default: v = ikd(KZ, cs[col + j * ps]); break;
+            }
+        }
+        out[e] = v;
+    }
+}
+
+// Plane sums of one term of the statistics over physical planes j = jlo..jhi
+// (one block per plane, FP64): acc[j] = (init ? 0 : acc[j]) + sum_{x,z} term.
+//  mode 0: f(j)^2
+//       1: (DYF(j-1) f(j)^2 + DYF(j) f(j-1)^2) / (2 DY(j))   (GYF values at GY)
+//       2: (((u(j)-m(j)) - (u(j-1)-m(j-1))) / DY(j))^2      (du/dy, dw/dy)
+//       3: (((u(j+1)-m(j)) - (u(j-1)-m(j-1))) * rg(j))^2    (dv/dy, rg = 1/(GY(j+1)-GY(j-1)))
+//       4: |f(j)-m(j)|^2                                    (thrms)
+//       5: (f(j)-m(j)) ((u(j)+u(j+1))/2 - (m2(j)+m2(j+1))/2) (thv)
+__global__ void __launch_bounds__(256) k_plane_terms(Dims d, int mode, const double* __restrict__ f,
+                                                     const double* __restrict__ u, const double* __restrict__ m,
+                                                     const double* __restrict__ m2, const double* __restrict__ dy,
+                                                     const double* __restrict__ dyf, const double* __restrict__ rg,
+                                                     int jlo, double* __restrict__ acc, int init) {
+    __shared__ double red[256];
+    const int j = jlo + blockIdx.x;
+    const size_t plane = (size_t)d.nz * d.nx;
+    const size_t c0 = (size_t)j * plane;
+    double s = 0.0;
+    for (size_t e = threadIdx.x; e < plane; e += 256) {
+        const size_t c = c0 + e;
+        double t;
+        switch (mode) {
+            case 0: t = f[c] * f[c]; break;
+            case 1: { const double a = f[c], b = f[c - plane];
+                      t = (dyf[j - 1] * a * a + dyf[j] * b * b) / (2.0 * dy[j]); } break;
+            case 2: { const double g = ((u[c] - m[j]) - (u[c - plane] - m[j - 1])) / dy[j]; t = g * g; } break;
+            case 3: { const double g = ((u[c + plane] - m[j]) - (u[c - plane] - m[j - 1])) * rg[j]; t = g * g; } break;
+            case 4: { const double a = fabs(f[c] - m[j]); t = a * a; } break;
+            default: t = (f[c] - m[j]) * (0.5 * (u[c] + u[c + plane]) - 0.5 * (m2[j] + m2[j + 1])); break;
+        }
+        s += t;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) acc[j] = (init ? 0.0 : acc[j]) + red[0];
+}
+
+cudaError_t launch_stats_spec(const Dims& d, int kind, const double2* cu, const double2* cs, double2* out,
+                              const double* kx, const double* kz, const double* dyf, const double* gyf,
+                              cudaStream_t st) {
+    k_stats_spec<<<1184, 256, 0, st>>>(d, kind, cu, cs, out, kx, kz, dyf, gyf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plane_terms(const Dims& d, int mode, const double* f, const double* u, const double* m,
+                               const double* m2, const double* dy, const double* dyf, const double* rg, int jlo,
+                               int jhi, double* acc, int init, cudaStream_t st) {
+    if (jhi < jlo) return cudaSuccess;
+    k_plane_terms<<<jhi - jlo + 1, 256, 0, st>>>(d, mode, f, u, m, m2, dy, dyf, rg, jlo, acc, init);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_grad_field(const Dims& d, int kind, const double2* cu, double2* out, const double* kx,
                               const double* kz, const double* dyf, cudaStream_t st) {
     k_grad_field<<<1184, 256, 0, st>>>(d, kind, cu, out, kx, kz, dyf);

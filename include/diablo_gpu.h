@@ -170,6 +170,36 @@ int diablo_gpu_courant(void* handle, double* delta_t, double* h_bar);
 #define DIABLO_NSTATS      17
 int diablo_gpu_stats(void* handle, double* profiles);
 
+/* Every profile SAVE_STATS_CHAN writes to mean.h5 and tke.h5
+ * (for/save_stats.f:104-536, 937-1135), in FP64, for the current state
+ * (after APPLY_BC_VEL, as the reference does).
+ *  chan:    DIABLO_NMEAN*(NY+2) doubles: profiles 0..12 as DIABLO_STAT_UME..
+ *           DIABLO_STAT_SHEAR, then the rms vorticity components omega_x,
+ *           omega_y, omega_z (save_stats.f:270-347), rows 1..NY.
+ *  scal:    N_TH*DIABLO_NSCAL*(NY+2) doubles (may be null when N_TH = 0):
+ *           per scalar n, thme, dthdy, thrms, thv and pe_diss (the mean
+ *           square scalar gradient, save_stats.f:465-536) at
+ *           [(n*DIABLO_NSCAL + s)*(NY+2) + j].
+ *  epsilon: NY+2 doubles or null: the pseudo-dissipation of tkebudget_chan
+ *           (save_stats.f:937-1135), NU <du_i/dx_j du_i/dx_j>, on rows
+ *           2..NY-1.  Rows 1 and NY are 0: there the reference's value
+ *           depends on work-array contents left by earlier calls.
+ * The reference's mean.h5 stores omega_y in the omega_z dataset
+ * (save_stats.f:421-423); this entry returns the true omega_z and leaves
+ * that choice to the writer.  Replaces the statistics part of
+ * SAVE_STATS_CHAN; its HDF5 writes stay on the host. */
+#define DIABLO_MEAN_OMEGA_X 13
+#define DIABLO_MEAN_OMEGA_Y 14
+#define DIABLO_MEAN_OMEGA_Z 15
+#define DIABLO_NMEAN        16
+#define DIABLO_SCAL_THME     0
+#define DIABLO_SCAL_DTHDY    1
+#define DIABLO_SCAL_THRMS    2
+#define DIABLO_SCAL_THV      3
+#define DIABLO_SCAL_PE_DISS  4
+#define DIABLO_NSCAL         5
+int diablo_gpu_mean_stats(void* handle, double* chan, double* scal, double* epsilon);
+
 /* The CUDA stream (a cudaStream_t) all work of the handle is queued on, as
  * an opaque pointer: callers may record timing events on it. */
 int diablo_gpu_get_stream(void* handle, void** stream);

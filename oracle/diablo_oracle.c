@@ -1970,6 +1970,141 @@ void orc_stats(orc_state* s, double* out) {
 }
 
 /* ------------------------------------------------------------------------ */
+/* The remaining profiles of SAVE_STATS_CHAN's mean.h5 and tke.h5, after      */
+/* orc_stats (which applies APPLY_BC_VEL):                                    */
+/*  - rms vorticity (save_stats.f:270-347): each component formed from CR =   */
+/*    CU on rows 1..NY, transformed, sqrt(sum S1^2 / (DBLE(NX) DBLE(NZ)));    */
+/*  - per scalar (save_stats.f:452-536): thme, dthdy, thrms, thv and pe_diss, */
+/*    the plane sum of |grad TH|^2 over DBLE(NX*NZ);                          */
+/*  - epsilon of tkebudget_chan (save_stats.f:937-1135) on rows 2..NY-1, its  */
+/*    nine terms in the reference's order.  Rows 1 and NY stay 0: there the   */
+/*    reference reads rows of S1 / CS1 that earlier code left behind.         */
+/* ------------------------------------------------------------------------ */
+static void stats_field(orc_state* s, int kind, const double* C, double* out) {
+    const int NY = s->NY, NXP = s->NXP, TNKZ = s->TNKZ;
+    const cplx CI = I;
+    memset(out, 0, sizeof(double) * s->nreal);
+    for (int j = 1; j <= NY; ++j)
+        for (int k = 0; k <= TNKZ; ++k)
+            for (int i = 0; i <= NXP - 1; ++i) {
+                const cplx ikx = CI * s->KX[i], ikz = CI * s->KZ[k];
+                const double d2 = 2.0 * s->DYF[j];
+                cplx v;
+                switch (kind) {
+                    case 0: v = (CX(s->U3, i, k, j + 1) - CX(s->U3, i, k, j - 1)) / d2 -
+                                ikz * 0.5 * (CX(s->U2, i, k, j + 1) + CX(s->U2, i, k, j)); break;
+                    case 1: v = ikz * CX(s->U1, i, k, j) - ikx * CX(s->U3, i, k, j); break;
+                    case 2: v = ikx * 0.5 * (CX(s->U2, i, k, j + 1) + CX(s->U2, i, k, j)) -
+                                (CX(s->U1, i, k, j + 1) - CX(s->U1, i, k, j - 1)) / d2; break;
+                    case 3: v = ikx * CX(s->U1, i, k, j); break;
+                    case 4: v = ikx * CX(s->U2, i, k, j); break;
+                    case 5: v = ikx * CX(s->U3, i, k, j); break;
+                    case 6: v = ikz * CX(s->U1, i, k, j); break;
+                    case 7: v = ikz * CX(s->U2, i, k, j); break;
+                    case 8: v = ikz * CX(s->U3, i, k, j); break;
+                    case 9: v = ikx * CX(C, i, k, j); break;
+                    case 10: v = (CX(C, i, k, j + 1) - CX(C, i, k, j - 1)) / (s->GYF[j + 1] - s->GYF[j - 1]); break;
+                    default: v = ikz * CX(C, i, k, j); break;
+                }
+                CX(out, i, k, j) = v;
+            }
+    orc_fft_xz_to_physical(s, out, out, 0, NY + 1);
+}
+
+void orc_mean_stats(orc_state* s, double* chan, double* scal, double* eps) {
+    const int NY = s->NY, NX = s->NX, NZ = s->NZ, NZP = s->NZP, NXM = s->NXM;
+    const size_t ny2 = (size_t)NY + 2;
+    double* base = (double*)malloc(sizeof(double) * DIABLO_NSTATS * ny2);
+    orc_stats(s, base);
+    memset(chan, 0, sizeof(double) * DIABLO_NMEAN * ny2);
+    memcpy(chan, base, sizeof(double) * DIABLO_STAT_THME * ny2);
+    const double* ume = base + DIABLO_STAT_UME * ny2;
+    const double* vme = base + DIABLO_STAT_VME * ny2;
+    const double* wme = base + DIABLO_STAT_WME * ny2;
+    double* S1 = (double*)malloc(sizeof(double) * s->nreal);
+    for (int c = 0; c < 3; ++c) {
+        stats_field(s, c, NULL, S1);
+        for (int j = 1; j <= NY; ++j) {
+            double a = 0.0;
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i) a += pow(PH(S1, i, k, j), 2.0);
+            chan[(DIABLO_MEAN_OMEGA_X + c) * ny2 + j] = sqrt(a / ((double)NX * (double)NZ));
+        }
+    }
+    double* u[3];
+    for (int c = 0; c < 3; ++c) {
+        u[c] = (double*)malloc(sizeof(double) * s->nreal);
+        memcpy(u[c], c == 0 ? s->U1 : c == 1 ? s->U2 : s->U3, sizeof(double) * s->nreal);
+        orc_fft_xz_to_physical(s, u[c], u[c], 0, NY + 1);
+    }
+    double *U1 = u[0], *U2 = u[1], *U3 = u[2];
+    if (eps) {
+        memset(eps, 0, sizeof(double) * ny2);
+        double* e = (double*)calloc(ny2, sizeof(double));
+        /* mode 0: S1(j)^2, 1: GYF values interpolated to GY */
+        #define EPS_ADD(mode)                                                                          \
+            for (int j = 2; j <= NY - 1; ++j)                                                          \
+                for (int k = 0; k <= NZP - 1; ++k)                                                     \
+                    for (int i = 0; i <= NXM; ++i)                                                     \
+                        e[j] += (mode) ? (s->DYF[j - 1] * pow(PH(S1, i, k, j), 2.0) +                  \
+                                          s->DYF[j] * pow(PH(S1, i, k, j - 1), 2.0)) / (2.0 * s->DY[j]) \
+                                       : pow(PH(S1, i, k, j), 2.0);
+        stats_field(s, 3, NULL, S1); EPS_ADD(1)                         /* du/dx */
+        stats_field(s, 4, NULL, S1); EPS_ADD(0)                         /* dv/dx */
+        for (int j = 2; j <= NY - 1; ++j)                               /* du/dy */
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i)
+                    e[j] += pow(((PH(U1, i, k, j) - ume[j]) - (PH(U1, i, k, j - 1) - ume[j - 1])) / s->DY[j], 2.0);
+        stats_field(s, 5, NULL, S1); EPS_ADD(1)                         /* dw/dx */
+        stats_field(s, 6, NULL, S1); EPS_ADD(1)                         /* du/dz */
+        for (int j = 2; j <= NY - 1; ++j)                               /* dv/dy */
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i)
+                    e[j] += pow(((PH(U2, i, k, j + 1) - vme[j]) - (PH(U2, i, k, j - 1) - vme[j - 1])) /
+                                    (s->GY[j + 1] - s->GY[j - 1]), 2.0);
+        for (int j = 2; j <= NY - 1; ++j)                               /* dw/dy */
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i)
+                    e[j] += pow(((PH(U3, i, k, j) - wme[j]) - (PH(U3, i, k, j - 1) - wme[j - 1])) / s->DY[j], 2.0);
+        stats_field(s, 7, NULL, S1); EPS_ADD(0)                         /* dv/dz */
+        stats_field(s, 8, NULL, S1); EPS_ADD(1)                         /* dw/dz */
+        #undef EPS_ADD
+        for (int j = 2; j <= NY - 1; ++j) eps[j] = s->p.nu * e[j] / (double)(NX * NZ);
+        free(e);
+    }
+    const double nn = (double)((float)NZ * (float)NX);
+    double* th = (double*)malloc(sizeof(double) * s->nreal);
+    double* R[3];
+    for (int c = 0; c < 3; ++c) R[c] = (double*)malloc(sizeof(double) * s->nreal);
+    for (int n = 0; n < s->NTH; ++n) {
+        const double* C = s->CTH + (size_t)n * s->nreal;
+        double* o = scal + (size_t)n * DIABLO_NSCAL * ny2;
+        memset(o, 0, sizeof(double) * DIABLO_NSCAL * ny2);
+        double* thme = o + DIABLO_SCAL_THME * ny2;
+        for (size_t j = 0; j < ny2; ++j) thme[j] = creal(CX(C, 0, 0, j));
+        for (int c = 0; c < 3; ++c) stats_field(s, 9 + c, C, R[c]);
+        memcpy(th, C, sizeof(double) * s->nreal);
+        orc_fft_xz_to_physical(s, th, th, 0, NY + 1);
+        for (int j = 1; j <= NY; ++j) {
+            double a = 0, b = 0, g = 0;
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i) {
+                    a += pow(fabs(PH(th, i, k, j) - thme[j]), 2.);
+                    b += (PH(th, i, k, j) - thme[j]) *
+                         (0.5 * (PH(U2, i, k, j) + PH(U2, i, k, j + 1)) - 0.5 * (vme[j] + vme[j + 1]));
+                    g += pow(PH(R[0], i, k, j), 2.0) + pow(PH(R[1], i, k, j), 2.0) + pow(PH(R[2], i, k, j), 2.0);
+                }
+            o[DIABLO_SCAL_THRMS * ny2 + j] = sqrt(a / nn);
+            o[DIABLO_SCAL_THV * ny2 + j] = b / nn;
+            o[DIABLO_SCAL_DTHDY * ny2 + j] = (thme[j] - thme[j - 1]) / (s->GYF[j] - s->GYF[j - 1]);
+            o[DIABLO_SCAL_PE_DISS * ny2 + j] = g / (double)(NX * NZ);
+        }
+    }
+    for (int c = 0; c < 3; ++c) { free(R[c]); free(u[c]); }
+    free(th); free(S1); free(base);
+}
+
+/* ------------------------------------------------------------------------ */
 /* filter_chan(n) (filter.f:1-98) on scalar n (1..N_TH): a sharpened raised   */
 /* cosine in the horizontal on every mode and rows J = 0..NY, then, for       */
 /* I = 1..NKX and K = 1..TNKZ, the vertical compact filter with alpha = 0,    */

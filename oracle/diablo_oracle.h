@@ -75,6 +75,9 @@ void orc_step(orc_state* s);
 void orc_filter_chan(orc_state* s, int n);
 /* Statistics of SAVE_STATS_CHAN (DIABLO_STAT_* profiles, NY+2 each). */
 void orc_stats(orc_state* s, double* profiles);
+/* Every mean.h5 / tke.h5 profile: chan DIABLO_NMEAN*(NY+2), scal
+ * N_TH*DIABLO_NSCAL*(NY+2), eps NY+2 (or NULL), as diablo_gpu_mean_stats. */
+void orc_mean_stats(orc_state* s, double* chan, double* scal, double* eps);
 /* Parameters of the learned closure (LES_MODEL_TYPE 4), in the layout of the
  * GPU library's diablo_mlp_set_params; NULL removes it. */
 void orc_set_mlp(orc_state* s, const float* params);

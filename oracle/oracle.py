@@ -59,6 +59,7 @@ def lib() -> ctypes.CDLL:
                      "orc_apply_bc_scalar", "orc_step"):
             getattr(L, name).argtypes = [vp]
         L.orc_stats.argtypes = [vp, dp]
+        L.orc_mean_stats.argtypes = [vp, dp, dp, dp]
         L.orc_set_mlp.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
         L.orc_cdft.restype = ip
         L.orc_cdft.argtypes = [ip, dp, ip]
@@ -203,6 +204,22 @@ class Oracle:
     def stats(self) -> np.ndarray:
         out = np.zeros((17, self.p.ny + 2))
         lib().orc_stats(self._h, _dptr(out))
+        return out
+
+    def mean_stats(self) -> dict:
+        """Every mean.h5 / tke.h5 profile, keyed as Channel.mean_stats."""
+        from diablo_b200.channel import MEAN_NAMES, SCAL_NAMES
+        p = self.p
+        ny2 = p.ny + 2
+        chan = np.zeros((len(MEAN_NAMES), ny2))
+        scal = np.zeros((max(p.n_th, 1), len(SCAL_NAMES), ny2))
+        eps = np.zeros(ny2)
+        lib().orc_mean_stats(self._h, _dptr(chan), _dptr(scal), _dptr(eps))
+        out = {name: chan[k] for k, name in enumerate(MEAN_NAMES)}
+        for n in range(p.n_th):
+            for k, name in enumerate(SCAL_NAMES):
+                out[f"{name}{n + 1:02d}"] = scal[n, k]
+        out["epsilon"] = eps
         return out
 
     # --- initial condition (CREATE_TH_CHAN then CREATE_FLOW_CHAN) ------------

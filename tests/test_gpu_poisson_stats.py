@@ -106,3 +106,42 @@ def test_stats_match_oracle(case):
         s = c.download()
         for f in range(3):
             assert relerr(layout.dealiased(p, s["cu"][f]), layout.dealiased(p, o.cu[f])) < 1e-14
+
+
+def kh2_pair(nx, ny, nz, steps):
+    """A shear layer with a second, passive scalar (Pr 2)."""
+    p = P.kelvin_helmholtz(nx, ny, nz)
+    p.n_th = 2
+    p.pr[1], p.ri[1] = 2.0, 0.0
+    p.th_bc_ymin[1] = p.th_bc_ymax[1] = 1
+    g = G.channel_grid(G.create_grid(2, ny, 20.0, 1.5))
+    u, th1 = ics.shear_layer(p, g, seed=5, amp=0.1)
+    th = np.stack([th1[0], 0.5 * th1[0] ** 2 + 0.1 * u[0]])
+    o = Oracle(p, g, 0.02)
+    o.init_from_physical(u, th)
+    o.step(steps)
+    return p, g, o
+
+
+@pytest.mark.parametrize("case", ["kh2", "channel"])
+def test_mean_stats_match_oracle(case):
+    """Every mean.h5 / tke.h5 profile (vorticity, pseudo-dissipation, the
+    per-scalar profiles) against the oracle's restatement of save_stats.f."""
+    if case == "kh2":
+        p, g, o = kh2_pair(48, 33, 36, steps=3)
+        dt = 0.02
+    else:
+        p, g, o = channel_pair(48, 33, 40, steps=2)
+        dt = 1e-3
+    with upload(p, g, o, dt) as c:
+        got = c.mean_stats()
+        ref = o.mean_stats()
+        assert sorted(got) == sorted(ref)
+        for k, r in ref.items():
+            a = got[k]
+            scale = max(np.abs(r).max(), 1e-300)
+            err = float(np.abs(a - r).max() / scale)
+            assert err < 1e-11, (k, err)
+        assert np.abs(ref["omega_z"]).max() > 0 and np.abs(ref["epsilon"]).max() > 0
+        if p.n_th > 1:
+            assert np.abs(ref["pe_diss02"]).max() > 0 and not np.allclose(ref["thrms02"], ref["thrms01"])

@@ -1,0 +1,135 @@
+"""The mean.h5 / tke.h5 / stats.h5 profiles of SAVE_STATS_CHAN
+(for/save_stats.f) on the CPU oracle against closed forms, and the file
+layout of WriteStatH5 / WriteHDF5_real (for/hdf5.f:1345-1622)."""
+import numpy as np
+import pytest
+
+from diablo_b200 import grid as G, params as P, statsfile
+from diablo_b200.channel import MEAN_NAMES, SCAL_NAMES
+from oracle.oracle import Oracle
+
+
+def modes_case(A=0.7, B=0.3, C=0.4):
+    """u1 = A cos(3 kz0 z), u3 = C cos(2 kx0 x), th = B cos(2 kx0 x), uniform
+    in y: closed forms for every vorticity, dissipation and scalar profile."""
+    p = P.kelvin_helmholtz(24, 17, 20)
+    g = G.channel_grid(G.create_grid(2, p.ny, 20.0, 1.5))
+    nx, ny, nz = p.nx, p.ny, p.nz
+    x = np.arange(nx) * p.lx / nx
+    z = np.arange(nz) * p.lz / nz
+    kx, kz = 2 * np.pi / p.lx * 2, 2 * np.pi / p.lz * 3
+    u = np.zeros((3, ny + 2, nz + 2, nx + 2))
+    th = np.zeros((1, ny + 2, nz + 2, nx + 2))
+    u[0, :, :nz, :nx] = A * np.cos(kz * z)[None, :, None]
+    u[2, :, :nz, :nx] = C * np.cos(kx * x)[None, None, :]
+    th[0, :, :nz, :nx] = B * np.cos(kx * x)[None, None, :]
+    o = Oracle(p, g, 0.01)
+    o.init_from_physical(u, th)
+    return p, g, o, kx, kz
+
+
+def test_oracle_mean_profiles_closed_forms():
+    A, B, C = 0.7, 0.3, 0.4
+    p, g, o, kx, kz = modes_case(A, B, C)
+    m = o.mean_stats()
+    ny = p.ny
+    J = slice(2, ny)                                 # rows whose y-neighbours are interior
+    # omega_y = du/dz - dw/dx, two orthogonal modes
+    assert np.allclose(m["omega_y"][1 : ny + 1], np.sqrt((A * kz) ** 2 + (C * kx) ** 2) / np.sqrt(2), rtol=1e-13)
+    assert np.abs(m["omega_x"][1 : ny + 1]).max() < 1e-14
+    assert np.abs(m["omega_z"][J]).max() < 1e-14
+    # epsilon = NU <du/dz^2 + dw/dx^2>, both GYF quantities interpolated to GY
+    w = (g.dyf[1 : ny - 1] + g.dyf[2:ny]) / (2 * g.dy[2:ny])
+    eps = p.nu * ((A * kz) ** 2 + (C * kx) ** 2) / 2 * w
+    assert np.allclose(m["epsilon"][J], eps, rtol=1e-13)
+    assert m["epsilon"][1] == 0.0 and m["epsilon"][ny] == 0.0
+    assert np.allclose(m["pe_diss01"][1 : ny + 1], (B * kx) ** 2 / 2, rtol=1e-13)
+    assert np.allclose(m["thrms01"][1 : ny + 1], B / np.sqrt(2), rtol=1e-13)
+    assert np.abs(m["thv01"]).max() < 1e-15
+    # the 13 profiles shared with the plane statistics are orc_stats'
+    base = o.stats()
+    for k in range(13):
+        assert np.array_equal(m[MEAN_NAMES[k]], base[k])
+
+
+def test_statfile_layout(tmp_path):
+    path = str(tmp_path / "mean.h5")
+    f = statsfile.StatFile(path)
+    assert f.write_real("time", 0.5) == 1
+    assert f.write_stat("ume", np.arange(5.0), 0.5) == 1
+    assert f.write_stat("ume", np.arange(5.0) + 1, 0.75) == 2
+    f2 = statsfile.StatFile(path)                    # reopened: SAMPLES continues
+    assert f2.samples("ume") == 2 and f2.samples("time") == 1 and f2.samples("vme") == 0
+    f2.write_real("time", 0.75)
+    raw = np.load(path)                              # plain numpy reads the datasets
+    assert np.array_equal(raw["ume/0002"], np.arange(5.0) + 1) and float(raw["ume/0002@Time"]) == 0.75
+    r = statsfile.read(path)
+    assert r["ume"]["SAMPLES"] == 2 and r["ume"]["data"].shape == (2, 5)
+    assert list(r["ume"]["Time"]) == [0.5, 0.75]
+    assert r["time"]["Time"] is None and list(r["time"]["data"][:, 0]) == [0.5, 0.75]
+
+
+class _OracleRun:
+    """What StatsWriter reads from a Channel, on the oracle."""
+
+    def __init__(self, o, t):
+        self.o, self.p, self.grid, self.time = o, o.p, o.grid, t
+
+    def mean_stats(self):
+        return self.o.mean_stats()
+
+
+@pytest.mark.parametrize("quirk", [True, False])
+def test_stats_writer_files(tmp_path, quirk):
+    p, g, o, _, _ = modes_case()
+    w = statsfile.StatsWriter(str(tmp_path), omega_z_quirk=quirk)
+    m1 = w.save(_OracleRun(o, 0.0))
+    o.step(2)
+    m2 = w.save(_OracleRun(o, 0.02))
+    w.save(_OracleRun(o, 0.02), final=True)
+    mean = statsfile.read(str(tmp_path / "mean.h5"))
+    names = ["time", "gyf"] + MEAN_NAMES + [f"{s}01" for s in SCAL_NAMES]
+    assert sorted(mean) == sorted(names)
+    assert all(mean[k]["SAMPLES"] == 2 for k in names)
+    rows = slice(1, p.ny + 1)
+    assert np.array_equal(mean["ume"]["data"][1], m2["ume"][rows])
+    assert np.array_equal(mean["gyf"]["data"][0], g.gyf[rows]) and list(mean["ume"]["Time"]) == [0.0, 0.02]
+    oz = mean["omega_z"]["data"][1]
+    assert np.array_equal(oz, (m2["omega_y"] if quirk else m2["omega_z"])[rows])
+    tke = statsfile.read(str(tmp_path / "tke.h5"))
+    assert sorted(tke) == ["epsilon", "gyf", "time"]
+    assert np.array_equal(tke["epsilon"]["data"][0], m1["epsilon"][rows])
+    stats = statsfile.read(str(tmp_path / "stats.h5"))
+    assert sorted(stats) == ["GYF", "THBAR01", "UBAR", "VBAR", "WBAR"]
+    # two samples: weights 1/2 and (2-1)/2, exact in REAL*4
+    assert np.array_equal(stats["UBAR"]["data"][0], 0.5 * m2["ume"][rows] + 0.5 * m1["ume"][rows])
+    assert np.array_equal(stats["THBAR01"]["data"][0], 0.5 * m2["thme01"][rows] + 0.5 * m1["thme01"][rows])
+
+
+class _Profiles:
+    def __init__(self, p, grid, value, t):
+        self.p, self.grid, self.time, self.value = p, grid, t, value
+
+    def mean_stats(self):
+        ny2 = self.p.ny + 2
+        m = {k: np.zeros(ny2) for k in MEAN_NAMES + ["epsilon"] + [f"{s}01" for s in SCAL_NAMES]}
+        m["ume"] = np.full(ny2, self.value)
+        return m
+
+
+def test_running_mean_weights_single_precision(tmp_path):
+    """UBAR(j) = (1./FLOAT(N)) U + ((FLOAT(N)-1.)/FLOAT(N)) UBAR with REAL*4
+    weights (save_stats.f:110-117): 1/3 and 2/3 are not the FP64 values."""
+    p = P.kelvin_helmholtz(12, 9, 10)
+    g = G.channel_grid(G.create_grid(2, p.ny, 20.0, 1.5))
+    w = statsfile.StatsWriter(str(tmp_path))
+    vals = [1.0, 2.0, 7.0]
+    for v in vals:
+        w.save(_Profiles(p, g, v, 0.0))
+    w.save(_Profiles(p, g, 0.0, 0.0), final=True)
+    ubar = 0.0
+    for n, v in enumerate(vals, 1):
+        n32 = np.float32(n)
+        ubar = float(np.float32(1.0) / n32) * v + float((n32 - np.float32(1.0)) / n32) * ubar
+    got = statsfile.read(str(tmp_path / "stats.h5"))["UBAR"]["data"][0]
+    assert np.all(got == ubar) and ubar != 10.0 / 3.0
