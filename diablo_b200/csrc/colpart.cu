@@ -655,6 +655,7 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
     }
 
     // ---- D: new CU (projected), CP update, phi out; row-parallel ----------
+    bool bad = false;                // a non-finite new CU value (DIABLO_ENAN)
     for (int e = tid; e < (nf + 1) * nyp * 2; e += NT) {
         const int c = e & 1, r = e >> 1;
         const int j = r % nyp, q = r / nyp;
@@ -669,6 +670,7 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
                 else if (j >= 2) v = v - RDY[j] * (phi - sPh[(j - 1) * 2 + c]);
             }
             a.cu[(size_t)q * fs + (size_t)j * ps + g] = v;
+            bad = bad || !(isfinite(v.x) && isfinite(v.y));
         } else if (proj && j >= 1 && j <= ny) {
             const double2 phi = sPh[j * 2 + c];
             if (A.update_cp && j >= 2) {
@@ -678,6 +680,7 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
             if (A.store_phi) A.phi[(size_t)j * ps + g] = phi;
         }
     }
+    if (bad && A.nan_flag) atomicOr(A.nan_flag, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -898,6 +901,11 @@ __global__ void __launch_bounds__(128) k_proj(RemDivArgs a) {
     __syncthreads();
     // corrected velocity (rows 1..NY; CU2 rows 2..NY), CP += phi/h (rows
     // 2..NY) and phi (rows 1..NY), row-parallel
+    bool bad = false;                // a non-finite new velocity value (DIABLO_ENAN)
+    auto put = [&](double2* dst, const double2 v) {
+        *dst = v;
+        bad = bad || !(isfinite(v.x) && isfinite(v.y));
+    };
     for (int e = tid; e < 5 * ny * 4; e += 128) {
         const int c = e & 3, r = e >> 2;
         const int j = 1 + r % ny, q = r / ny;
@@ -906,17 +914,18 @@ __global__ void __launch_bounds__(128) k_proj(RemDivArgs a) {
         const size_t o = (size_t)j * ps + g;
         const double2 phi = sPh[j * 4 + c];
         if (q == 0) {
-            a.cu[o] = sV[((size_t)0 * NROW + j) * 4 + c] - ik(a.kx[g % d.ldx], phi);
+            put(a.cu + o, sV[((size_t)0 * NROW + j) * 4 + c] - ik(a.kx[g % d.ldx], phi));
         } else if (q == 2) {
-            a.cu[2 * fs + o] = sV[((size_t)2 * NROW + j) * 4 + c] - ik(a.kz[g / d.ldx], phi);
+            put(a.cu + 2 * fs + o, sV[((size_t)2 * NROW + j) * 4 + c] - ik(a.kz[g / d.ldx], phi));
         } else if (q == 1) {
-            if (j >= 2) a.cu[fs + o] = sV[((size_t)1 * NROW + j) * 4 + c] - RDY[j] * (phi - sPh[(j - 1) * 4 + c]);
+            if (j >= 2) put(a.cu + fs + o, sV[((size_t)1 * NROW + j) * 4 + c] - RDY[j] * (phi - sPh[(j - 1) * 4 + c]));
         } else if (q == 3) {
             if (a.update_cp && j >= 2) a.cp[o] = a.cp[o] + a.inv_h * phi;
         } else {
             a.phi[o] = phi;
         }
     }
+    if (bad && a.nan_flag) atomicOr(a.nan_flag, 1);
 }
 
 size_t phi_table_doubles(const Dims& d) { return d.splane() * (size_t)(NPART * 16); }

@@ -60,6 +60,7 @@ struct Handle {
     double* bcv = nullptr;        // [nf][nyp] BC-row values of the (0,0) mode
     double* d_tabs = nullptr;     // [nf][part_table_doubles] CN partition factors
     double* d_phitab = nullptr;   // [column][phi_table_doubles/column] phi partition factors
+    int* d_nan = nullptr;         // set by the kernels that write CU when a value is not finite
     signed char* kind = nullptr;
     double* dtmin = nullptr;
     double* d_k2 = nullptr;       // (KX^2+KZ^2)**BETA per padded column
@@ -137,7 +138,7 @@ void free_handle(Handle* h) {
     if (!h) return;
     for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
-                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_msums, h->d_tabs, h->d_phitab,
+                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_msums, h->d_nan, h->d_tabs, h->d_phitab,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
                     h->twz_f, h->nut, h->lu, h->la, h->lb, h->d_delta, h->ls, h->lr, h->lx, h->d_dyn,
                     h->mlp_x, h->mlp_t, h->mlp_s};
@@ -145,6 +146,18 @@ void free_handle(Handle* h) {
         if (q) cudaFree(q);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
+}
+
+// After a stream synchronisation: DIABLO_ENAN, once, if a kernel that writes
+// CU (the column kernel, the projection) met a value that is not finite
+// since the last check; the flag is cleared.
+static int take_nan(Handle* h) {
+    int v = 0;
+    CK(cudaMemcpyAsync(&v, h->d_nan, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (!v) return DIABLO_OK;
+    CK(cudaMemsetAsync(h->d_nan, 0, sizeof(int), h->st));
+    return fail(DIABLO_ENAN, "a non-finite value appeared in the state (CU) during a step");
 }
 
 // Host Fortran complex array (0:NXP,0:NZ+1,0:NY+1) <-> device spectral field.
@@ -416,6 +429,8 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = dmalloc(&h->yb, sizeof(double2) * h->x_field * d.np);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_tabs, sizeof(double) * part_table_doubles(d.nyp) * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_phitab, sizeof(double) * phi_table_doubles(d));
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_nan, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->d_nan, 0, sizeof(int));
     if (e == cudaSuccess) e = dmalloc((void**)&h->bcv, sizeof(double) * nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->kind, nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->dtmin, sizeof(double));
@@ -552,7 +567,7 @@ int diablo_gpu_download_state(void* handle, double* cu1, double* cu2, double* cu
     }
     if (cp) CK(copy_fourier(h, h->cp, nullptr, cp, 0, d.nyp));
     CK(cudaStreamSynchronize(h->st));
-    return DIABLO_OK;
+    return take_nan(h);
 }
 
 int diablo_gpu_download_phi(void* handle, double* phi) {
@@ -577,6 +592,7 @@ static int rem_div(Handle* h, int update_cp, double inv_h) {
     a.dyf = h->d_dyf;
     a.inv_h = inv_h;
     a.update_cp = update_cp;
+    a.nan_flag = h->d_nan;
     { ProfScope ps(h, DIABLO_KERNEL_REMDIV); CK(launch_remdiv(a, h->st)); }
     h->launches += 1;
     return DIABLO_OK;
@@ -612,6 +628,7 @@ static int courant(Handle* h, double* delta_t, double* h_bar, const double* phys
     double vmin = inf;
     CK(cudaMemcpyAsync(&vmin, h->dtmin, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
+    if (int rc = take_nan(h)) return rc;   // DELTA_T and H_BAR keep their values
     dt = std::fmin(dt, vmin);
     double DELTA_T;
     if (dt <= 0) DELTA_T = 0.0001;
@@ -890,6 +907,7 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     ca.project = cfl ? 0 : 1;     // COURANT sees the velocity before the projection
     ca.update_cp = 1;
     ca.store_phi = 0;             // phi stays where REM_DIV_CHAN alone puts it
+    ca.nan_flag = h->d_nan;
     {
         ProfScope ps(h, DIABLO_KERNEL_COLUMN);
         if (h->fp32) CK(launch_colpart<cpx<float>>(ca, (const cpx<float>*)h->nl, h->d_tabs, h->st));
@@ -1340,7 +1358,7 @@ int diablo_gpu_synchronize(void* handle) {
     Handle* h = (Handle*)handle;
     if (!h) return fail(DIABLO_EINVAL, "null handle");
     CK(cudaStreamSynchronize(h->st));
-    return DIABLO_OK;
+    return take_nan(h);
 }
 
 int diablo_gpu_get_stream(void* handle, void** stream) {

@@ -86,6 +86,7 @@ struct ColArgs {
     int project;          // run the REM_DIV projection
     int update_cp;        // CP += phi/h on J = 2..NY
     int store_phi;
+    int* nan_flag;        // set to 1 when a new CU value is not finite (may be null)
 };
 
 struct RemDivArgs {
@@ -101,6 +102,7 @@ struct RemDivArgs {
     const double* dyf;
     double inv_h;         // 1/TEMP4 for the pressure update
     int update_cp;        // CP += phi/h on J = 2..NY
+    int* nan_flag;        // set to 1 when a new velocity value is not finite (may be null)
 };
 
 // Physical-space CN steps of the LES branch (les.cu).

@@ -39,10 +39,16 @@ extern "C" {
 #define DIABLO_EINVAL       -1   /* bad dimensions or parameters, null pointer */
 #define DIABLO_ERADIX       -2   /* NX or NZ is not a product of 2, 3 and 5 */
 #define DIABLO_ECUDA        -3   /* a CUDA runtime call failed */
-#define DIABLO_ENOTSUP      -4   /* feature not supported (RK_CHAN_2, LES) */
-#define DIABLO_ENAN         -5   /* a non-finite value was found in the state */
+#define DIABLO_ENOTSUP      -4   /* feature not supported (RK_CHAN_2, LES_MODEL_TYPE 3) */
+#define DIABLO_ENAN         -5   /* a non-finite value was found in the state: the kernels
+                                    that write CU flag it on the device, and the next call
+                                    that synchronises (diablo_gpu_synchronize,
+                                    download_state, COURANT inside rk_chan_1 or
+                                    diablo_gpu_courant) returns it once */
 #define DIABLO_ENOMEM       -6   /* device allocation failed */
-#define DIABLO_ETIMEOUT     -7   /* a bounded wait inside a kernel gave up */
+#define DIABLO_ETIMEOUT     -7   /* a bounded wait inside a kernel gave up; reserved: no
+                                    kernel of this library waits on another block, stream
+                                    or device, so no call returns it */
 
 #define DIABLO_MAX_TH        4   /* largest N_TH the library accepts */
 
