@@ -42,10 +42,26 @@ EXPORTS = [
     "diablo_gpu_get_stream", "diablo_gpu_set_profiling", "diablo_gpu_kernel_times",
     "diablo_gpu_rem_div_chan_noalloc", "diablo_gpu_autotune", "diablo_gpu_batch_create",
     "diablo_gpu_batch_step", "diablo_gpu_batch_destroy", "diablo_gpu_filter_chan", "diablo_gpu_download_nu_t",
-    "diablo_gpu_mean_stats",
+    "diablo_gpu_mean_stats", "diablo_gpu_set_user_rhs",
     "diablo_gpu_sgs_samples", "diablo_gpu_set_sgs_mlp",
 ]
 KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
+
+
+class UserRhsArgs(ctypes.Structure):
+    """diablo_user_rhs_args: what a USER_RHS_CHAN_FOURIER / _PHYSICAL
+    callback receives (device pointers, strides, the handle's stream)."""
+    _fields_ = [("rk_step", ctypes.c_int), ("time_step", ctypes.c_int), ("time", ctypes.c_double),
+                ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("n_th", ctypes.c_int),
+                ("nkx", ctypes.c_int), ("tnkz", ctypes.c_int),
+                ("s_field", ctypes.c_longlong), ("s_plane", ctypes.c_longlong), ("s_row", ctypes.c_longlong),
+                ("p_field", ctypes.c_longlong), ("p_plane", ctypes.c_longlong),
+                ("cu", ctypes.c_void_p), ("cf_add", ctypes.c_void_p), ("u", ctypes.c_void_p),
+                ("f_add", ctypes.c_void_p), ("stream", ctypes.c_void_p)]
+
+
+USER_RHS_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.POINTER(UserRhsArgs))
+USER_RHS_FOURIER, USER_RHS_PHYSICAL = 0, 1
 
 
 class DiabloError(RuntimeError):
@@ -81,6 +97,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_courant.argtypes = [vp, dp, dp]
     L.diablo_gpu_stats.argtypes = [vp, dp]
     L.diablo_gpu_mean_stats.argtypes = [vp, dp, dp, dp]
+    L.diablo_gpu_set_user_rhs.argtypes = [vp, ip, USER_RHS_FN, vp]
     L.diablo_gpu_kernel_launches.argtypes = [vp]
     L.diablo_gpu_kernel_launches.restype = ctypes.c_longlong
     L.diablo_gpu_last_error.restype = ctypes.c_char_p
@@ -212,6 +229,21 @@ class Channel:
         buf = np.zeros(physical_shape(self.p))
         _check(self.L.diablo_gpu_download_nu_t(self._h, _dp(buf)), "diablo_gpu_download_nu_t")
         return buf[:, : self.p.nz, : self.p.nx].copy()
+
+    def set_user_rhs(self, kind: int, fn) -> None:
+        """USER_RHS_CHAN_FOURIER (kind USER_RHS_FOURIER) or _PHYSICAL
+        (USER_RHS_PHYSICAL): fn(args: UserRhsArgs) runs once per substage and
+        writes the terms to add to CF into args.cf_add / args.f_add on
+        args.stream; None removes the hook."""
+        if not hasattr(self, "_user_rhs"):
+            self._user_rhs = {}
+        if fn is None:
+            self._user_rhs.pop(kind, None)
+            _check(self.L.diablo_gpu_set_user_rhs(self._h, kind, USER_RHS_FN(), None), "diablo_gpu_set_user_rhs")
+            return
+        cb = USER_RHS_FN(lambda _user, args: fn(args.contents))
+        self._user_rhs[kind] = cb
+        _check(self.L.diablo_gpu_set_user_rhs(self._h, kind, cb, None), "diablo_gpu_set_user_rhs")
 
     def set_sgs_mlp(self, mlp) -> None:
         """Attach a closure network (diablo_b200.mlp.SgsMlp) for

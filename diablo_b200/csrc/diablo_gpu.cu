@@ -61,6 +61,13 @@ struct Handle {
     double* d_tabs = nullptr;     // [nf][part_table_doubles] CN partition factors
     double* d_phitab = nullptr;   // [column][phi_table_doubles/column] phi partition factors
     int* d_nan = nullptr;         // set by the kernels that write CU when a value is not finite
+    // user right-hand-side hooks (USER_RHS_CHAN_FOURIER / _PHYSICAL), their
+    // Fourier-space addend (nf fields, S) and, for the physical hook, the
+    // physical fields and their addend (2 nf fields, P); allocated on first use
+    diablo_user_rhs_fn urhs_fn[2] = {nullptr, nullptr};
+    void* urhs_user[2] = {nullptr, nullptr};
+    double2* ufa = nullptr;
+    double* uphys = nullptr;
     signed char* kind = nullptr;
     double* dtmin = nullptr;
     double* d_k2 = nullptr;       // (KX^2+KZ^2)**BETA per padded column
@@ -138,7 +145,7 @@ void free_handle(Handle* h) {
     if (!h) return;
     for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
-                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_msums, h->d_nan, h->d_tabs, h->d_phitab,
+                    h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_msums, h->d_nan, h->ufa, h->uphys, h->d_tabs, h->d_phitab,
                     h->bcv, h->kind, h->dtmin, h->d_k2, h->d_rows, h->twn_d, h->twm_d, h->twz_d, h->twn_f, h->twm_f,
                     h->twz_f, h->nut, h->lu, h->la, h->lb, h->d_delta, h->ls, h->lr, h->lx, h->d_dyn,
                     h->mlp_x, h->mlp_t, h->mlp_s};
@@ -199,6 +206,15 @@ cudaError_t copy_physical(Handle* h, double* dev, const double* host_in, double*
     if (host_in) { c.srcPtr = hp; c.dstPtr = dp; c.kind = cudaMemcpyHostToDevice; }
     else { c.srcPtr = dp; c.dstPtr = hp; c.kind = cudaMemcpyDeviceToHost; }
     return cudaMemcpy3DAsync(&c, h->st);
+}
+
+// dst += src over n complex elements (the user right-hand side added to NL or CF).
+template <typename T>
+__global__ void k_add_user(cpx<T>* __restrict__ dst, const double2* __restrict__ src, size_t n) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const double2 v = src[e];
+        dst[e] = dst[e] + mk(T(v.x), T(v.y));
+    }
 }
 
 // APPLY_BC_VEL_LOWER / _UPPER (channel.f:2285-2492) on the device state.
@@ -713,6 +729,67 @@ static cudaError_t les_to_fourier(Handle* h, const double* P, int nfld, double2*
     return e;
 }
 
+// USER_RHS_CHAN_FOURIER / USER_RHS_CHAN_PHYSICAL (user_rhs.f:1-122): run the
+// callbacks that are set and leave the sum of their Fourier-space terms in
+// h->ufa (*any = true).  U (P layout, nf fields) is the physical state when
+// the caller already has it (the LES branch); otherwise, and only for the
+// physical hook, it is made here from CU with the FP64 transforms.  Uses xb
+// and api_s as scratch: call before the substage's own transforms.
+static int user_rhs(Handle* h, int rk_step, int time_step, double time, const double* U, bool* any) {
+    *any = false;
+    if (!h->urhs_fn[0] && !h->urhs_fn[1]) return DIABLO_OK;
+    const Dims& d = h->d;
+    const size_t pf = (size_t)d.nyp * d.nz * d.nx;
+    if (!h->ufa) {
+        cudaError_t e = cudaMalloc((void**)&h->ufa, sizeof(double2) * h->s_field * d.nf);
+        if (e != cudaSuccess) { h->ufa = nullptr; return fail(DIABLO_ENOMEM, "user right-hand side buffer"); }
+    }
+    CK(cudaMemsetAsync(h->ufa, 0, sizeof(double2) * h->s_field * d.nf, h->st));
+    diablo_user_rhs_args a;
+    std::memset(&a, 0, sizeof(a));
+    a.rk_step = rk_step; a.time_step = time_step; a.time = time;
+    a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.n_th = d.nth; a.nkx = d.nkx; a.tnkz = d.tnkz;
+    a.s_field = (long long)h->s_field; a.s_plane = (long long)h->s_plane; a.s_row = d.ldx;
+    a.p_field = (long long)pf; a.p_plane = (long long)d.nz * d.nx;
+    a.cu = reinterpret_cast<const double*>(h->cu);
+    a.cf_add = reinterpret_cast<double*>(h->ufa);
+    a.stream = (void*)h->st;
+    if (h->urhs_fn[DIABLO_USER_RHS_FOURIER]) {
+        h->urhs_fn[DIABLO_USER_RHS_FOURIER](h->urhs_user[DIABLO_USER_RHS_FOURIER], &a);
+        CK(cudaGetLastError());
+    }
+    if (h->urhs_fn[DIABLO_USER_RHS_PHYSICAL]) {
+        if (!h->uphys) {
+            cudaError_t e = cudaMalloc((void**)&h->uphys, sizeof(double) * pf * 2 * d.nf);
+            if (e != cudaSuccess) { h->uphys = nullptr; return fail(DIABLO_ENOMEM, "user right-hand side fields"); }
+        }
+        double* fadd = h->uphys + pf * d.nf;
+        if (!U) {
+            CK(launch_zinv<double>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, h->twz_d, h->st));
+            for (int f = 0; f < d.nf; ++f)
+                CK(launch_xinv(d, (const double2*)h->xb + (size_t)f * h->x_field, h->uphys + (size_t)f * pf, 0, d.nyp,
+                               h->pm, h->twm_d, h->twn_d, h->st));
+            h->launches += 1 + d.nf;
+            U = h->uphys;
+        }
+        CK(cudaMemsetAsync(fadd, 0, sizeof(double) * pf * d.nf, h->st));
+        a.u = U;
+        a.f_add = fadd;
+        h->urhs_fn[DIABLO_USER_RHS_PHYSICAL](h->urhs_user[DIABLO_USER_RHS_PHYSICAL], &a);
+        CK(cudaGetLastError());
+        for (int f = 0; f < d.nf; ++f) {       // FFT_XZ_TO_FOURIER(S1,CS1,0,NY+1), then CF += CS1
+            CK(launch_xfwd(d, fadd + (size_t)f * pf, h->xb, 0, d.nyp, h->pm, h->twm_d, h->twn_d, h->st));
+            CK(launch_zfwd_pack(d, h->xb, h->api_s, 0, d.nyp, h->pz, h->twz_d, h->st));
+            k_add_user<double><<<1184, 256, 0, h->st>>>(reinterpret_cast<cpx<double>*>(h->ufa + (size_t)f * h->s_field),
+                                                        h->api_s, h->s_field);
+            CK(cudaGetLastError());
+        }
+        h->launches += 3 * d.nf;
+    }
+    *any = true;
+    return DIABLO_OK;
+}
+
 // RK_CHAN_1 with LES set (channel.f:62-1073 with the LES branches), in the
 // reference's order: Fourier right-hand sides; when the subgrid model runs
 // (sgs), les_chan (strain rates, |S|, NU_T, tau_ij and the cross terms into
@@ -796,6 +873,17 @@ static int les_substage(Handle* h, int rk_step, int time_step, double time, doub
         CK(les_to_phys(h, h->cu, 3, h->lu, 0, nyp));
     }
     if (d.nth > 0) CK(les_to_phys(h, h->cu + 3 * h->s_field, d.nth, h->lu + 3 * pf, 0, nyp));
+    {   // USER_RHS_CHAN_FOURIER / _PHYSICAL (channel.f:297, 578): CF += their terms
+        bool any = false;
+        int rc = user_rhs(h, rk_step, time_step, time, h->lu, &any);
+        if (rc) return rc;
+        if (any) {
+            k_add_user<double><<<1184, 256, 0, h->st>>>(reinterpret_cast<cpx<double>*>(h->cf), h->ufa,
+                                                        h->s_field * d.nf);
+            CK(cudaGetLastError());
+            h->launches += 1;
+        }
+    }
     // nonlinear terms from the physical fields: x spectra, then the products
     // and z-forward kernels of the Fourier-space path
     for (int f = 0; f < d.nf; ++f)
@@ -860,9 +948,17 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     const double TEMP4 = h_bar[r];
     const double TEMP5 = beta_bar[r] * h_bar[r];
     int rc;
+    bool user = false;    // USER_RHS_CHAN_FOURIER / _PHYSICAL (channel.f:297, 578)
+    if ((rc = user_rhs(h, rk_step, time_step, time, nullptr, &user))) return rc;
     if (h->fp32) rc = run_transforms<float>(h);
     else rc = run_transforms<double>(h);
     if (rc) return rc;
+    if (user) {           // their terms join the nonlinear term, which CF takes whole
+        if (h->fp32) k_add_user<float><<<1184, 256, 0, h->st>>>((cpx<float>*)h->nl, h->ufa, h->s_field * d.nf);
+        else k_add_user<double><<<1184, 256, 0, h->st>>>((cpx<double>*)h->nl, h->ufa, h->s_field * d.nf);
+        CK(cudaGetLastError());
+        h->launches += 1;
+    }
     CnArgs a;
     a.d = d;
     a.cu = h->cu;
@@ -966,6 +1062,16 @@ int diablo_gpu_sgs_samples(void* handle, int width, int stride, float* x, float*
     cudaFree(ds_);
     h->launches += 5;
     if (e != cudaSuccess) return fail(DIABLO_ECUDA, std::string("closure samples: ") + cudaGetErrorString(e));
+    return DIABLO_OK;
+}
+
+int diablo_gpu_set_user_rhs(void* handle, int kind, diablo_user_rhs_fn fn, void* user) {
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(DIABLO_EINVAL, "null handle");
+    if (kind != DIABLO_USER_RHS_FOURIER && kind != DIABLO_USER_RHS_PHYSICAL)
+        return fail(DIABLO_EINVAL, "kind must be DIABLO_USER_RHS_FOURIER or DIABLO_USER_RHS_PHYSICAL");
+    h->urhs_fn[kind] = fn;
+    h->urhs_user[kind] = fn ? user : nullptr;
     return DIABLO_OK;
 }
 
@@ -1513,6 +1619,7 @@ int diablo_gpu_batch_create(void* const* handles, const double* delta_t, int n, 
         if (h->p.variable_dt) return fail(DIABLO_ENOTSUP, "batched instances need a fixed time step (variable_dt = 0)");
         if (h->p.f_type == 2) return fail(DIABLO_ENOTSUP, "batched instances cannot have time-dependent forcing");
         if (h->p.les) return fail(DIABLO_ENOTSUP, "batched instances cannot run the LES branch");
+        if (h->urhs_fn[0] || h->urhs_fn[1]) return fail(DIABLO_ENOTSUP, "batched instances cannot have user right-hand sides");
         if (h->profiling) return fail(DIABLO_EINVAL, "batched instance with profiling on");
         if (!(delta_t[i] > 0.0)) return fail(DIABLO_EINVAL, "batched instance with delta_t <= 0");
     }

@@ -206,6 +206,45 @@ int diablo_gpu_stats(void* handle, double* profiles);
 #define DIABLO_NSCAL         5
 int diablo_gpu_mean_stats(void* handle, double* chan, double* scal, double* epsilon);
 
+/* USER_RHS_CHAN_FOURIER and USER_RHS_CHAN_PHYSICAL (for/user_rhs.f:1-122),
+ * which RK_CHAN_1 calls at for/channel.f:297 and :578 so that a user can
+ * add terms to the right-hand sides CF1..CF3, CFTH (empty in the reference).
+ * Here the user's host callback gets device pointers and the handle's stream
+ * and writes the terms to add; the library adds them to CF in every substage,
+ * where the reference forms CF (rows JSTART..JEND, CF2 rows 2..NY).  Nothing
+ * of this runs while no callback is set.
+ *  DIABLO_USER_RHS_FOURIER:  cu holds CU1..CU3, CTH(1..N_TH) at the start of
+ *    the substage; write Fourier-space terms into cf_add (zeroed).
+ *  DIABLO_USER_RHS_PHYSICAL: u holds U1..U3, TH(1..N_TH) in physical space
+ *    (planes 0..NY+1); write physical-space terms into f_add (zeroed); the
+ *    library transforms them with FFT_XZ_TO_FOURIER and adds them to CF,
+ *    the pattern of user_rhs.f:14-40.
+ * Device layouts, FP64: Fourier field f, plane J, packed kz row m (0..TNKZ),
+ * kx (0..NKX) is the complex element f*s_field + J*s_plane + m*s_row + kx
+ * (interleaved re, im); physical field f, plane J, z, x is the double
+ * f*p_field + J*p_plane + z*NX + x.  The callback enqueues its work on
+ * `stream` (a cudaStream_t) or finishes it before returning.  In FP32-split
+ * mode the Fourier-space terms join the nonlinear term and are rounded to
+ * FP32 with it.  fn = NULL removes the hook.  No counterpart in the
+ * reference's interface beyond the two subroutines; batched handles reject
+ * hooks. */
+typedef struct diablo_user_rhs_args {
+    int rk_step, time_step;
+    double time;
+    int nx, ny, nz, n_th, nkx, tnkz;
+    long long s_field, s_plane, s_row;    /* complex elements */
+    long long p_field, p_plane;           /* doubles */
+    const double* cu;
+    double* cf_add;
+    const double* u;                      /* physical hook only, else NULL */
+    double* f_add;                        /* physical hook only, else NULL */
+    void* stream;
+} diablo_user_rhs_args;
+typedef void (*diablo_user_rhs_fn)(void* user, const diablo_user_rhs_args* args);
+#define DIABLO_USER_RHS_FOURIER  0
+#define DIABLO_USER_RHS_PHYSICAL 1
+int diablo_gpu_set_user_rhs(void* handle, int kind, diablo_user_rhs_fn fn, void* user);
+
 /* The CUDA stream (a cudaStream_t) all work of the handle is queued on, as
  * an opaque pointer: callers may record timing events on it. */
 int diablo_gpu_get_stream(void* handle, void** stream);

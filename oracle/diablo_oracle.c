@@ -121,6 +121,10 @@ struct orc_state {
      * TEMP<->CTEMP share one buffer each as header_les:31-37 equivalences them */
     double *NU_T, *SIJ[6], *TEMP;
     float* MLP;           /* learned closure parameters (LES_MODEL_TYPE 4), or NULL */
+    /* USER_RHS_CHAN_FOURIER / _PHYSICAL: called with the state as the
+     * reference's user routines see it, or NULL (the reference's empty ones) */
+    void (*user_fn[2])(void*);
+    void* user_data[2];
     fftplan px_plan, pz_plan;
 };
 
@@ -1324,7 +1328,9 @@ void orc_rk_chan_1(orc_state* s, int rk_step) {
                     CX(CFTHn, i, k, j) = CX(CFTHn, i, k, j) - CX(CU1, i, k, j) * p->drhodx[n] -
                                          CX(CU3, i, k, j) * p->drhodz[n];
     }
-    /* USER_RHS_CHAN_FOURIER: empty hook (user_rhs.f:77-121). */
+    /* USER_RHS_CHAN_FOURIER (user_rhs.f:77-121): CU in Fourier space, CF the
+     * Fourier right-hand sides so far */
+    if (s->user_fn[0]) s->user_fn[0](s->user_data[0]);
     if (p->les && (!p->create_new_flow || s->TIME_STEP > 100)) {
         /* LES branch (channel.f:303-384): subgrid stress into CF, U to
          * physical space, physical BCs re-applied, then the explicit
@@ -1422,7 +1428,9 @@ void orc_rk_chan_1(orc_state* s, int rk_step) {
              0.25 * pow(PH(U2, i, k, j) + PH(U2, i, k, j - 1), 2.0)) /
                 DY[j]);
     ACCUM(2, NY, CX(CF2, i, k, j) = CX(CF2, i, k, j) - CX(CS1, i, k, j));
-    /* USER_RHS_CHAN_PHYSICAL: empty hook (user_rhs.f:1-74). */
+    /* USER_RHS_CHAN_PHYSICAL (user_rhs.f:1-74): U1..U3, TH in physical space,
+     * CF in Fourier space */
+    if (s->user_fn[1]) s->user_fn[1](s->user_data[1]);
 
     /* CR += beta h CF (channel.f:581-595) */
 #pragma omp parallel for num_threads(nthreads())
@@ -2113,6 +2121,12 @@ void orc_mean_stats(orc_state* s, double* chan, double* scal, double* eps) {
 /* keeps its horizontally filtered value: the reference copies an element of  */
 /* VEC_C that it never sets there.                                            */
 /* ------------------------------------------------------------------------ */
+void orc_set_user_rhs(orc_state* s, int kind, void (*fn)(void*), void* user) {
+    if (kind < 0 || kind > 1) return;
+    s->user_fn[kind] = fn;
+    s->user_data[kind] = user;
+}
+
 void orc_filter_chan(orc_state* s, int n) {
     if (n < 1 || n > s->NTH) return;
     const int NY = s->NY, NKX = s->NKX, TNKZ = s->TNKZ;

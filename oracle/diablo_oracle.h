@@ -78,6 +78,10 @@ void orc_stats(orc_state* s, double* profiles);
 /* Every mean.h5 / tke.h5 profile: chan DIABLO_NMEAN*(NY+2), scal
  * N_TH*DIABLO_NSCAL*(NY+2), eps NY+2 (or NULL), as diablo_gpu_mean_stats. */
 void orc_mean_stats(orc_state* s, double* chan, double* scal, double* eps);
+/* USER_RHS_CHAN_FOURIER (kind 0, channel.f:297) / USER_RHS_CHAN_PHYSICAL
+ * (kind 1, channel.f:578): fn(user) runs at that point of orc_rk_chan_1 and
+ * may change CF1..CF3, CFTH through orc_array; NULL removes it. */
+void orc_set_user_rhs(orc_state* s, int kind, void (*fn)(void*), void* user);
 /* Parameters of the learned closure (LES_MODEL_TYPE 4), in the layout of the
  * GPU library's diablo_mlp_set_params; NULL removes it. */
 void orc_set_mlp(orc_state* s, const float* params);

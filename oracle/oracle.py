@@ -24,6 +24,9 @@ _LIB = os.path.join(_HERE, "liboracle.so")
  ORC_GY, ORC_GYF, ORC_DY, ORC_DYF, ORC_KX, ORC_KZ, ORC_NU_T) = range(24)
 
 
+USER_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p)
+
+
 def build() -> str:
     """Compile liboracle.so with the committed Makefile if it is missing or stale."""
     src = [os.path.join(_HERE, f) for f in ("diablo_oracle.c", "diablo_oracle.h", "Makefile")]
@@ -60,6 +63,7 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [vp]
         L.orc_stats.argtypes = [vp, dp]
         L.orc_mean_stats.argtypes = [vp, dp, dp, dp]
+        L.orc_set_user_rhs.argtypes = [vp, ip, USER_FN, vp]
         L.orc_set_mlp.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
         L.orc_cdft.restype = ip
         L.orc_cdft.argtypes = [ip, dp, ip]
@@ -192,6 +196,20 @@ class Oracle:
 
     def filter_chan(self, n: int = 1) -> None:
         lib().orc_filter_chan(self._h, n)
+
+    def set_user_rhs(self, kind: int, fn) -> None:
+        """USER_RHS_CHAN_FOURIER (kind 0) / _PHYSICAL (kind 1): fn(oracle)
+        runs at that point of RK_CHAN_1 and may change self.cf / self.cfth
+        in place; None removes it."""
+        if not hasattr(self, "_user"):
+            self._user = {}
+        if fn is None:
+            self._user.pop(kind, None)
+            lib().orc_set_user_rhs(self._h, kind, USER_FN(), None)
+            return
+        cb = USER_FN(lambda _: fn(self))
+        self._user[kind] = cb
+        lib().orc_set_user_rhs(self._h, kind, cb, None)
 
     def set_mlp(self, params) -> None:
         """The learned closure's parameters (LES_MODEL_TYPE 4), or None."""
