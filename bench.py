@@ -68,8 +68,8 @@ def parse_args():
     ap.add_argument("--closure-steps", type=int, default=20000)
     ap.add_argument("--only", choices=["les", "closure"], default=None,
                     help="run one leg alone and print its JSON (for profiling captures)")
-    ap.add_argument("--error-steps", type=int, default=500,
-                    help="steps after which FP32-split is compared with FP64 (besides 100)")
+    ap.add_argument("--error-steps", type=int, default=2000,
+                    help="last step count at which FP32-split is compared with FP64 (besides 100 and 500)")
     return ap.parse_args()
 
 
@@ -461,12 +461,12 @@ def run_ours(args, rank, world, local_rank):
         ms64 = timed_steps(c64, args.steps, torch)
         c64.close()
         # error of FP32-split against the all-FP64 path from the same start,
-        # after 100 and args.error_steps time steps
+        # after 100, 500 and args.error_steps time steps
         c64, _, _ = make_channel(w, PREC_FP64, u, th)
         c32b, _, _ = make_channel(w, PREC_FP32SPLIT, u, th)
         errs = {}
         done = 0
-        for n in sorted({100, args.error_steps}):
+        for n in sorted({100, 500, args.error_steps}):
             c64.step(n - done)
             c32b.step(n - done)
             done = n
