@@ -16,6 +16,16 @@ keeps (it increments it once per dataset written).
 The reference writes omega_y into mean.h5's ``omega_z`` group
 (save_stats.f:421-423); ``StatsWriter(omega_z_quirk=True)``, the default,
 does the same, and ``False`` writes the true omega_z.
+
+``formats`` may add ``"txt"``: the files the reference writes when it is
+built without HDF5 (save_stats.f:68-89, 427-447, 639-658, 1191-1205) --
+mean.txt, mean_th.txt and tke.txt, which a run appends to (the reference
+never closes their units), and stats.txt on the final call.  Their rows use
+the reference's FORMAT statements and are reproduced byte for byte (F
+editing rounds like Python's fixed-point formatting; a value too wide for
+its field prints as asterisks); the list-directed header lines (TIME_STEP,
+TIME, DELTA_T and UBULK) follow gfortran's list-directed style: integers in
+12 columns, REAL*8 as G25.17E3 after one blank.
 """
 from __future__ import annotations
 
@@ -88,16 +98,70 @@ def read(path: str) -> dict:
     return out
 
 
+def fortran_f(x: float, w: int, d: int) -> str:
+    """Fortran Fw.d of one value."""
+    t = f"{x:{w}.{d}f}"
+    return "*" * w if len(t) > w else t
+
+
+def fortran_i(i: int, w: int) -> str:
+    t = f"{i:{w}d}"
+    return "*" * w if len(t) > w else t
+
+
+def list_directed(*items) -> str:
+    """One gfortran list-directed record: INTEGER in 12 columns, REAL*8 as
+    1PG25.17E3 preceded by a blank."""
+    out = []
+    for v in items:
+        if isinstance(v, (int, np.integer)):
+            out.append(f"{int(v):12d}")
+            continue
+        x = float(v)
+        a = abs(x)
+        r = float(f"{a:.16e}") if a != 0.0 else 0.0          # 17 significant digits
+        if r == 0.0 or 0.1 <= r < 1e17:
+            # G editing: 10**(k-1) <= |x| < 10**k prints d - k = 17 - k decimals (zero: 16)
+            k = 1 if r == 0.0 else (0 if r < 1.0 else len(str(int(r))))
+            body = f"{x:.{17 - k}f}".rjust(20) + " " * 5
+        else:
+            m, e = f"{x:.16E}".split("E")
+            body = f"{m}E{int(e):+04d}".rjust(25)
+        out.append(" " + body)
+    return "".join(out)
+
+
+def ubulk(p, grid, ume: np.ndarray) -> float:
+    """INTEGRATE_Y_VAR of the mean velocity (mpi.f:1610-1632): the GY-point
+    trapezoid sum over J = 2..NY divided by LY."""
+    dy = np.asarray(grid.dy, dtype=np.float64)
+    res = 0.0
+    for j in range(2, p.ny + 1):
+        res = res + 0.5 * (ume[j] + ume[j - 1]) * dy[j]
+    return res / p.ly
+
+
 class StatsWriter:
     """The output side of SAVE_STATS_CHAN for one channel run: mean.h5 and
     tke.h5 on every call, the running means UBAR, VBAR, WBAR, THBARnn
     (save_stats.f:104-123) and stats.h5 on the final call."""
 
-    def __init__(self, directory: str, omega_z_quirk: bool = True):
+    def __init__(self, directory: str, omega_z_quirk: bool = True, formats=("h5",)):
         self.dir = directory
         self.omega_z_quirk = omega_z_quirk
+        self.formats = tuple(formats)
         self.nsamples = 0
         self.bar: dict[str, np.ndarray] = {}
+        self._opened: set[str] = set()
+
+    def _text(self, name: str, lines: list[str]) -> None:
+        """Write records to a text file the run keeps open: the first write
+        of the run starts it afresh, later ones append."""
+        path = os.path.join(self.dir, name)
+        mode = "a" if name in self._opened else "w"
+        self._opened.add(name)
+        with open(path, mode) as f:
+            f.write("".join(line + "\n" for line in lines))
 
     def _f(self, name: str) -> StatFile:
         return StatFile(os.path.join(self.dir, name))
@@ -108,10 +172,23 @@ class StatsWriter:
         p, gyf, t = c.p, np.asarray(c.grid.gyf, dtype=np.float64), float(c.time)
         rows = slice(1, p.ny + 1)
         if final:
-            f = self._f("stats.h5")
-            f.write_stat("GYF", gyf[rows], t)
-            for name in ["UBAR", "VBAR", "WBAR"] + [f"THBAR{n + 1:02d}" for n in range(p.n_th)]:
-                f.write_stat(name, self.bar.get(name, np.zeros(p.ny + 2))[rows], t)
+            zero = np.zeros(p.ny + 2)
+            if "h5" in self.formats:
+                f = self._f("stats.h5")
+                f.write_stat("GYF", gyf[rows], t)
+                for name in ["UBAR", "VBAR", "WBAR"] + [f"THBAR{n + 1:02d}" for n in range(p.n_th)]:
+                    f.write_stat(name, self.bar.get(name, zero)[rows], t)
+            if "txt" in self.formats:
+                # 201 FORMAT(I3,',',F16.9,',',F16.9,',',F16.9,',',F16.9), 202 for each scalar
+                ub, vb, wb = (self.bar.get(k, zero) for k in ("UBAR", "VBAR", "WBAR"))
+                lines = [",".join([fortran_i(j, 3)] + [fortran_f(v, 16, 9) for v in (gyf[j], ub[j], vb[j], wb[j])])
+                         for j in range(1, p.ny + 1)]
+                for n in range(p.n_th):
+                    tb = self.bar.get(f"THBAR{n + 1:02d}", zero)
+                    lines += [",".join([fortran_i(j, 3), fortran_f(gyf[j], 16, 9), fortran_f(tb[j], 16, 9)])
+                              for j in range(1, p.ny + 1)]
+                with open(os.path.join(self.dir, "stats.txt"), "w") as f:
+                    f.write("".join(line + "\n" for line in lines))
             return None
         m = c.mean_stats()
         # running means with REAL*4 weights: (1./FLOAT(N)) and ((FLOAT(N)-1.)/FLOAT(N))
@@ -127,17 +204,41 @@ class StatsWriter:
             new = old.copy()
             new[rows] = w1 * v[rows] + w2 * old[rows]
             self.bar[name] = new
-        mean = self._f("mean.h5")
-        mean.write_real("time", t)
-        mean.write_stat("gyf", gyf[rows], t)
-        for name in MEAN_NAMES:
-            v = m["omega_y"] if (name == "omega_z" and self.omega_z_quirk) else m[name]
-            mean.write_stat(name, v[rows], t)
-        for n in range(p.n_th):
-            for name in SCAL_NAMES:
-                mean.write_stat(f"{name}{n + 1:02d}", m[f"{name}{n + 1:02d}"][rows], t)
-        tke = self._f("tke.h5")
-        tke.write_real("time", t)
-        tke.write_stat("gyf", gyf[rows], t)
-        tke.write_stat("epsilon", m["epsilon"][rows], t)
+        if "h5" in self.formats:
+            mean = self._f("mean.h5")
+            mean.write_real("time", t)
+            mean.write_stat("gyf", gyf[rows], t)
+            for name in MEAN_NAMES:
+                v = m["omega_y"] if (name == "omega_z" and self.omega_z_quirk) else m[name]
+                mean.write_stat(name, v[rows], t)
+            for n in range(p.n_th):
+                for name in SCAL_NAMES:
+                    mean.write_stat(f"{name}{n + 1:02d}", m[f"{name}{n + 1:02d}"][rows], t)
+            tke = self._f("tke.h5")
+            tke.write_real("time", t)
+            tke.write_stat("gyf", gyf[rows], t)
+            tke.write_stat("epsilon", m["epsilon"][rows], t)
+        if "txt" in self.formats:
+            step, dt = int(c.time_step), float(c.delta_t)
+            ub = ubulk(p, c.grid, m["ume"])
+            head = [list_directed(step, t, dt), list_directed(ub)]
+            # 401 FORMAT(I3,' ',17(F30.20,' ')): V averaged to GYF, the true omega_z
+            cols = ["ume", None, "wme", "urms", "vrms", "wrms", "uv", "uw", "wv", "dudy", "dwdy", "cp", "shear",
+                    "omega_x", "omega_y", "omega_z"]
+            lines = []
+            for j in range(1, p.ny + 1):
+                vals = [gyf[j]] + [0.5 * (m["vme"][j + 1] + m["vme"][j]) if k is None else m[k][j] for k in cols]
+                lines.append(fortran_i(j, 3) + " " + "".join(fortran_f(v, 30, 20) + " " for v in vals))
+            self._text("mean.txt", head + lines)
+            # 402 FORMAT(I3,' ',6(F30.20,' '))
+            lines = []
+            for n in range(p.n_th):
+                for j in range(1, p.ny + 1):
+                    vals = [gyf[j]] + [m[f"{k}{n + 1:02d}"][j] for k in SCAL_NAMES]
+                    lines.append(fortran_i(j, 3) + " " + "".join(fortran_f(v, 30, 20) + " " for v in vals))
+            self._text("mean_th.txt", head + lines)
+            # tkebudget_chan's 401 FORMAT(I3,' ',2(F20.9,' ')), J = 2..NY-1
+            lines = [fortran_i(j, 3) + " " + fortran_f(gyf[j], 20, 9) + " " + fortran_f(m["epsilon"][j], 20, 9) + " "
+                     for j in range(2, p.ny)]
+            self._text("tke.txt", [list_directed(step, t, dt)] + lines)
         return m

@@ -133,3 +133,60 @@ def test_running_mean_weights_single_precision(tmp_path):
         ubar = float(np.float32(1.0) / n32) * v + float((n32 - np.float32(1.0)) / n32) * ubar
     got = statsfile.read(str(tmp_path / "stats.h5"))["UBAR"]["data"][0]
     assert np.all(got == ubar) and ubar != 10.0 / 3.0
+
+
+class _TextRun(_OracleRun):
+    def __init__(self, o, t, step, dt):
+        super().__init__(o, t)
+        self.time_step, self.delta_t = step, dt
+
+
+def test_fortran_edit_descriptors():
+    assert statsfile.fortran_f(1.5, 30, 20) == "        1.50000000000000000000"
+    assert statsfile.fortran_f(-1e-30, 16, 9) == "    -0.000000000"
+    assert statsfile.fortran_f(1e20, 16, 9) == "*" * 16             # too wide: asterisks
+    assert statsfile.fortran_i(7, 3) == "  7" and statsfile.fortran_i(1000, 3) == "***"
+    # gfortran list-directed: I12, then 1PG25.17E3 after a blank
+    assert statsfile.list_directed(10, 0.01, 1e-3) == \
+        "          10   1.0000000000000000E-002   1.0000000000000000E-003"
+    assert statsfile.list_directed(0.5) == "  0.50000000000000000     "
+    assert statsfile.list_directed(1.5) == "   1.5000000000000000     "
+
+
+def test_text_files(tmp_path):
+    """mean.txt / mean_th.txt / tke.txt (appended per call) and stats.txt:
+    the reference's FORMAT statements and columns (save_stats.f:427-447,
+    639-658, 1191-1205, 68-89)."""
+    p, g, o, _, _ = modes_case()
+    w = statsfile.StatsWriter(str(tmp_path), formats=("txt",))
+    m1 = w.save(_TextRun(o, 0.0, 0, 0.01))
+    o.step(1)
+    m2 = w.save(_TextRun(o, 0.01, 1, 0.01))
+    w.save(_TextRun(o, 0.01, 1, 0.01), final=True)
+    assert not (tmp_path / "mean.h5").exists()
+    lines = (tmp_path / "mean.txt").read_text().splitlines()
+    ny = p.ny
+    assert len(lines) == 2 * (2 + ny)
+    step, t, dt = lines[2 + ny].split()
+    assert (int(step), float(t), float(dt)) == (1, 0.01, 0.01)
+    ub = statsfile.ubulk(p, g, m2["ume"])
+    assert float(lines[3 + ny]) == pytest.approx(ub, rel=1e-15, abs=1e-300)
+    row = lines[4 + ny + 4]                                   # J = 5 of the second sample
+    assert len(row) == 3 + 1 + 17 * 31 and row[:3] == "  5"
+    v = [float(x) for x in row.split()[1:]]
+    assert v[0] == pytest.approx(g.gyf[5], abs=1e-20)
+    assert v[1] == pytest.approx(m2["ume"][5], abs=1e-20)
+    assert v[2] == pytest.approx(0.5 * (m2["vme"][6] + m2["vme"][5]), abs=1e-20)
+    assert v[16] == pytest.approx(m2["omega_z"][5], abs=1e-20)   # the true omega_z here
+    th = (tmp_path / "mean_th.txt").read_text().splitlines()
+    assert len(th) == 2 * (2 + ny) and float(th[2 + 6].split()[5]) == pytest.approx(m1["thv01"][7], abs=1e-20)
+    tke = (tmp_path / "tke.txt").read_text().splitlines()
+    assert len(tke) == 2 * (1 + ny - 2)
+    j, y, eps = tke[1].split()
+    assert (int(j), float(eps)) == (2, pytest.approx(m1["epsilon"][2], abs=1e-9))
+    st = (tmp_path / "stats.txt").read_text().splitlines()
+    assert len(st) == 2 * ny and st[0].count(",") == 4
+    assert float(st[0].split(",")[2]) == pytest.approx(0.5 * (m1["ume"][1] + m2["ume"][1]), abs=1e-9)
+    # a new writer (a new run) starts the files afresh
+    statsfile.StatsWriter(str(tmp_path), formats=("txt",)).save(_TextRun(o, 0.02, 2, 0.01))
+    assert len((tmp_path / "mean.txt").read_text().splitlines()) == 2 + ny
