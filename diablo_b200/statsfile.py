@@ -42,7 +42,9 @@ _MEMBER = re.compile(r"^(?P<g>[^/]+)/(?P<n>\d{4,})(?P<a>@Time)?\.npy$")
 
 
 class StatFile:
-    """One mean.h5-style file, opened for appending."""
+    """One mean.h5-style file, opened for appending.  Every append rewrites
+    the archive's central directory, so a caller groups the datasets of one
+    SAVE_STATS call into one write_many."""
 
     def __init__(self, path: str):
         self.path = path
@@ -57,26 +59,31 @@ class StatFile:
     def samples(self, gname: str) -> int:
         return self._samples.get(gname, 0)
 
-    def _append(self, gname: str, value: np.ndarray, time: float | None) -> int:
-        n = self.samples(gname) + 1                       # NSAMP = NSAMP + 1; dname = '(I0.4)'
-        members = [(f"{gname}/{n:04d}.npy", np.ascontiguousarray(value, dtype="<f8"))]
-        if time is not None:
-            members.append((f"{gname}/{n:04d}@Time.npy", np.array(time, dtype="<f8")))
+    def write_many(self, entries) -> list[int]:
+        """Append datasets (gname, value, time or None) in one pass over the
+        archive: each gets the group's next number; returns them."""
+        members, numbers = [], []
+        for gname, value, time in entries:
+            n = self.samples(gname) + 1                   # NSAMP = NSAMP + 1; dname = '(I0.4)'
+            self._samples[gname] = n
+            numbers.append(n)
+            members.append((f"{gname}/{n:04d}.npy", np.ascontiguousarray(value, dtype="<f8")))
+            if time is not None:
+                members.append((f"{gname}/{n:04d}@Time.npy", np.array(time, dtype="<f8")))
         with zipfile.ZipFile(self.path, "a") as z:
             for name, a in members:
                 buf = io.BytesIO()
                 np.lib.format.write_array(buf, a, allow_pickle=False)
                 z.writestr(name, buf.getvalue())
-        self._samples[gname] = n
-        return n
+        return numbers
 
     def write_real(self, gname: str, value: float) -> int:
         """WriteHDF5_real (hdf5.f:1345-1464): one value, no attribute."""
-        return self._append(gname, np.array([value]), None)
+        return self.write_many([(gname, np.array([value]), None)])[0]
 
     def write_stat(self, gname: str, diag: np.ndarray, time: float) -> int:
         """WriteStatH5 (hdf5.f:1466-1622): Diag(1:NY) with its Time."""
-        return self._append(gname, np.asarray(diag, dtype=np.float64), time)
+        return self.write_many([(gname, np.asarray(diag, dtype=np.float64), time)])[0]
 
 
 def read(path: str) -> dict:
@@ -174,10 +181,9 @@ class StatsWriter:
         if final:
             zero = np.zeros(p.ny + 2)
             if "h5" in self.formats:
-                f = self._f("stats.h5")
-                f.write_stat("GYF", gyf[rows], t)
-                for name in ["UBAR", "VBAR", "WBAR"] + [f"THBAR{n + 1:02d}" for n in range(p.n_th)]:
-                    f.write_stat(name, self.bar.get(name, zero)[rows], t)
+                names = ["UBAR", "VBAR", "WBAR"] + [f"THBAR{n + 1:02d}" for n in range(p.n_th)]
+                self._f("stats.h5").write_many([("GYF", gyf[rows], t)] +
+                                               [(k, self.bar.get(k, zero)[rows], t) for k in names])
             if "txt" in self.formats:
                 # 201 FORMAT(I3,',',F16.9,',',F16.9,',',F16.9,',',F16.9), 202 for each scalar
                 ub, vb, wb = (self.bar.get(k, zero) for k in ("UBAR", "VBAR", "WBAR"))
@@ -205,19 +211,16 @@ class StatsWriter:
             new[rows] = w1 * v[rows] + w2 * old[rows]
             self.bar[name] = new
         if "h5" in self.formats:
-            mean = self._f("mean.h5")
-            mean.write_real("time", t)
-            mean.write_stat("gyf", gyf[rows], t)
+            entries = [("time", np.array([t]), None), ("gyf", gyf[rows], t)]
             for name in MEAN_NAMES:
                 v = m["omega_y"] if (name == "omega_z" and self.omega_z_quirk) else m[name]
-                mean.write_stat(name, v[rows], t)
+                entries.append((name, v[rows], t))
             for n in range(p.n_th):
                 for name in SCAL_NAMES:
-                    mean.write_stat(f"{name}{n + 1:02d}", m[f"{name}{n + 1:02d}"][rows], t)
-            tke = self._f("tke.h5")
-            tke.write_real("time", t)
-            tke.write_stat("gyf", gyf[rows], t)
-            tke.write_stat("epsilon", m["epsilon"][rows], t)
+                    entries.append((f"{name}{n + 1:02d}", m[f"{name}{n + 1:02d}"][rows], t))
+            self._f("mean.h5").write_many(entries)
+            self._f("tke.h5").write_many([("time", np.array([t]), None), ("gyf", gyf[rows], t),
+                                          ("epsilon", m["epsilon"][rows], t)])
         if "txt" in self.formats:
             step, dt = int(c.time_step), float(c.delta_t)
             ub = ubulk(p, c.grid, m["ume"])
