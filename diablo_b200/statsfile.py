@@ -19,8 +19,9 @@ does the same, and ``False`` writes the true omega_z.
 
 ``formats`` may add ``"txt"``: the files the reference writes when it is
 built without HDF5 (save_stats.f:68-89, 427-447, 639-658, 1191-1205) --
-mean.txt, mean_th.txt and tke.txt, which a run appends to (the reference
-never closes their units), and stats.txt on the final call.  Their rows use
+mean.txt, mean_th.txt, tke.txt and, with LES, tke_les.txt, which a run
+appends to (the reference never closes their units), and stats.txt on the
+final call.  With LES, tke.h5 also gets tkebudget_chan_les's epsilon_sgs.  Their rows use
 the reference's FORMAT statements and are reproduced byte for byte (F
 editing rounds like Python's fixed-point formatting; a value too wide for
 its field prints as asterisks); the list-directed header lines (TIME_STEP,
@@ -148,6 +149,49 @@ def ubulk(p, grid, ume: np.ndarray) -> float:
     return res / p.ly
 
 
+def epsilon_sgs(p, grid, u1: np.ndarray, u2: np.ndarray, u3: np.ndarray, nu_t: np.ndarray) -> np.ndarray:
+    """tkebudget_chan_les (save_stats.f:859-900) on physical [J][K][I] fields
+    (planes 0..NY+1): per plane J = 1..NY, the sum over the plane of U_i
+    times the implicit vertical eddy-viscosity term of U_i (U1, U3 at GYF,
+    U2 at GY, NU_T at GY).  Plane sums, not means, as the reference writes."""
+    dy = np.asarray(grid.dy, dtype=np.float64)[:, None, None]
+    dyf = np.asarray(grid.dyf, dtype=np.float64)[:, None, None]
+    c, n, m = slice(1, p.ny + 1), slice(2, p.ny + 2), slice(0, p.ny)
+    nt = nu_t
+
+    def gyf_term(u):
+        return u[c] * ((nt[n] * (u[n] - u[c]) / dy[n] - nt[c] * (u[c] - u[m]) / dy[c]) / dyf[c])
+
+    def flux(coef, du, h):
+        # a zero eddy viscosity carries no flux: at J = 1 the reference
+        # divides 0 by DYF(0), which it never sets (0), and gets NaN
+        with np.errstate(divide="ignore", invalid="ignore"):
+            return np.where(coef == 0.0, 0.0, coef * du / h)
+
+    t = gyf_term(u1) + gyf_term(u3) + u2[c] * (
+        (flux(0.5 * (nt[c] + nt[n]), u2[n] - u2[c], dyf[c]) - flux(0.5 * (nt[c] + nt[m]), u2[c] - u2[m], dyf[m]))
+        / dy[c])
+    out = np.zeros(p.ny + 2)
+    out[1 : p.ny + 1] = t.sum(axis=(1, 2))
+    return out
+
+
+def _physical(c, cu: np.ndarray) -> np.ndarray:
+    from .layout import new_physical
+    p = c.p
+    v = new_physical(p)
+    c.fft_xz_to_physical(np.ascontiguousarray(cu).copy(), v, 0, p.ny + 1)
+    return v[:, : p.nz, : p.nx]
+
+
+def les_epsilon_sgs(c) -> np.ndarray:
+    """epsilon_sgs of an LES instance's current state (after the APPLY_BC_VEL
+    of the statistics) and its NU_T."""
+    s = c.download()
+    u = [_physical(c, s["cu"][k]) for k in range(3)]
+    return epsilon_sgs(c.p, c.grid, *u, c.download_nu_t())
+
+
 class StatsWriter:
     """The output side of SAVE_STATS_CHAN for one channel run: mean.h5 and
     tke.h5 on every call, the running means UBAR, VBAR, WBAR, THBARnn
@@ -197,6 +241,8 @@ class StatsWriter:
                     f.write("".join(line + "\n" for line in lines))
             return None
         m = c.mean_stats()
+        if p.les:                     # tkebudget_chan_les (save_stats.f:170, 859-935)
+            m["epsilon_sgs"] = les_epsilon_sgs(c)
         # running means with REAL*4 weights: (1./FLOAT(N)) and ((FLOAT(N)-1.)/FLOAT(N))
         self.nsamples += 1
         n32 = np.float32(self.nsamples)
@@ -219,8 +265,10 @@ class StatsWriter:
                 for name in SCAL_NAMES:
                     entries.append((f"{name}{n + 1:02d}", m[f"{name}{n + 1:02d}"][rows], t))
             self._f("mean.h5").write_many(entries)
-            self._f("tke.h5").write_many([("time", np.array([t]), None), ("gyf", gyf[rows], t),
-                                          ("epsilon", m["epsilon"][rows], t)])
+            tke = [("time", np.array([t]), None), ("gyf", gyf[rows], t), ("epsilon", m["epsilon"][rows], t)]
+            if p.les:
+                tke.append(("epsilon_sgs", m["epsilon_sgs"][rows], t))
+            self._f("tke.h5").write_many(tke)
         if "txt" in self.formats:
             step, dt = int(c.time_step), float(c.delta_t)
             ub = ubulk(p, c.grid, m["ume"])
@@ -244,4 +292,8 @@ class StatsWriter:
             lines = [fortran_i(j, 3) + " " + fortran_f(gyf[j], 20, 9) + " " + fortran_f(m["epsilon"][j], 20, 9) + " "
                      for j in range(2, p.ny)]
             self._text("tke.txt", [list_directed(step, t, dt)] + lines)
+            if p.les:                 # 460 FORMAT(I3,' ',2(F30.20,' ')), J = 1..NY
+                lines = [fortran_i(j, 3) + " " + fortran_f(gyf[j], 30, 20) + " " +
+                         fortran_f(m["epsilon_sgs"][j], 30, 20) + " " for j in range(1, p.ny + 1)]
+                self._text("tke_les.txt", [list_directed(step, t, dt)] + lines)
         return m

@@ -2121,6 +2121,49 @@ void orc_mean_stats(orc_state* s, double* chan, double* scal, double* eps) {
 /* keeps its horizontally filtered value: the reference copies an element of  */
 /* VEC_C that it never sets there.                                            */
 /* ------------------------------------------------------------------------ */
+/* tkebudget_chan_les (save_stats.f:859-900): the plane sums, J = 1..NY, of
+ * U_i times the implicit vertical eddy-viscosity term of U_i, on the
+ * physical velocity after APPLY_BC_VEL (orc_stats applies it) and NU_T of
+ * the last LES substage.  out: NY+2 values, rows 1..NY.  Row 1 is finite
+ * where the reference's is NaN (FLUX below). */
+/* a zero eddy viscosity carries no flux: at J = 1 the reference divides 0 by
+ * DYF(0), which it never sets (0), and gets NaN */
+#define FLUX(coef, du, h) ((coef) == 0.0 ? 0.0 : (coef) * (du) / (h))
+void orc_epsilon_sgs(orc_state* s, double* out) {
+    const int NY = s->NY, NZP = s->NZP, NXM = s->NXM;
+    memset(out, 0, sizeof(double) * (NY + 2));
+    if (!s->p.les) return;
+    double* base = (double*)malloc(sizeof(double) * DIABLO_NSTATS * (NY + 2));
+    orc_stats(s, base);                         /* APPLY_BC_VEL on the state */
+    free(base);
+    double* u[3];
+    for (int c = 0; c < 3; ++c) {
+        u[c] = (double*)malloc(sizeof(double) * s->nreal);
+        memcpy(u[c], c == 0 ? s->U1 : c == 1 ? s->U2 : s->U3, sizeof(double) * s->nreal);
+        orc_fft_xz_to_physical(s, u[c], u[c], 0, NY + 1);
+    }
+    const double *U1 = u[0], *U2 = u[1], *U3 = u[2], *NT = s->NU_T, *DY = s->DY, *DYF = s->DYF;
+    for (int j = 1; j <= NY; ++j) {
+        double e = 0.0;
+        for (int i = 0; i <= NXM; ++i)
+            for (int k = 0; k <= NZP - 1; ++k) {
+                const double t =
+                    PH(U1, i, k, j) * ((PH(NT, i, k, j + 1) * (PH(U1, i, k, j + 1) - PH(U1, i, k, j)) / DY[j + 1] -
+                                        PH(NT, i, k, j) * (PH(U1, i, k, j) - PH(U1, i, k, j - 1)) / DY[j]) / DYF[j]) +
+                    PH(U3, i, k, j) * ((PH(NT, i, k, j + 1) * (PH(U3, i, k, j + 1) - PH(U3, i, k, j)) / DY[j + 1] -
+                                        PH(NT, i, k, j) * (PH(U3, i, k, j) - PH(U3, i, k, j - 1)) / DY[j]) / DYF[j]) +
+                    PH(U2, i, k, j) * ((FLUX(0.5 * (PH(NT, i, k, j) + PH(NT, i, k, j + 1)),
+                                             PH(U2, i, k, j + 1) - PH(U2, i, k, j), DYF[j]) -
+                                        FLUX(0.5 * (PH(NT, i, k, j) + PH(NT, i, k, j - 1)),
+                                             PH(U2, i, k, j) - PH(U2, i, k, j - 1), DYF[j - 1])) / DY[j]);
+                e += t;
+            }
+        out[j] = e;
+    }
+    for (int c = 0; c < 3; ++c) free(u[c]);
+}
+#undef FLUX
+
 void orc_set_user_rhs(orc_state* s, int kind, void (*fn)(void*), void* user) {
     if (kind < 0 || kind > 1) return;
     s->user_fn[kind] = fn;

@@ -82,6 +82,8 @@ void orc_mean_stats(orc_state* s, double* chan, double* scal, double* eps);
  * (kind 1, channel.f:578): fn(user) runs at that point of orc_rk_chan_1 and
  * may change CF1..CF3, CFTH through orc_array; NULL removes it. */
 void orc_set_user_rhs(orc_state* s, int kind, void (*fn)(void*), void* user);
+/* tkebudget_chan_les's epsilon_sgs (plane sums, NY+2 values, rows 1..NY). */
+void orc_epsilon_sgs(orc_state* s, double* out);
 /* Parameters of the learned closure (LES_MODEL_TYPE 4), in the layout of the
  * GPU library's diablo_mlp_set_params; NULL removes it. */
 void orc_set_mlp(orc_state* s, const float* params);

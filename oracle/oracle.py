@@ -64,6 +64,7 @@ def lib() -> ctypes.CDLL:
         L.orc_stats.argtypes = [vp, dp]
         L.orc_mean_stats.argtypes = [vp, dp, dp, dp]
         L.orc_set_user_rhs.argtypes = [vp, ip, USER_FN, vp]
+        L.orc_epsilon_sgs.argtypes = [vp, dp]
         L.orc_set_mlp.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
         L.orc_cdft.restype = ip
         L.orc_cdft.argtypes = [ip, dp, ip]
@@ -196,6 +197,12 @@ class Oracle:
 
     def filter_chan(self, n: int = 1) -> None:
         lib().orc_filter_chan(self._h, n)
+
+    def epsilon_sgs(self) -> np.ndarray:
+        """tkebudget_chan_les's epsilon_sgs (plane sums, rows 1..NY)."""
+        out = np.zeros(self.p.ny + 2)
+        lib().orc_epsilon_sgs(self._h, _dptr(out))
+        return out
 
     def set_user_rhs(self, kind: int, fn) -> None:
         """USER_RHS_CHAN_FOURIER (kind 0) / _PHYSICAL (kind 1): fn(oracle)

@@ -190,3 +190,39 @@ def test_text_files(tmp_path):
     # a new writer (a new run) starts the files afresh
     statsfile.StatsWriter(str(tmp_path), formats=("txt",)).save(_TextRun(o, 0.02, 2, 0.01))
     assert len((tmp_path / "mean.txt").read_text().splitlines()) == 2 + ny
+
+
+class _LesRun(_TextRun):
+    """An LES oracle seen through the Channel calls the writer makes."""
+
+    def download(self):
+        return {"cu": self.o.cu}
+
+    def fft_xz_to_physical(self, vv, v, jmin, jmax):
+        self.o.fft_xz_to_physical(vv, v, jmin, jmax)
+
+    def download_nu_t(self):
+        return self.o.nu_t
+
+
+def test_epsilon_sgs_matches_oracle(tmp_path):
+    """tkebudget_chan_les (save_stats.f:859-935): the writer's numpy form on
+    the state's physical fields and NU_T against the oracle's restatement,
+    and its tke.h5 group and tke_les.txt rows."""
+    from test_gpu_les import les_channel
+    p, g, u, th = les_channel(24, 33, 16)
+    o = Oracle(p, g, 1e-3)
+    o.init_from_physical(u, th)
+    o.step(2)
+    assert np.abs(o.nu_t).max() > 0
+    w = statsfile.StatsWriter(str(tmp_path), formats=("h5", "txt"))
+    m = w.save(_LesRun(o, 0.002, 2, 1e-3))
+    ref = o.epsilon_sgs()
+    rows = slice(1, p.ny + 1)
+    assert np.abs(ref[rows]).max() > 0
+    assert np.allclose(m["epsilon_sgs"][rows], ref[rows], rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+    tke = statsfile.read(str(tmp_path / "tke.h5"))
+    assert np.array_equal(tke["epsilon_sgs"]["data"][0], m["epsilon_sgs"][rows])
+    lines = (tmp_path / "tke_les.txt").read_text().splitlines()
+    assert len(lines) == 1 + p.ny and len(lines[1]) == 3 + 1 + 2 * 31
+    assert float(lines[3].split()[2]) == pytest.approx(m["epsilon_sgs"][3], abs=1e-20)
