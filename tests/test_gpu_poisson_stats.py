@@ -145,3 +145,25 @@ def test_mean_stats_match_oracle(case):
         assert np.abs(ref["omega_z"]).max() > 0 and np.abs(ref["epsilon"]).max() > 0
         if p.n_th > 1:
             assert np.abs(ref["pe_diss02"]).max() > 0 and not np.allclose(ref["thrms02"], ref["thrms01"])
+
+
+def test_les_epsilon_sgs_matches_oracle(tmp_path):
+    """tkebudget_chan_les through the statistics writer on an LES instance
+    (NU_T and the state from the device) against the oracle."""
+    from diablo_b200 import statsfile
+    from test_gpu_les import les_channel
+    p, g, u, th = les_channel(32, 33, 24)
+    o = Oracle(p, g, 1e-3)
+    o.init_from_physical(u, th)
+    with Channel(p, g, 1e-3) as c:
+        c.upload([x.copy() for x in o.cu], o.cp.copy(), o.cth.copy())
+        for _ in range(2):
+            o.step()
+            c.step()
+        m = statsfile.StatsWriter(str(tmp_path)).save(c)
+        ref = o.epsilon_sgs()
+        rows = slice(1, p.ny + 1)
+        scale = np.abs(ref[rows]).max()
+        assert scale > 0
+        assert np.abs(m["epsilon_sgs"][rows] - ref[rows]).max() <= 1e-8 * scale
+        assert statsfile.read(str(tmp_path / "tke.h5"))["epsilon_sgs"]["SAMPLES"] == 1
