@@ -76,3 +76,27 @@ def test_params_struct_matches_header_field_order():
         if m:
             names += [n.strip().split("[")[0] for n in m.group(2).split(",")]
     assert names == [f for f, _ in P.DiabloParams._fields_]
+
+
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """sizeof and field offsets of diablo_params and diablo_user_rhs_args as
+    gcc lays them out, against the ctypes mirrors."""
+    import subprocess
+    from diablo_b200.channel import UserRhsArgs
+    structs = {"diablo_params": P.DiabloParams, "diablo_user_rhs_args": UserRhsArgs}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "diablo_gpu.h"', "int main(void) {"]
+    for cname, ct in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in ct._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, ct in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(ct), cname
+        for f, _ in ct._fields_:
+            assert got[(cname, f)] == getattr(ct, f).offset, (cname, f)
