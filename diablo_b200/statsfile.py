@@ -192,15 +192,67 @@ def les_epsilon_sgs(c) -> np.ndarray:
     return epsilon_sgs(c.p, c.grid, *u, c.download_nu_t())
 
 
+def movie_indices(p, grid, xc: float, yc: float, zc: float) -> tuple:
+    """INIT_CHAN_MOVIE (channel.f:1516-1560) for one process: NxMovie,
+    NyMovie, NzMovie from the slice centres of MOVIE.dat.  NyMovie is the
+    GYF interval holding yc when GYF(JSTART) <= yc < GYF(JEND+1) (JSTART = 2,
+    JEND = NY-1); otherwise no process holds the x-z slice (RankYMovie = -1)
+    and it is None, as is NzMovie when it falls outside 0..NZ-1 (no process
+    holds the x-y slice).  An NxMovie outside 0..NX-1 is an error here; the
+    reference would index outside its arrays."""
+    gyf = np.asarray(grid.gyf, dtype=np.float64)
+    nx_m = int(xc * p.nx / p.lx)
+    nz_m = int(zc * p.nz / p.lz)
+    if not 0 <= nx_m < p.nx:
+        raise ValueError(f"XcMovie {xc} gives NxMovie {nx_m} outside 0..{p.nx - 1}")
+    ny_m = None
+    if gyf[2] <= yc < gyf[p.ny]:
+        i = 1
+        while not (gyf[i] <= yc < gyf[i + 1]):
+            i += 1
+        ny_m = i
+    return nx_m, ny_m, (nz_m if 0 <= nz_m < p.nz else None)
+
+
+def movie_planes(p, u1, u2, u3, th, nu_t, idx) -> list:
+    """The movie.h5 slices of SAVE_STATS_CHAN (save_stats.f:538-580, 677-839)
+    from physical [J][K][I] fields: (group, 2-D array) in the byte order of
+    WriteHDF5_XYPLANE / _XZPLANE / _ZYPLANE (Fortran (NX,NY), (NX,NZ), (NZ,NY)
+    arrays, i.e. C-order (NY,NX), (NZ,NX), (NY,NZ)).  V is averaged to GYF;
+    NU_T planes only with LES."""
+    nxm, nym, nzm = idx
+    rows = slice(1, p.ny + 1)
+    vg = 0.5 * (u2[1 : p.ny + 1] + u2[2 : p.ny + 2])             # V at GYF, J = 1..NY
+    out = []
+    for n in range(p.n_th):
+        f = th[n]
+        if nzm is not None:
+            out.append((f"th{n + 1:02d}_xy", f[rows, nzm, :]))
+        if nym is not None:
+            out.append((f"th{n + 1:02d}_xz", f[nym, :, :]))
+        out.append((f"th{n + 1:02d}_zy", f[rows, :, nxm]))
+    fields = [("u", u1[rows], u1), ("v", vg, None), ("w", u3[rows], u3)]
+    if p.les:
+        fields.append(("nu_t", nu_t[rows], nu_t))
+    if nzm is not None:
+        out += [(f"{name}_xy", vol[:, nzm, :]) for name, vol, _ in fields]
+    if nym is not None:
+        out += [(f"{name}_xz", 0.5 * (u2[nym] + u2[nym + 1]) if full is None else full[nym])
+                for name, _, full in fields]
+    out += [(f"{name}_zy", vol[:, :, nxm]) for name, vol, _ in fields]
+    return [(g, np.ascontiguousarray(a, dtype=np.float64)) for g, a in out]
+
+
 class StatsWriter:
     """The output side of SAVE_STATS_CHAN for one channel run: mean.h5 and
     tke.h5 on every call, the running means UBAR, VBAR, WBAR, THBARnn
     (save_stats.f:104-123) and stats.h5 on the final call."""
 
-    def __init__(self, directory: str, omega_z_quirk: bool = True, formats=("h5",)):
+    def __init__(self, directory: str, omega_z_quirk: bool = True, formats=("h5",), movie=None):
         self.dir = directory
         self.omega_z_quirk = omega_z_quirk
         self.formats = tuple(formats)
+        self.movie = movie            # MOVIE.dat's (XcMovie, YcMovie, ZcMovie), or None
         self.nsamples = 0
         self.bar: dict[str, np.ndarray] = {}
         self._opened: set[str] = set()
@@ -243,6 +295,13 @@ class StatsWriter:
         m = c.mean_stats()
         if p.les:                     # tkebudget_chan_les (save_stats.f:170, 859-935)
             m["epsilon_sgs"] = les_epsilon_sgs(c)
+        if self.movie is not None and "h5" in self.formats:
+            st = c.download()        # the state after the statistics' APPLY_BC_VEL
+            u = [_physical(c, st["cu"][k]) for k in range(3)]
+            th = [_physical(c, st["cth"][n]) for n in range(p.n_th)]
+            nt = c.download_nu_t() if p.les else None
+            idx = movie_indices(p, c.grid, *self.movie)
+            self._f("movie.h5").write_many([(g, a, t) for g, a in movie_planes(p, *u, th, nt, idx)])
         # running means with REAL*4 weights: (1./FLOAT(N)) and ((FLOAT(N)-1.)/FLOAT(N))
         self.nsamples += 1
         n32 = np.float32(self.nsamples)

@@ -196,7 +196,7 @@ class _LesRun(_TextRun):
     """An LES oracle seen through the Channel calls the writer makes."""
 
     def download(self):
-        return {"cu": self.o.cu}
+        return {"cu": self.o.cu, "cth": self.o.cth}
 
     def fft_xz_to_physical(self, vv, v, jmin, jmax):
         self.o.fft_xz_to_physical(vv, v, jmin, jmax)
@@ -215,8 +215,13 @@ def test_epsilon_sgs_matches_oracle(tmp_path):
     o.init_from_physical(u, th)
     o.step(2)
     assert np.abs(o.nu_t).max() > 0
-    w = statsfile.StatsWriter(str(tmp_path), formats=("h5", "txt"))
+    centres = (0.5 * p.lx, float(g.gyf[p.ny // 2]), 0.25 * p.lz)
+    w = statsfile.StatsWriter(str(tmp_path), formats=("h5", "txt"), movie=centres)
     m = w.save(_LesRun(o, 0.002, 2, 1e-3))
+    nx_m, ny_m, nz_m = statsfile.movie_indices(p, g, *centres)
+    mv = statsfile.read(str(tmp_path / "movie.h5"))
+    assert np.array_equal(mv["nu_t_xy"]["data"][0], o.nu_t[1 : p.ny + 1, nz_m, :])
+    assert np.array_equal(mv["nu_t_xz"]["data"][0], o.nu_t[ny_m])
     ref = o.epsilon_sgs()
     rows = slice(1, p.ny + 1)
     assert np.abs(ref[rows]).max() > 0
@@ -226,3 +231,33 @@ def test_epsilon_sgs_matches_oracle(tmp_path):
     lines = (tmp_path / "tke_les.txt").read_text().splitlines()
     assert len(lines) == 1 + p.ny and len(lines[1]) == 3 + 1 + 2 * 31
     assert float(lines[3].split()[2]) == pytest.approx(m["epsilon_sgs"][3], abs=1e-20)
+
+
+def test_movie_planes(tmp_path):
+    """movie.h5 slices (save_stats.f:538-580, 677-839; INIT_CHAN_MOVIE,
+    channel.f:1516-1560) against the oracle's physical fields."""
+    from test_checkpoint import oracle_physical
+    p, g, o, _, _ = modes_case()
+    xc, yc, zc = 0.3 * p.lx, float(g.gyf[10]) + 1e-9, 0.55 * p.lz
+    nx_m, ny_m, nz_m = statsfile.movie_indices(p, g, xc, yc, zc)
+    assert (nx_m, ny_m, nz_m) == (int(0.3 * p.nx), 10, int(0.55 * p.nz))
+    w = statsfile.StatsWriter(str(tmp_path), movie=(xc, yc, zc))
+    w.save(_LesRun(o, 0.0, 0, 0.01))
+    o.step(1)
+    w.save(_LesRun(o, 0.01, 1, 0.01))
+    mv = statsfile.read(str(tmp_path / "movie.h5"))
+    names = [f"{q}_{s}" for q in ("u", "v", "w", "th01") for s in ("xy", "xz", "zy")]
+    assert sorted(mv) == sorted(names) and all(mv[k]["SAMPLES"] == 2 for k in names)
+    u1, u2 = oracle_physical(o, o.cu[0]), oracle_physical(o, o.cu[1])
+    th = oracle_physical(o, o.cth[0])
+    rows = slice(1, p.ny + 1)
+    assert mv["u_xy"]["data"][1].shape == (p.ny, p.nx) and np.array_equal(mv["u_xy"]["data"][1], u1[rows, nz_m, :])
+    assert mv["th01_xz"]["data"][1].shape == (p.nz, p.nx) and np.array_equal(mv["th01_xz"]["data"][1], th[ny_m])
+    assert mv["u_zy"]["data"][1].shape == (p.ny, p.nz) and np.array_equal(mv["u_zy"]["data"][1], u1[rows, :, nx_m])
+    assert np.array_equal(mv["v_xz"]["data"][1], 0.5 * (u2[ny_m] + u2[ny_m + 1]))
+    assert list(mv["v_xy"]["Time"]) == [0.0, 0.01]
+    # outside the walls' GYF range no process holds the x-z slice; beyond LZ, the x-y one
+    assert statsfile.movie_indices(p, g, xc, float(g.gyf[p.ny]) + 1.0, zc)[1] is None
+    assert statsfile.movie_indices(p, g, xc, yc, 1.5 * p.lz)[2] is None
+    with pytest.raises(ValueError):
+        statsfile.movie_indices(p, g, 2.0 * p.lx, yc, zc)
