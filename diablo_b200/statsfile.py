@@ -184,6 +184,54 @@ def _physical(c, cu: np.ndarray) -> np.ndarray:
     return v[:, : p.nz, : p.nx]
 
 
+def epsilon_field(c) -> np.ndarray:
+    """tkebudget_chan's 3-D dissipation field F1 (save_stats.f:957-1131) of an
+    instance's current state (after the statistics' APPLY_BC_VEL): NU times
+    du/dx, dv/dx, du/dy, dw/dx, du/dz, dv/dy, dw/dy, dv/dz, dw/dz squared, the
+    x and z derivatives of U1 and U3 interpolated from GYF to GY, the y
+    derivatives with the mean removed; rows 2..NY-1 of [J][K][I] (rows 1 and
+    NY read rows of S1 that earlier code left behind in the reference: 0
+    here).  The x and z derivatives go to physical space through the
+    instance's own transforms."""
+    from .layout import new_fourier
+    p = c.p
+    s = c.download()
+    cu = s["cu"]
+    nkx, nkz, tnkz = p.nx // 3, p.nz // 3, 2 * (p.nz // 3)
+    kx = np.zeros(p.nx // 2 + 1)
+    kx[: nkx + 1] = np.arange(nkx + 1) * 2.0 * np.pi / p.lx
+    kk = np.arange(tnkz + 1)
+    kz = np.zeros(p.nz + 2)
+    kz[: tnkz + 1] = np.where(kk <= nkz, kk, kk - tnkz - 1) * 2.0 * np.pi / p.lz
+
+    def deriv(f, along):                     # ikx or ikz of CU on rows 1..NY, to physical space
+        a = new_fourier(p)
+        k = kx[None, None, :] if along == "x" else kz[None, :, None]
+        a[1 : p.ny + 1] = 1j * k * f[1 : p.ny + 1]
+        return _physical(c, a)
+
+    u1, u2, u3 = (_physical(c, f) for f in cu)
+    ume, vme, wme = (f[:, 0, 0].real for f in cu)
+    dy = np.asarray(c.grid.dy, dtype=np.float64)[:, None, None]
+    dyf = np.asarray(c.grid.dyf, dtype=np.float64)[:, None, None]
+    gy = np.asarray(c.grid.gy, dtype=np.float64)
+    j, jm = slice(2, p.ny), slice(1, p.ny - 1)
+
+    def interp(sq):                          # (DYF(j-1) S(j)^2 + DYF(j) S(j-1)^2) / (2 DY(j))
+        return (dyf[jm] * sq[j] ** 2 + dyf[j] * sq[jm] ** 2) / (2.0 * dy[j])
+
+    e = interp(deriv(cu[0], "x")) + deriv(cu[1], "x")[j] ** 2
+    e = e + (((u1[j] - ume[j, None, None]) - (u1[jm] - ume[jm, None, None])) / dy[j]) ** 2
+    e = e + interp(deriv(cu[2], "x")) + interp(deriv(cu[0], "z"))
+    e = e + (((u2[3 : p.ny + 1] - vme[j, None, None]) - (u2[jm] - vme[jm, None, None]))
+             / (gy[3 : p.ny + 1] - gy[1 : p.ny - 1])[:, None, None]) ** 2
+    e = e + (((u3[j] - wme[j, None, None]) - (u3[jm] - wme[jm, None, None])) / dy[j]) ** 2
+    e = e + deriv(cu[1], "z")[j] ** 2 + interp(deriv(cu[2], "z"))
+    out = np.zeros((p.ny + 2, p.nz, p.nx))
+    out[j] = p.nu * e
+    return out
+
+
 def les_epsilon_sgs(c) -> np.ndarray:
     """epsilon_sgs of an LES instance's current state (after the APPLY_BC_VEL
     of the statistics) and its NU_T."""
@@ -214,12 +262,13 @@ def movie_indices(p, grid, xc: float, yc: float, zc: float) -> tuple:
     return nx_m, ny_m, (nz_m if 0 <= nz_m < p.nz else None)
 
 
-def movie_planes(p, u1, u2, u3, th, nu_t, idx) -> list:
+def movie_planes(p, u1, u2, u3, th, nu_t, idx, eps=None) -> list:
     """The movie.h5 slices of SAVE_STATS_CHAN (save_stats.f:538-580, 677-839)
     from physical [J][K][I] fields: (group, 2-D array) in the byte order of
     WriteHDF5_XYPLANE / _XZPLANE / _ZYPLANE (Fortran (NX,NY), (NX,NZ), (NZ,NY)
     arrays, i.e. C-order (NY,NX), (NZ,NX), (NY,NZ)).  V is averaged to GYF;
-    NU_T planes only with LES."""
+    NU_T planes only with LES; eps, tkebudget_chan's F1, adds the epsilon
+    slices (save_stats.f:1151-1189)."""
     nxm, nym, nzm = idx
     rows = slice(1, p.ny + 1)
     vg = 0.5 * (u2[1 : p.ny + 1] + u2[2 : p.ny + 2])             # V at GYF, J = 1..NY
@@ -240,6 +289,12 @@ def movie_planes(p, u1, u2, u3, th, nu_t, idx) -> list:
         out += [(f"{name}_xz", 0.5 * (u2[nym] + u2[nym + 1]) if full is None else full[nym])
                 for name, _, full in fields]
     out += [(f"{name}_zy", vol[:, :, nxm]) for name, vol, _ in fields]
+    if eps is not None:
+        if nzm is not None:
+            out.append(("epsilon_xy", eps[rows, nzm, :]))
+        if nym is not None:
+            out.append(("epsilon_xz", eps[nym]))
+        out.append(("epsilon_zy", eps[rows, :, nxm]))
     return [(g, np.ascontiguousarray(a, dtype=np.float64)) for g, a in out]
 
 
@@ -301,7 +356,8 @@ class StatsWriter:
             th = [_physical(c, st["cth"][n]) for n in range(p.n_th)]
             nt = c.download_nu_t() if p.les else None
             idx = movie_indices(p, c.grid, *self.movie)
-            self._f("movie.h5").write_many([(g, a, t) for g, a in movie_planes(p, *u, th, nt, idx)])
+            eps = epsilon_field(c)
+            self._f("movie.h5").write_many([(g, a, t) for g, a in movie_planes(p, *u, th, nt, idx, eps)])
         # running means with REAL*4 weights: (1./FLOAT(N)) and ((FLOAT(N)-1.)/FLOAT(N))
         self.nsamples += 1
         n32 = np.float32(self.nsamples)

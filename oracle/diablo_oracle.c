@@ -2126,6 +2126,57 @@ void orc_mean_stats(orc_state* s, double* chan, double* scal, double* eps) {
  * physical velocity after APPLY_BC_VEL (orc_stats applies it) and NU_T of
  * the last LES substage.  out: NY+2 values, rows 1..NY.  Row 1 is finite
  * where the reference's is NaN (FLUX below). */
+/* tkebudget_chan's 3-D dissipation field F1 (save_stats.f:957-1131): NU times
+ * the nine squared gradient terms at each point, GYF quantities
+ * interpolated to GY, on rows 2..NY-1 (0 elsewhere: rows 1 and NY read rows
+ * of S1 that earlier code left behind).  F1 in the physical layout. */
+void orc_epsilon_field(orc_state* s, double* F1) {
+    const int NY = s->NY, NZP = s->NZP, NXM = s->NXM;
+    memset(F1, 0, sizeof(double) * s->nreal);
+    double* base = (double*)malloc(sizeof(double) * DIABLO_NSTATS * (NY + 2));
+    orc_stats(s, base);                         /* APPLY_BC_VEL on the state */
+    const double* ume = base + DIABLO_STAT_UME * (NY + 2);
+    const double* vme = base + DIABLO_STAT_VME * (NY + 2);
+    const double* wme = base + DIABLO_STAT_WME * (NY + 2);
+    double* u[3];
+    for (int c = 0; c < 3; ++c) {
+        u[c] = (double*)malloc(sizeof(double) * s->nreal);
+        memcpy(u[c], c == 0 ? s->U1 : c == 1 ? s->U2 : s->U3, sizeof(double) * s->nreal);
+        orc_fft_xz_to_physical(s, u[c], u[c], 0, NY + 1);
+    }
+    double* S1 = (double*)malloc(sizeof(double) * s->nreal);
+    const int order[9] = {3, 4, -1, 5, 6, -2, -3, 7, 8};   /* tkebudget_chan's order of terms */
+    for (int t = 0; t < 9; ++t) {
+        const int kind = order[t];
+        if (kind >= 0) stats_field(s, kind, NULL, S1);
+        const int interp = kind == 3 || kind == 5 || kind == 6 || kind == 8;
+        for (int j = 2; j <= NY - 1; ++j)
+            for (int k = 0; k <= NZP - 1; ++k)
+                for (int i = 0; i <= NXM; ++i) {
+                    double v;
+                    if (kind >= 0 && interp)
+                        v = (s->DYF[j - 1] * pow(PH(S1, i, k, j), 2.0) + s->DYF[j] * pow(PH(S1, i, k, j - 1), 2.0)) /
+                            (2.0 * s->DY[j]);
+                    else if (kind >= 0)
+                        v = pow(PH(S1, i, k, j), 2.0);
+                    else if (kind == -1)
+                        v = pow(((PH(u[0], i, k, j) - ume[j]) - (PH(u[0], i, k, j - 1) - ume[j - 1])) / s->DY[j], 2.0);
+                    else if (kind == -2)
+                        v = pow(((PH(u[1], i, k, j + 1) - vme[j]) - (PH(u[1], i, k, j - 1) - vme[j - 1])) /
+                                    (s->GY[j + 1] - s->GY[j - 1]), 2.0);
+                    else
+                        v = pow(((PH(u[2], i, k, j) - wme[j]) - (PH(u[2], i, k, j - 1) - wme[j - 1])) / s->DY[j], 2.0);
+                    PH(F1, i, k, j) += v;
+                }
+    }
+    for (int j = 2; j <= NY - 1; ++j)
+        for (int k = 0; k <= NZP - 1; ++k)
+            for (int i = 0; i <= NXM; ++i) PH(F1, i, k, j) *= s->p.nu;
+    for (int c = 0; c < 3; ++c) free(u[c]);
+    free(S1);
+    free(base);
+}
+
 /* a zero eddy viscosity carries no flux: at J = 1 the reference divides 0 by
  * DYF(0), which it never sets (0), and gets NaN */
 #define FLUX(coef, du, h) ((coef) == 0.0 ? 0.0 : (coef) * (du) / (h))

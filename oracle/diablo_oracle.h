@@ -84,6 +84,8 @@ void orc_mean_stats(orc_state* s, double* chan, double* scal, double* eps);
 void orc_set_user_rhs(orc_state* s, int kind, void (*fn)(void*), void* user);
 /* tkebudget_chan_les's epsilon_sgs (plane sums, NY+2 values, rows 1..NY). */
 void orc_epsilon_sgs(orc_state* s, double* out);
+/* tkebudget_chan's 3-D dissipation field F1 (rows 2..NY-1), physical layout. */
+void orc_epsilon_field(orc_state* s, double* F1);
 /* Parameters of the learned closure (LES_MODEL_TYPE 4), in the layout of the
  * GPU library's diablo_mlp_set_params; NULL removes it. */
 void orc_set_mlp(orc_state* s, const float* params);

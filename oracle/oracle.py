@@ -65,6 +65,7 @@ def lib() -> ctypes.CDLL:
         L.orc_mean_stats.argtypes = [vp, dp, dp, dp]
         L.orc_set_user_rhs.argtypes = [vp, ip, USER_FN, vp]
         L.orc_epsilon_sgs.argtypes = [vp, dp]
+        L.orc_epsilon_field.argtypes = [vp, dp]
         L.orc_set_mlp.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
         L.orc_cdft.restype = ip
         L.orc_cdft.argtypes = [ip, dp, ip]
@@ -203,6 +204,12 @@ class Oracle:
         out = np.zeros(self.p.ny + 2)
         lib().orc_epsilon_sgs(self._h, _dptr(out))
         return out
+
+    def epsilon_field(self) -> np.ndarray:
+        """tkebudget_chan's F1 as [J][K][I] (NY+2, NZ, NX), rows 2..NY-1."""
+        buf = np.zeros(physical_shape(self.p))
+        lib().orc_epsilon_field(self._h, _dptr(buf))
+        return buf[:, : self.p.nz, : self.p.nx].copy()
 
     def set_user_rhs(self, kind: int, fn) -> None:
         """USER_RHS_CHAN_FOURIER (kind 0) / _PHYSICAL (kind 1): fn(oracle)

@@ -246,7 +246,7 @@ def test_movie_planes(tmp_path):
     o.step(1)
     w.save(_LesRun(o, 0.01, 1, 0.01))
     mv = statsfile.read(str(tmp_path / "movie.h5"))
-    names = [f"{q}_{s}" for q in ("u", "v", "w", "th01") for s in ("xy", "xz", "zy")]
+    names = [f"{q}_{s}" for q in ("u", "v", "w", "th01", "epsilon") for s in ("xy", "xz", "zy")]
     assert sorted(mv) == sorted(names) and all(mv[k]["SAMPLES"] == 2 for k in names)
     u1, u2 = oracle_physical(o, o.cu[0]), oracle_physical(o, o.cu[1])
     th = oracle_physical(o, o.cth[0])
@@ -261,3 +261,28 @@ def test_movie_planes(tmp_path):
     assert statsfile.movie_indices(p, g, xc, yc, 1.5 * p.lz)[2] is None
     with pytest.raises(ValueError):
         statsfile.movie_indices(p, g, 2.0 * p.lx, yc, zc)
+
+
+def test_epsilon_field_matches_oracle(tmp_path):
+    """tkebudget_chan's F1 (save_stats.f:957-1131): the writer's host form
+    against the oracle's, and its plane means against the epsilon profile."""
+    from test_checkpoint import kh
+    p, g, u, th = kh(24, 33, 20)
+    o = Oracle(p, g, 0.01)
+    o.init_from_physical(u, th)
+    o.step(2)
+    o.stats()                                             # the statistics' APPLY_BC_VEL
+    ref = o.epsilon_field()
+    host = statsfile.epsilon_field(_LesRun(o, 0.02, 2, 0.01))
+    scale = np.abs(ref).max()
+    assert scale > 0 and np.abs(host - ref).max() <= 1e-12 * scale
+    assert not ref[[0, 1, p.ny, p.ny + 1]].any()
+    means = ref.sum(axis=(1, 2)) / (p.nx * p.nz)
+    eps = o.mean_stats()["epsilon"]
+    assert np.allclose(means, eps, rtol=1e-12, atol=1e-14 * np.abs(eps).max())
+    centres = (0.25 * p.lx, float(g.gyf[p.ny // 2]), 0.5 * p.lz)
+    statsfile.StatsWriter(str(tmp_path), movie=centres).save(_LesRun(o, 0.02, 2, 0.01))
+    nx_m, ny_m, nz_m = statsfile.movie_indices(p, g, *centres)
+    mv = statsfile.read(str(tmp_path / "movie.h5"))
+    assert np.abs(mv["epsilon_xz"]["data"][0] - ref[ny_m]).max() <= 1e-12 * scale
+    assert mv["epsilon_zy"]["data"][0].shape == (p.ny, p.nz)
