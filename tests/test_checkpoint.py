@@ -265,3 +265,28 @@ def test_oracle_restart_from_legacy_files(tmp_path):
     o2.step(3)
     for a, b in zip(state(o2), state(o)):
         assert rel(a, b) < 1e-13
+
+
+@pytest.mark.parametrize("n_th", [0, 2])
+def test_scalar_counts_round_trip(tmp_path, n_th):
+    """No scalar and two scalars through both formats."""
+    p, _, _, _ = kh(12, 9, 10)
+    p.n_th = n_th
+    if n_th > 1:
+        p.pr[1], p.ri[1] = 2.0, 0.0
+    rng = np.random.default_rng(5)
+    f = {k: rng.standard_normal((p.ny + 2, p.nz, p.nx)) for k in ["U", "V", "W"] + ck.scalar_names(p)}
+    path = str(tmp_path / "out.npz")
+    ck.write(path, p, f, 0.5, 3)
+    r = ck.read(path, p)
+    assert sorted(r["fields"]) == sorted(["U", "V", "W"] + ck.scalar_names(p))
+    for k in ck.scalar_names(p):
+        assert np.array_equal(r["fields"][k][1:-1], f[k][1:-1])
+    for n in range(n_th):
+        th = layout.new_fourier(p)
+        th[...] = rng.standard_normal(th.shape)
+        sp = str(tmp_path / f"diablo_th{n + 1:02d}.saved")
+        ck.write_legacy_scalar(sp, p, th, 0.5, 3)
+        got = ck.read_legacy_scalar(sp, p)["cth"]
+        blk = np.s_[: p.ny + 1, : p.tnkz + 1, : p.nkx + 1]
+        assert np.array_equal(got[blk], th[blk])
