@@ -126,7 +126,7 @@ bool is_235(int n) {
 }
 
 template <typename T>
-void* make_twiddles(int n, cudaError_t* err) {
+void* make_twiddles(int n, cudaStream_t st, cudaError_t* err) {
     std::vector<T> h(2 * (size_t)n);
     const long double pi = 3.141592653589793238462643383279502884L;
     for (int k = 0; k < n; ++k) {
@@ -137,7 +137,8 @@ void* make_twiddles(int n, cudaError_t* err) {
     }
     void* d = nullptr;
     *err = cudaMalloc(&d, sizeof(T) * h.size());
-    if (*err == cudaSuccess) *err = cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
+    // stream-ordered with the handle's kernels; a pageable source is consumed before the call returns
+    if (*err == cudaSuccess) *err = cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, st);
     return d;
 }
 
@@ -420,12 +421,14 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     h->s_field = h->s_plane * d.nyp;
     h->x_plane = (size_t)d.nz * d.ldx;
     h->x_field = h->x_plane * d.nyp;
+    // Every set-up memset and copy goes on the handle's non-blocking stream: work on the legacy
+    // default stream would not be ordered before the kernels that read these buffers.
+    cudaError_t e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
     auto dmalloc = [&](void** ptr, size_t bytes) -> cudaError_t {
         cudaError_t e = cudaMalloc(ptr, bytes);
-        if (e == cudaSuccess) e = cudaMemset(*ptr, 0, bytes);
+        if (e == cudaSuccess) e = cudaMemsetAsync(*ptr, 0, bytes, h->st);
         return e;
     };
-    cudaError_t e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
     const size_t sb = sizeof(double2) * h->s_field;
     const size_t nyp = (size_t)d.nyp;
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_dy, sizeof(double) * nyp);
@@ -446,7 +449,6 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_tabs, sizeof(double) * part_table_doubles(d.nyp) * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_phitab, sizeof(double) * phi_table_doubles(d));
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_nan, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(h->d_nan, 0, sizeof(int));
     if (e == cudaSuccess) e = dmalloc((void**)&h->bcv, sizeof(double) * nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->kind, nyp * d.nf);
     if (e == cudaSuccess) e = dmalloc((void**)&h->dtmin, sizeof(double));
@@ -479,7 +481,7 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     std::vector<double> k2(d.splane(), 0.0);
     for (int m = 0; m < d.nkzp; ++m)
         for (int i = 0; i < d.ldx; ++i) k2[(size_t)m * d.ldx + i] = std::pow(kx[i] * kx[i] + kz[m] * kz[m], p->beta);
-    e = cudaMemcpy(h->d_k2, k2.data(), sizeof(double) * k2.size(), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(h->d_k2, k2.data(), sizeof(double) * k2.size(), cudaMemcpyHostToDevice, h->st);
     {
         std::vector<double> rows((size_t)RT_COUNT * nyp, 0.0);
         auto R = [&](int t, int j) -> double& { return rows[(size_t)t * nyp + j]; };
@@ -497,13 +499,13 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
             R(RT_BY1, j) = DYj != 0.0 ? DYFj / (2.0 * DYj) : 0.0;
         }
         if (e == cudaSuccess)
-            e = cudaMemcpy(h->d_rows, rows.data(), sizeof(double) * rows.size(), cudaMemcpyHostToDevice);
+            e = cudaMemcpyAsync(h->d_rows, rows.data(), sizeof(double) * rows.size(), cudaMemcpyHostToDevice, h->st);
     }
-    if (e == cudaSuccess) e = cudaMemcpy(h->d_kx, kx.data(), sizeof(double) * d.ldx, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(h->d_kz, kz.data(), sizeof(double) * d.nkzp, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(h->d_dy, dy, sizeof(double) * nyp, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(h->d_dyf, dyf, sizeof(double) * nyp, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(h->d_gyf, gyf, sizeof(double) * nyp, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_kx, kx.data(), sizeof(double) * d.ldx, cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_kz, kz.data(), sizeof(double) * d.nkzp, cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_dy, dy, sizeof(double) * nyp, cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_dyf, dyf, sizeof(double) * nyp, cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_gyf, gyf, sizeof(double) * nyp, cudaMemcpyHostToDevice, h->st);
     if (e == cudaSuccess && p->les) {
         // filter widths with -2 C_s^2 absorbed, C_s = 0.13, beta_sgs = 1
         // (les.f:196-217), Delta_YF at GYF and Delta_Y at GY points, J = 1..NY+1
@@ -513,14 +515,14 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
             w[j] = -2.0 * (C_SMAG * C_SMAG) * std::pow(h->dx * beta_sgs * dyf[j] * 2.0 * h->dz * beta_sgs, 2.0 / 3.0);
             w[nyp + j] = -2.0 * (C_SMAG * C_SMAG) * std::pow(h->dx * beta_sgs * dy[j] * 2.0 * h->dz * beta_sgs, 2.0 / 3.0);
         }
-        e = cudaMemcpy(h->d_delta, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(h->d_delta, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, h->st);
     }
-    if (e == cudaSuccess) h->twn_d = make_twiddles<double>(d.nx, &e);
-    if (e == cudaSuccess) h->twm_d = make_twiddles<double>(d.nx / 2, &e);
-    if (e == cudaSuccess) h->twz_d = make_twiddles<double>(d.nz, &e);
-    if (e == cudaSuccess) h->twn_f = make_twiddles<float>(d.nx, &e);
-    if (e == cudaSuccess) h->twm_f = make_twiddles<float>(d.nx / 2, &e);
-    if (e == cudaSuccess) h->twz_f = make_twiddles<float>(d.nz, &e);
+    if (e == cudaSuccess) h->twn_d = make_twiddles<double>(d.nx, h->st, &e);
+    if (e == cudaSuccess) h->twm_d = make_twiddles<double>(d.nx / 2, h->st, &e);
+    if (e == cudaSuccess) h->twz_d = make_twiddles<double>(d.nz, h->st, &e);
+    if (e == cudaSuccess) h->twn_f = make_twiddles<float>(d.nx, h->st, &e);
+    if (e == cudaSuccess) h->twm_f = make_twiddles<float>(d.nx / 2, h->st, &e);
+    if (e == cudaSuccess) h->twz_f = make_twiddles<float>(d.nz, h->st, &e);
     if (e == cudaSuccess) e = launch_phi_part(d, h->d_rows, h->d_kx, h->d_kz, h->d_phitab, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
     if (e != cudaSuccess) {
@@ -1355,7 +1357,7 @@ int diablo_gpu_mean_stats(void* handle, double* chan, double* scal, double* epsi
         }
         std::vector<double> rg(nyp, 0.0);
         for (int j = 1; j <= d.ny; ++j) rg[j] = 1.0 / (h->gy[j + 1] - h->gy[j - 1]);
-        CK(cudaMemcpy(h->d_msums + (size_t)nsum * nyp, rg.data(), sizeof(double) * nyp, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(h->d_msums + (size_t)nsum * nyp, rg.data(), sizeof(double) * nyp, cudaMemcpyHostToDevice, h->st));
     }
     ProfScope ps(h, DIABLO_KERNEL_OTHER);
     double* acc = h->d_msums;

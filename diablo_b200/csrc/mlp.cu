@@ -522,7 +522,7 @@ int stage(Mlp* m, const float* x, const float* t, long long n) {
 int run_grad(Mlp* m, long long s_begin, long long n, float inv_batch) {
     MlpDev md{m->wb, m->p};
     const size_t smem = grad_smem();
-    cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    MCK(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long tiles = (n + TS - 1) / TS;
     long long nb = (tiles + NW - 1) / NW;
     if (nb > m->nblocks) nb = m->nblocks;
@@ -538,7 +538,8 @@ cudaError_t launch_mlp_forward(const void* mlp, const float* x, long long n, flo
     const Mlp* m = (const Mlp*)mlp;
     MlpDev md{m->wb, m->p};
     const size_t smem = fwd_smem();
-    cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     const long long tiles = (n + TS - 1) / TS;
     long long nb = (tiles + FW - 1) / FW;
     if (nb > 148 * 4) nb = 148 * 4;
@@ -564,11 +565,16 @@ int diablo_mlp_create(void** mlp) {
     if (e == cudaSuccess) e = cudaMalloc((void**)&m->m2, sizeof(float) * NTRAIN);
     if (e == cudaSuccess) e = cudaMalloc((void**)&m->wb, sizeof(uint16_t) * SWN);
     if (e == cudaSuccess) e = cudaMalloc((void**)&m->loss, sizeof(double));
-    if (e == cudaSuccess) e = cudaMemset(m->p, 0, sizeof(float) * NPARAM);
-    if (e == cudaSuccess) e = cudaMemset(m->g, 0, sizeof(float) * NTRAIN);
-    if (e == cudaSuccess) e = cudaMemset(m->m1, 0, sizeof(float) * NTRAIN);
-    if (e == cudaSuccess) e = cudaMemset(m->m2, 0, sizeof(float) * NTRAIN);
-    if (e == cudaSuccess) e = cudaMemset(m->wb, 0, sizeof(uint16_t) * SWN);
+    // Zeroed on the network's own non-blocking stream and waited for here: a memset on the
+    // legacy default stream is not ordered before the later uploads and packing on m->st,
+    // and could land after them (packed weights wiped to zero, Adam moments reset mid-run).
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->p, 0, sizeof(float) * NPARAM, m->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->g, 0, sizeof(float) * NTRAIN, m->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->m1, 0, sizeof(float) * NTRAIN, m->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->m2, 0, sizeof(float) * NTRAIN, m->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->wb, 0, sizeof(uint16_t) * SWN, m->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->loss, 0, sizeof(double), m->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->st);
     int dev = 0, sms = 148;
     if (e == cudaSuccess) e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -3,12 +3,12 @@
 //
 // Who needs it: a host that keeps its fields in device memory it obtained
 // itself -- a Fortran code with OpenACC or CUDA Fortran device arrays, a
-// framework that hands out memory from its own pool, code that runs while a
-// CUDA graph is being captured -- and therefore cannot let a library call
-// cudaMalloc (the allocation would bypass its pool, or is forbidden in that
-// context).  This entry point only launches one kernel on the caller's stream;
-// its working storage is the file-scope array below, which is created when
-// the library is loaded and held by every GPU that loads it until the process
+// framework that hands out memory from its own pool -- and therefore cannot
+// let a library call cudaMalloc (the allocation would bypass the runtime or
+// pool that owns the device memory).  This entry point only queues two small
+// copies of the grid metrics and one kernel on the caller's stream; its
+// working storage is the file-scope array below, which is created when the
+// library is loaded and held by every GPU that loads it until the process
 // exits.
 //
 // Limits and sharing: the array holds 2^20 doubles (8 MiB).  A call needs

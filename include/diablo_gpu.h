@@ -268,13 +268,17 @@ int diablo_gpu_kernel_times(void* handle, long long* launches, double* ms);
 /* REM_DIV_CHAN for callers that cannot allocate device memory.  This entry
  * point has no counterpart in the reference: it exists for hosts that keep
  * CU1, CU2, CU3 in device memory they obtained themselves (OpenACC or CUDA
- * Fortran device arrays, a framework's memory pool, code running during
- * stream capture) and cannot let a library call cudaMalloc.  It allocates
- * nothing: it launches one kernel on `stream` (a cudaStream_t, NULL for the
- * default stream) and keeps its working storage in an 8 MiB array of static
- * device memory that every GPU loading this library holds until exit.
+ * Fortran device arrays, a framework's memory pool) and cannot let a library
+ * call cudaMalloc, because that memory is managed by the host's runtime or
+ * pool and a second allocator would bypass it.  It allocates nothing: it
+ * queues two small host-to-device copies of the grid metrics and one kernel
+ * on `stream` (a cudaStream_t, NULL for the default stream) and keeps its
+ * working storage in an 8 MiB array of static device memory that every GPU
+ * loading this library holds until exit.
  *   p        sizes and LX, LZ (other fields unused)
- *   dy, dyf  HOST pointers to DY(0:NY+1), DYF(0:NY+1)
+ *   dy, dyf  HOST pointers to DY(0:NY+1), DYF(0:NY+1); pageable memory is
+ *            read before the call returns, page-locked memory when the copy
+ *            runs on `stream`, so keep it unchanged until then
  *   cu1..3   DEVICE pointers, Fortran layout (0:NXP,0:NZ+1,0:NY+1) complex;
  *            projected in place (dealiased block, J = 1..NY)
  *   phi      DEVICE pointer, same layout; receives phi on J = 1..NY

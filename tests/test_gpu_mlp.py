@@ -71,3 +71,24 @@ def test_training_lowers_loss():
     assert np.isfinite(losses).all()
     assert after < 0.2 * before, (before, after)
     assert np.array_equal(q[M.NTRAIN:], p[M.NTRAIN:])      # normalisation is not trained
+
+
+def test_training_is_reproducible():
+    """Two trainings from the same seed and data on fresh networks.  The
+    gradient sums use FP32 atomics, whose order varies from run to run, so
+    the two loss curves agree statistically rather than bit for bit: the
+    means of the last 100 mini-batch losses within 5% and the final
+    full-data losses within 5%."""
+    x, t, p = data(9, 20000)
+    runs = []
+    for _ in range(2):
+        with ML.SgsMlp(p) as m:
+            losses = m.train(x, t, batch=512, steps=600, lr=2e-3)
+            after, _ = m.gradient(x, t)
+        runs.append((losses, after))
+    (l0, a0), (l1, a1) = runs
+    assert np.isfinite(l0).all() and np.isfinite(l1).all()
+    assert abs(l0[0] - l1[0]) <= 1e-5 * l0[0]        # the first mini-batch sees identical weights
+    m0, m1 = l0[-100:].mean(), l1[-100:].mean()
+    assert abs(m0 - m1) <= 0.05 * max(m0, m1), (m0, m1)
+    assert abs(a0 - a1) <= 0.05 * max(a0, a1), (a0, a1)

@@ -5,8 +5,8 @@ and cannot let a library call cudaMalloc; it works in place on device arrays
 in the Fortran layout and keeps its scratch in static device memory.  This
 test owns the device arrays itself (torch allocates them, the entry point
 does not) and checks two consecutive calls, with different fields, against
-diablo_gpu_rem_div_chan on a library handle.  The file name makes pytest
-collect it last."""
+diablo_gpu_rem_div_chan on a library handle and against the CPU oracle's
+REM_DIV_CHAN.  The file name makes pytest collect it last."""
 import ctypes
 
 import numpy as np
@@ -66,6 +66,47 @@ def test_rem_div_noalloc_matches_handle_path_on_two_calls():
             assert _relerr(a, b) < TOL64, (call, k)
         phi_h = phi.cpu().numpy().view(np.complex128).reshape(layout.fourier_shape(p))
         assert _relerr(layout.dealiased(p, phi_h)[1: p.ny + 1], layout.dealiased(p, ref_phi)[1: p.ny + 1]) < TOL64
+
+
+def test_rem_div_noalloc_matches_oracle_on_two_calls():
+    """Two calls in a row on the same device arrays (the second starts from
+    the first one's projected field plus new noise), each against the CPU
+    oracle's REM_DIV_CHAN on the same input: CU1..CU3 and phi on J = 1..NY."""
+    import torch
+
+    from oracle.oracle import ORC_U1, ORC_U2, ORC_U3, Oracle
+
+    L = load_library()
+    w = workloads.kh(40, 17, 30)
+    p, g = w.p, w.grid
+    rng = np.random.default_rng(77)
+    dy = np.ascontiguousarray(g.dy)
+    dyf = np.ascontiguousarray(g.dyf)
+    cu = _random_velocity(p, rng)
+    dev = [torch.from_numpy(x.view(np.float64).reshape(-1).copy()).cuda() for x in cu]
+    phi = torch.full_like(dev[0], float("nan"))
+    o = Oracle(p, g, w.dt)
+    for call in range(2):
+        if call:
+            noise = _random_velocity(p, rng)
+            for k in range(3):
+                dev[k] += torch.from_numpy(0.5 * noise[k].view(np.float64).reshape(-1)).cuda()
+        start = [t.cpu().numpy().copy() for t in dev]
+        for k, which in enumerate((ORC_U1, ORC_U2, ORC_U3)):
+            o.raw(which)[:] = start[k]
+        o.rem_div_chan()
+        stream = torch.cuda.current_stream().cuda_stream
+        rc = L.diablo_gpu_rem_div_chan_noalloc(ctypes.byref(p), _dp(dy), _dp(dyf), dev[0].data_ptr(),
+                                                dev[1].data_ptr(), dev[2].data_ptr(), phi.data_ptr(),
+                                                ctypes.c_void_p(stream))
+        assert rc == DIABLO_OK, L.diablo_gpu_last_error()
+        torch.cuda.synchronize()
+        for k in range(3):
+            a = layout.dealiased(p, dev[k].cpu().numpy().view(np.complex128).reshape(layout.fourier_shape(p)))
+            b = layout.dealiased(p, o.cu[k])
+            assert _relerr(a[1: p.ny + 1], b[1: p.ny + 1]) < TOL64, (call, k)
+        phi_h = phi.cpu().numpy().view(np.complex128).reshape(layout.fourier_shape(p))
+        assert _relerr(layout.dealiased(p, phi_h)[1: p.ny + 1], layout.dealiased(p, o.phi)[1: p.ny + 1]) < TOL64
 
 
 def test_rem_div_noalloc_rejects_grids_beyond_its_scratch():
