@@ -1,6 +1,6 @@
 """Regenerate the committed fixtures of tests/golden/.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <path of the reference checkout>
 
 * kh_grid_y.txt     -- the 66 GY values stored in the reference's
                        KH_test/grid.h5 (/grids/y), read straight from the
@@ -56,7 +56,7 @@ def oracle_fixture(path: str) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the reference checkout (holds diablo_2.0/)")
     a = ap.parse_args()
     kh = os.path.join(a.reference, "diablo_2.0", "KH_test")
     gy = read_grid_h5(os.path.join(kh, "grid.h5"), 66)
