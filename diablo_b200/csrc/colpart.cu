@@ -477,7 +477,21 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
                           (fu2 * (1.0 - fzm) * a.ri[n] * a.grav_y) * (BY0[j] * thj + BY1[j] * thm);
                 }
             }
-            const double2 CF = (-nuf * k2) * w1 + cpl + as_d2(nlv[it]);
+            double2 CF = (-nuf * k2) * w1 + cpl + as_d2(nlv[it]);
+            if (A.mean_split && zero_mode && j >= A.jlo_prod && j <= ny) {
+                // the mean x mean part of the y-flux product, -d/dy of (Q V) with
+                // Q this field's plane mean and V = U2's (channel.f:514-516,
+                // 535-537, 557-558): the only products that reach the (0,0) mode
+                const double v0 = sU[slot(1, j, 0)].x, vp = sU[slot(1, jp, 0)].x, vm = sU[slot(1, jm, 0)].x;
+                double mm;
+                if (isu2) {
+                    mm = 0.25 * ((v0 + vp) * (v0 + vp) - (v0 + vm) * (v0 + vm)) * RDY[j];
+                } else {
+                    const double q0 = sU[slot(f, j, 0)].x, qp = sU[slot(f, jp, 0)].x, qm = sU[slot(f, jm, 0)].x;
+                    mm = ((qp + q0) * vp - (q0 + qm) * v0) * (0.5 * RDYF[j]);
+                }
+                CF.x -= mm;
+            }
             const double2 cpj = sP[j * 2 + c];
             const double2 cpm = wm * sP[jm * 2 + c];
             const double2 cfo = cfv[it];

@@ -347,11 +347,13 @@ int run_transforms(Handle* h) {
     const void* twn = f ? h->twn_f : h->twn_d;
     const void* twm = f ? h->twm_f : h->twm_d;
     const void* twz = f ? h->twz_f : h->twz_d;
+    // FP32 transforms carry each field's fluctuation about its plane mean; the
+    // means (the (0,0) mode, O(1) in a shear layer or channel) stay FP64
     { ProfScope ps(h, DIABLO_KERNEL_ZINV);
-      CK(launch_zinv<T>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, twz, h->st)); }
+      CK(launch_zinv<T>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, twz, h->st, f ? 1 : 0)); }
     { ProfScope ps(h, DIABLO_KERNEL_PRODUCTS);
       CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, h->prod_chunk, h->d_dy, h->d_dyf, h->d_kx, h->pm, twm, twn,
-                            h->st)); }
+                            h->st, f ? h->cu : nullptr, h->s_field)); }
     { ProfScope ps(h, DIABLO_KERNEL_ZFWD_NL);
       CK(launch_zfwd_nl<T>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->zf_planes, h->d_kx, h->d_kz, h->pz, twz, h->st)); }
     h->launches += 3;
@@ -1006,6 +1008,8 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     ca.update_cp = 1;
     ca.store_phi = 0;             // phi stays where REM_DIV_CHAN alone puts it
     ca.nan_flag = h->d_nan;
+    ca.mean_split = h->fp32 ? 1 : 0;
+    ca.jlo_prod = h->jlo_prod;
     {
         ProfScope ps(h, DIABLO_KERNEL_COLUMN);
         if (h->fp32) CK(launch_colpart<cpx<float>>(ca, (const cpx<float>*)h->nl, h->d_tabs, h->st));

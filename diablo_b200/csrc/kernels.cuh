@@ -87,6 +87,9 @@ struct ColArgs {
     int update_cp;        // CP += phi/h on J = 2..NY
     int store_phi;
     int* nan_flag;        // set to 1 when a new CU value is not finite (may be null)
+    int mean_split;       // the nonlinear term lacks the mean x mean products: add them to
+                          // the (0,0) mode in FP64 on the product planes jlo_prod..NY
+    int jlo_prod;
 };
 
 struct RemDivArgs {

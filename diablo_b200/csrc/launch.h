@@ -12,10 +12,12 @@ namespace dgpu {
 
 // Planes [j0, j0+nplanes) of fields [0,nfields) of S (FP64 spectral) ->
 // X (x-spectrum, type T): unpack kz, backward z transform (mpi.f:1562-1577).
+// skip_mean: leave out the (0,0) mode, so X is the fluctuation about the
+// plane mean (the FP32 transform path; the mean stays FP64).
 template <typename T>
 cudaError_t launch_zinv(const Dims& d, const double2* S, size_t s_fstride, void* X, size_t x_fstride,
                         int nfields, int j0, int nplanes, const FftPlan& pz, const void* twz,
-                        cudaStream_t st);
+                        cudaStream_t st, int skip_mean = 0);
 
 // Fused per z-row: backward x transform of the fields at planes jlo-1..jhi+1,
 // the 8 + 3*N_TH physical products of RK_CHAN_1 (channel.f:410-571,
@@ -23,10 +25,15 @@ cudaError_t launch_zinv(const Dims& d, const double2* S, size_t s_fstride, void*
 // to kx <= NKX (mpi.f:1493-1508), combined into 2 outputs per field
 // (ikx*Pa + Pflux, Pz) -> Y.
 // pm/twm: plan and table of the NX/2-point complex FFT; twn: table of NX.
+// means (S layout, field stride means_fstride): when given, X holds each
+// field's fluctuation about its plane mean (launch_zinv with skip_mean) and
+// the products are formed without their mean x mean part, which only the
+// (0,0) mode carries (the column kernel adds it in FP64).
 template <typename T>
 cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int jhi, int chunk,
                             const double* dy, const double* dyf, const double* kx, const FftPlan& pm,
-                            const void* twm, const void* twn, cudaStream_t st);
+                            const void* twm, const void* twn, cudaStream_t st, const double2* means = nullptr,
+                            size_t means_fstride = 0);
 
 // Per plane (zp planes per block, 0 = default): forward z transform of the 2
 // product outputs of every field,

@@ -73,10 +73,12 @@ __device__ __forceinline__ void col_fft(cpx<T>* buf, const FftPlan& P, const cpx
 // K1: spectral (FP64) -> x-spectrum (T); inverse z transform along columns.
 // Block (kx tile of TX columns, plane J, field f); 256 threads.
 // ---------------------------------------------------------------------------
+// With skip_mean the (kx,kz) = (0,0) mode (the plane mean) is left out, so X
+// holds the fluctuation about each plane's mean.
 template <typename T, int NC, int TX>
 __global__ void __launch_bounds__(256) k_zinv(Dims d, const double2* __restrict__ S, size_t s_fstride,
                                               cpx<T>* __restrict__ X, size_t x_fstride, int j0,
-                                              FftPlan pz, const cpx<T>* __restrict__ twz) {
+                                              FftPlan pz, const cpx<T>* __restrict__ twz, int skip_mean) {
     extern __shared__ unsigned char smem_raw[];
     cpx<T>* buf = reinterpret_cast<cpx<T>*>(smem_raw);   // [nz][TX]
     const int nz = NC > 0 ? NC : d.nz;
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, const double2* __restrict_
         if (z <= nkz) m = z;
         else if (z >= nz - nkz) m = z - nz + nkzt;
         cpx<T> v = mk<T>(0, 0);
-        if (m >= 0 && kx < d.nkxp) v = ld<T>(src + (size_t)m * d.ldx + kx);
+        if (m >= 0 && kx < d.nkxp && !(skip_mean && m == 0 && kx == 0)) v = ld<T>(src + (size_t)m * d.ldx + kx);
         buf[e] = v;
     }
     __syncthreads();
@@ -188,8 +190,10 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
                                                      const double* __restrict__ dyf,
                                                      const double* __restrict__ kxw, FftPlan pm,
                                                      const cpx<T>* __restrict__ twm,
-                                                     const cpx<T>* __restrict__ twn) {
+                                                     const cpx<T>* __restrict__ twn,
+                                                     const double2* __restrict__ means, size_t means_fs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T smean[RING][MAXF];   // plane means of the ring planes (zero without mean split)
     const int M = MC > 0 ? MC : d.nx / 2;
     const int nx = 2 * M;
     const int nf = d.nf, np = d.np, nrow = nf + np;
@@ -229,6 +233,8 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
     stage(jb - 1);
     for (int J = jb - 1; J <= je + 2; ++J) {
         const bool do_inv = (J <= je + 1);
+        if (do_inv && threadIdx.x < nf)   // slot(J) last held plane J-4, which no product reads any more
+            smean[slot(J)][threadIdx.x] = means ? (T)means[threadIdx.x * means_fs + (size_t)J * d.splane()].x : T(0);
         if (do_inv) {
             if (J + 1 <= je + 1) {
                 stage(J + 1);
@@ -261,6 +267,15 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
             const int p0 = max(c0, nf) - nf, p1 = c0 + nr - nf;       // products p0..p1-1 here
             if (p1 > p0) {
                 const int sm = slot(jp - 1), s0 = slot(jp), sp = slot(jp + 1);
+                // The ring holds each field as fluctuation a' about its plane mean
+                // abar (abar = 0 without the mean split).  A product ab is formed
+                // as its part beyond abar*bbar: a'(bbar + b') + abar b', whose
+                // rounding error is relative to the fluctuations, not to the O(1)
+                // means.  abar*bbar reaches only the (0,0) mode, which the column
+                // kernel adds in FP64.
+                const T m1m = smean[sm][0], m1 = smean[s0][0], m1p = smean[sp][0];
+                const T m2m = smean[sm][1], m2 = smean[s0][1], m2p = smean[sp][1];
+                const T m3m = smean[sm][2], m3 = smean[s0][2], m3p = smean[sp][2];
                 for (int x = threadIdx.x; x < nx; x += 256) {
                     const T* r_m = ring + (size_t)sm * nf * nx + x;
                     const T* r_c = ring + (size_t)s0 * nf * nx + x;
@@ -268,16 +283,19 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
                     const T u1m = r_m[0], u1 = r_c[0], u1p = r_p[0];
                     const T u2m = r_m[nx], u2 = r_c[nx], u2p = r_p[nx];
                     const T u3m = r_m[2 * nx], u3 = r_c[2 * nx], u3p = r_p[2 * nx];
+                    const T U1 = m1 + u1, U2 = m2 + u2, U2p = m2p + u2p, U3 = m3 + u3;
                     T v[8];
-                    v[0] = u3 * u1;
-                    v[1] = u1 * u1;
-                    v[2] = u3 * u3;
-                    v[3] = (a1 * u1 + a0 * u1m) * u2;
-                    v[4] = (a1 * u3 + a0 * u3m) * u2;
-                    v[5] = (u1p * u2p + u1 * u2p - u1 * u2 - u1m * u2) * i2dyf;
-                    v[6] = (u3p * u2p + u3 * u2p - u3 * u2 - u3m * u2) * i2dyf;
-                    const T s1 = u2 + u2p, s2 = u2 + u2m;
-                    v[7] = (T(0.25) * s1 * s1 - T(0.25) * s2 * s2) * idy;
+                    v[0] = u3 * U1 + m3 * u1;                                   // U1 U3
+                    v[1] = u1 * (U1 + m1);                                      // U1 U1
+                    v[2] = u3 * (U3 + m3);                                      // U3 U3
+                    v[3] = (a1 * u1 + a0 * u1m) * U2 + (a1 * m1 + a0 * m1m) * u2;   // (U1 at GY) U2
+                    v[4] = (a1 * u3 + a0 * u3m) * U2 + (a1 * m3 + a0 * m3m) * u2;   // (U3 at GY) U2
+                    // (U1(j+1) + U1(j)) U2(j+1) - (U1(j) + U1(j-1)) U2(j), over 2 DYF(j)
+                    v[5] = ((u1p + u1) * U2p + (m1p + m1) * u2p - (u1 + u1m) * U2 - (m1 + m1m) * u2) * i2dyf;
+                    v[6] = ((u3p + u3) * U2p + (m3p + m3) * u2p - (u3 + u3m) * U2 - (m3 + m3m) * u2) * i2dyf;
+                    // (U2(j) + U2(j+1))^2/4 - (U2(j) + U2(j-1))^2/4, over DY(j)
+                    const T s1 = u2 + u2p, s2 = u2 + u2m, S1 = m2 + m2p, S2 = m2 + m2m;
+                    v[7] = T(0.25) * (s1 * (s1 + T(2) * S1) - s2 * (s2 + T(2) * S2)) * idy;
                     const int eoff = 2 * lay.at(x >> 1, 0) + (x & 1);
                     const int rstride = 2 * (lay.at(0, 1) - lay.at(0, 0));
 #pragma unroll
@@ -285,10 +303,11 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
                         if (p >= p0 && p < p1) tbuf[eoff + (nf + p - c0) * rstride] = v[p];
                     for (int n = 0; n < d.nth; ++n) {
                         const T thm = r_m[(3 + n) * nx], th = r_c[(3 + n) * nx], thp = r_p[(3 + n) * nx];
+                        const T tm = smean[sm][3 + n], tc = smean[s0][3 + n], tp = smean[sp][3 + n];
                         T w[3];
-                        w[0] = th * u1;
-                        w[1] = th * u3;
-                        w[2] = (thp * u2p + th * u2p - th * u2 - thm * u2) * i2dyf;
+                        w[0] = th * U1 + tc * u1;                               // TH U1
+                        w[1] = th * U3 + tc * u3;                               // TH U3
+                        w[2] = ((thp + th) * U2p + (tp + tc) * u2p - (th + thm) * U2 - (tc + tm) * u2) * i2dyf;
 #pragma unroll
                         for (int r = 0; r < 3; ++r) {
                             const int p = 8 + 3 * n + r;
@@ -516,14 +535,15 @@ __global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __rest
 template <typename T>
 cudaError_t launch_zinv(const Dims& d, const double2* S, size_t s_fstride, void* X, size_t x_fstride,
                         int nfields, int j0, int nplanes, const FftPlan& pz, const void* twz,
-                        cudaStream_t st) {
+                        cudaStream_t st, int skip_mean) {
     constexpr int TX = ZTile<T>::TX;
     if (nplanes <= 0 || nfields <= 0) return cudaSuccess;
     const size_t smem = sizeof(cpx<T>) * (size_t)d.nz * TX;
     dim3 grid(d.ldx / TX, nplanes, nfields);
     auto go = [&](auto kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, 256, smem, st>>>(d, S, s_fstride, (cpx<T>*)X, x_fstride, j0, pz, (const cpx<T>*)twz);
+        kern<<<grid, 256, smem, st>>>(d, S, s_fstride, (cpx<T>*)X, x_fstride, j0, pz, (const cpx<T>*)twz,
+                                      skip_mean);
     };
     switch (d.nz) {
 #define CASE(N) case N: go(k_zinv<T, N, TX>); break;
@@ -544,7 +564,8 @@ int products_group(int nx) {
 template <typename T>
 cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int jhi, int chunk,
                             const double* dy, const double* dyf, const double* kx, const FftPlan& pm,
-                            const void* twm, const void* twn, cudaStream_t st) {
+                            const void* twm, const void* twn, cudaStream_t st, const double2* means,
+                            size_t means_fstride) {
     if (jhi < jlo) return cudaSuccess;
     const int group = products_group(d.nx);
     if (group < 1) return cudaErrorInvalidValue;
@@ -557,7 +578,7 @@ cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int 
     auto go = [&](auto kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<grid, 256, smem, st>>>(d, (const cpx<T>*)X, (cpx<T>*)Y, jlo, jhi, chunk, group, dy, dyf, kx, pm,
-                                      (const cpx<T>*)twm, (const cpx<T>*)twn);
+                                      (const cpx<T>*)twm, (const cpx<T>*)twn, means, means_fstride);
     };
     switch (M) {
 #define CASE(N) case N: go(k_products<T, N>); break;
@@ -811,15 +832,15 @@ cudaError_t launch_cfl(const Dims& d, const void* X, size_t x_fstride, const Fft
 
 // explicit instantiations
 template cudaError_t launch_zinv<float>(const Dims&, const double2*, size_t, void*, size_t, int, int, int,
-                                        const FftPlan&, const void*, cudaStream_t);
+                                        const FftPlan&, const void*, cudaStream_t, int);
 template cudaError_t launch_zinv<double>(const Dims&, const double2*, size_t, void*, size_t, int, int, int,
-                                         const FftPlan&, const void*, cudaStream_t);
+                                         const FftPlan&, const void*, cudaStream_t, int);
 template cudaError_t launch_products<float>(const Dims&, const void*, void*, int, int, int, const double*,
                                             const double*, const double*, const FftPlan&, const void*, const void*,
-                                            cudaStream_t);
+                                            cudaStream_t, const double2*, size_t);
 template cudaError_t launch_products<double>(const Dims&, const void*, void*, int, int, int, const double*,
                                              const double*, const double*, const FftPlan&, const void*, const void*,
-                                             cudaStream_t);
+                                             cudaStream_t, const double2*, size_t);
 template cudaError_t launch_zfwd_nl<float>(const Dims&, const void*, void*, int, int, int, const double*,
                                            const double*, const FftPlan&, const void*, cudaStream_t);
 template cudaError_t launch_zfwd_nl<double>(const Dims&, const void*, void*, int, int, int, const double*,
