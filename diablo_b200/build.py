@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libdiablo_gpu.so")
-SOURCES = ["diablo_gpu.cu", "transforms.cu", "colpart.cu", "noalloc.cu", "poisson_stats.cu", "filter.cu", "les.cu", "mlp.cu"]
+SOURCES = ["diablo_gpu.cu", "transforms.cu", "products_hw.cu", "colpart.cu", "noalloc.cu", "poisson_stats.cu", "filter.cu", "les.cu", "mlp.cu"]
 HEADERS = ["fft.cuh", "fftct.cuh", "kernels.cuh", "launch.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -352,8 +352,12 @@ int run_transforms(Handle* h) {
     { ProfScope ps(h, DIABLO_KERNEL_ZINV);
       CK(launch_zinv<T>(d, h->cu, h->s_field, h->xb, h->x_field, d.nf, 0, d.nyp, h->pz, twz, h->st, f ? 1 : 0)); }
     { ProfScope ps(h, DIABLO_KERNEL_PRODUCTS);
-      CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, h->prod_chunk, h->d_dy, h->d_dyf, h->d_kx, h->pm, twm, twn,
-                            h->st, f ? h->cu : nullptr, h->s_field)); }
+      if (f && products_hw_supported(d))
+          CK(launch_products_hw(d, h->xb, h->yb, h->jlo_prod, d.ny, h->prod_chunk, h->d_dy, h->d_dyf, h->d_kx, twm, twn,
+                                h->st, h->cu, h->s_field));
+      else
+          CK(launch_products<T>(d, h->xb, h->yb, h->jlo_prod, d.ny, h->prod_chunk, h->d_dy, h->d_dyf, h->d_kx, h->pm, twm,
+                                twn, h->st, f ? h->cu : nullptr, h->s_field)); }
     { ProfScope ps(h, DIABLO_KERNEL_ZFWD_NL);
       CK(launch_zfwd_nl<T>(d, h->yb, h->nl, h->jlo_prod, d.ny, h->zf_planes, h->d_kx, h->d_kz, h->pz, twz, h->st)); }
     h->launches += 3;

@@ -35,6 +35,14 @@ cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int 
                             const void* twm, const void* twn, cudaStream_t st, const double2* means = nullptr,
                             size_t means_fstride = 0);
 
+// The same products for NX = 512 in FP32 (products_hw.cu): one block per
+// z-row, one half-warp per field, register-resident 256-point transforms.
+bool products_hw_supported(const Dims& d);
+size_t products_hw_smem(const Dims& d);
+cudaError_t launch_products_hw(const Dims& d, const void* X, void* Y, int jlo, int jhi, int chunk, const double* dy,
+                               const double* dyf, const double* kx, const void* twm, const void* twn, cudaStream_t st,
+                               const double2* means, size_t means_fstride);
+
 // Per plane (zp planes per block, 0 = default): forward z transform of the 2
 // product outputs of every field,
 // kz packing and 1/NZ (mpi.f:1526-1540), then NL = -(first) - ikz (second)
