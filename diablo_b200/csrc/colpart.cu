@@ -333,7 +333,7 @@ cudaError_t launch_cn_part(const Dims& d, const CnArgs& a, double* tabs, double*
 // The nonlinear term and the old CF are read straight from global memory,
 // each thread issuing the loads of all its rows before it uses any.
 // ---------------------------------------------------------------------------
-template <int NW, int RC, typename TN>
+template <int NW, int RC, typename TN, bool PB>
 __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 1)
 k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs, int tstride) {
     constexpr int NROW = NPART * RC;
@@ -441,8 +441,9 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
 #pragma unroll
         for (int it = 0; it < NIT; ++it) {
             const bool v = tid + it * NT < nitem;
-            const size_t o = (size_t)ff[it] * fs + (size_t)jj[it] * ps + g0 + c;
-            if (v) nlv[it] = nl[o];
+            const size_t o = (size_t)ff[it] * fs + spec_at(d, PB, jj[it], g0 + c);    // CF
+            const size_t on = (size_t)ff[it] * fs + spec_at(d, false, jj[it], g0 + c); // NL: S layout
+            if (v) nlv[it] = nl[on];
             cfv[it] = (v && rk1) ? a.cf[o] : zero;
         }
         const bool zero_mode = zm0 && c == 0;
@@ -503,7 +504,7 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
             const int knd = sK[f * NROW + j];
             double2 G = inr ? Gi : zero;
             if (knd != 0) G = zero_mode ? make_double2(a.bcv[f * nyp + j], 0.0) : zero;
-            if (valid && inr && a.store_cf) a.cf[(size_t)f * fs + (size_t)j * ps + g0 + c] = CF;
+            if (valid && inr && a.store_cf) a.cf[(size_t)f * fs + spec_at(d, PB, j, g0 + c)] = CF;
             Gv[it] = G;
         }
         __syncthreads();             // every old CU has been read
@@ -996,18 +997,22 @@ cudaError_t launch_colpart(const ColArgs& a, const TN* nl, const double* tabs, c
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<nblk, 32 * nw, smem, st>>>(a, nl, tabs, tstride);
     };
+#define DGPU_RC_PB(NW, R)                                                       \
+    if (a.pair_blocked) go(k_colpart<NW, R, TN, true>, NW);                     \
+    else go(k_colpart<NW, R, TN, false>, NW);
 #define DGPU_RC_CASES(NW)                                        \
     switch (RC) {                                                \
-        case 3: go(k_colpart<NW, 3, TN>, NW); break;             \
-        case 5: go(k_colpart<NW, 5, TN>, NW); break;             \
-        case 9: go(k_colpart<NW, 9, TN>, NW); break;             \
-        case 17: go(k_colpart<NW, 17, TN>, NW); break;           \
+        case 3: DGPU_RC_PB(NW, 3) break;                         \
+        case 5: DGPU_RC_PB(NW, 5) break;                         \
+        case 9: DGPU_RC_PB(NW, 9) break;                         \
+        case 17: DGPU_RC_PB(NW, 17) break;                       \
         default: return cudaErrorInvalidValue;                   \
     }
     if (d.nf <= 4) { DGPU_RC_CASES(8) }
     else if (d.nf <= 8) { DGPU_RC_CASES(16) }
     else return cudaErrorInvalidValue;
 #undef DGPU_RC_CASES
+#undef DGPU_RC_PB
     return cudaGetLastError();
 }
 

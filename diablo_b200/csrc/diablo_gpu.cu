@@ -42,6 +42,7 @@ struct Handle {
     double dx, dz, pi;
     std::vector<double> gy, gyf, dy, dyf;
     bool fp32;
+    bool pb;          // CF pair-blocked (spec_at): the Fourier-space path without LES
     cudaStream_t st = nullptr;
     size_t s_plane, s_field;      // elements
     size_t x_plane, x_field;      // elements
@@ -218,6 +219,42 @@ __global__ void k_add_user(cpx<T>* __restrict__ dst, const double2* __restrict__
     }
 }
 
+// One spectral field between the S layout and the pair-blocked one.
+__global__ void k_to_pair_blocked(Dims d, const double2* __restrict__ src, double2* __restrict__ dst) {
+    const size_t ps = d.splane(), n = ps * d.nyp;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        dst[spec_at(d, true, (int)(e / ps), e % ps)] = src[e];
+}
+__global__ void k_from_pair_blocked(Dims d, const double2* __restrict__ src, double2* __restrict__ dst) {
+    const size_t ps = d.splane(), n = ps * d.nyp;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        dst[e] = src[spec_at(d, true, (int)(e / ps), e % ps)];
+}
+
+// CF of field f <-> the host array; CF is pair-blocked on the Fourier-space
+// path (h->pb) and passes through the API scratch field.  host == nullptr on
+// upload zeroes the field.
+cudaError_t cf_upload(Handle* h, int f, const double* host) {
+    double2* dev = h->cf + (size_t)f * h->s_field;
+    if (!host) return cudaMemsetAsync(dev, 0, sizeof(double2) * h->s_field, h->st);
+    if (!h->pb) return copy_fourier(h, dev, host, nullptr, 0, h->d.nyp);
+    cudaError_t e = cudaMemsetAsync(h->api_s, 0, sizeof(double2) * h->s_field, h->st);
+    if (e == cudaSuccess) e = copy_fourier(h, h->api_s, host, nullptr, 0, h->d.nyp);
+    if (e != cudaSuccess) return e;
+    k_to_pair_blocked<<<1184, 256, 0, h->st>>>(h->d, h->api_s, dev);
+    return cudaGetLastError();
+}
+
+cudaError_t cf_download(Handle* h, int f, double* host) {
+    const double2* dev = h->cf + (size_t)f * h->s_field;
+    if (!h->pb) return copy_fourier(h, const_cast<double2*>(dev), nullptr, host, 0, h->d.nyp);
+    k_from_pair_blocked<<<1184, 256, 0, h->st>>>(h->d, dev, h->api_s);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = copy_fourier(h, h->api_s, nullptr, host, 0, h->d.nyp);
+    return e;
+}
+
+
 // APPLY_BC_VEL_LOWER / _UPPER (channel.f:2285-2492) on the device state.
 __global__ void k_apply_bc_vel(Dims d, double2* cu, const double* dy, const double* dyf, diablo_params p) {
     const int kx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -392,6 +429,7 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     d.nyp = p->ny + 2;
     h->nxp = p->nx / 2;
     h->fp32 = p->precision == DIABLO_PREC_FP32SPLIT;
+    h->pb = !p->les;      // the LES branch's kernels take CF in the S layout
     h->pi = 4.0 * std::atan(1.0);
     h->dx = p->lx / p->nx;
     h->dz = p->lz / p->nz;
@@ -561,14 +599,8 @@ int diablo_gpu_upload_state(void* handle, const double* cu1, const double* cu2, 
         CK(copy_fourier(h, h->cu + (3 + n) * h->s_field, cth + n * fstride, nullptr, 0, d.nyp));
     CK(copy_fourier(h, h->cp, cp, nullptr, 0, d.nyp));
     const double* cfs[3] = {cf1, cf2, cf3};
-    for (int f = 0; f < 3; ++f) {
-        if (cfs[f]) CK(copy_fourier(h, h->cf + f * h->s_field, cfs[f], nullptr, 0, d.nyp));
-        else CK(cudaMemsetAsync(h->cf + f * h->s_field, 0, sizeof(double2) * h->s_field, h->st));
-    }
-    for (int n = 0; n < d.nth; ++n) {
-        if (cfth) CK(copy_fourier(h, h->cf + (3 + n) * h->s_field, cfth + n * fstride, nullptr, 0, d.nyp));
-        else CK(cudaMemsetAsync(h->cf + (3 + n) * h->s_field, 0, sizeof(double2) * h->s_field, h->st));
-    }
+    for (int f = 0; f < 3; ++f) CK(cf_upload(h, f, cfs[f]));
+    for (int n = 0; n < d.nth; ++n) CK(cf_upload(h, 3 + n, cfth ? cfth + n * fstride : nullptr));
     CK(cudaStreamSynchronize(h->st));
     return DIABLO_OK;
 }
@@ -583,11 +615,11 @@ int diablo_gpu_download_state(void* handle, double* cu1, double* cu2, double* cu
     double* cfs[3] = {cf1, cf2, cf3};
     for (int f = 0; f < 3; ++f) {
         if (cus[f]) CK(copy_fourier(h, h->cu + f * h->s_field, nullptr, cus[f], 0, d.nyp));
-        if (cfs[f]) CK(copy_fourier(h, h->cf + f * h->s_field, nullptr, cfs[f], 0, d.nyp));
+        if (cfs[f]) CK(cf_download(h, f, cfs[f]));
     }
     for (int n = 0; n < d.nth; ++n) {
         if (cth) CK(copy_fourier(h, h->cu + (3 + n) * h->s_field, nullptr, cth + n * fstride, 0, d.nyp));
-        if (cfth) CK(copy_fourier(h, h->cf + (3 + n) * h->s_field, nullptr, cfth + n * fstride, 0, d.nyp));
+        if (cfth) CK(cf_download(h, 3 + n, cfth + n * fstride));
     }
     if (cp) CK(copy_fourier(h, h->cp, nullptr, cp, 0, d.nyp));
     CK(cudaStreamSynchronize(h->st));
@@ -1013,6 +1045,7 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     ca.store_phi = 0;             // phi stays where REM_DIV_CHAN alone puts it
     ca.nan_flag = h->d_nan;
     ca.mean_split = h->fp32 ? 1 : 0;
+    ca.pair_blocked = h->pb ? 1 : 0;
     ca.jlo_prod = h->jlo_prod;
     {
         ProfScope ps(h, DIABLO_KERNEL_COLUMN);

@@ -27,6 +27,16 @@ struct Dims {
     __host__ __device__ size_t splane() const { return (size_t)nkzp * ldx; }
 };
 
+// Offset of element (plane J, column g = m*ldx + kx) within one field of a
+// spectral array, in the S layout or in the pair-blocked layout that CF
+// takes on the Fourier-space path: column pairs (g, g+1) with g even, each
+// pair's NY+2 rows contiguous ([pair][J][2]), so that the column kernel,
+// which handles one pair per block and is CF's only reader and writer there,
+// reads and writes it as one contiguous run.
+__host__ __device__ __forceinline__ size_t spec_at(const Dims& d, bool pair_blocked, int J, size_t g) {
+    return pair_blocked ? (g >> 1) * (size_t)(2 * d.nyp) + (size_t)J * 2 + (g & 1) : (size_t)J * d.splane() + g;
+}
+
 // Everything K4 (the column kernel) needs besides the arrays.
 struct CnArgs {
     Dims d;
@@ -87,6 +97,7 @@ struct ColArgs {
     int update_cp;        // CP += phi/h on J = 2..NY
     int store_phi;
     int* nan_flag;        // set to 1 when a new CU value is not finite (may be null)
+    int pair_blocked;     // CF is in the pair-blocked layout (spec_at)
     int mean_split;       // the nonlinear term lacks the mean x mean products: add them to
                           // the (0,0) mode in FP64 on the product planes jlo_prod..NY
     int jlo_prod;
