@@ -294,10 +294,22 @@ __global__ void __launch_bounds__(256) k_cn_part(CoefParams c, int RC, double* _
     }
 }
 
+CoefParams make_coef(const Dims& d, const CnArgs& a, const int* bc_type, const double* bc_c1);
+
 cudaError_t launch_cn_part(const Dims& d, const CnArgs& a, double* tabs, double* bcv, signed char* kind,
                            const int* bc_type, const double* bc_c1, cudaStream_t st) {
     const int RC = part_rows(d.nyp);
     if (RC == 0) return cudaErrorInvalidValue;
+    const CoefParams c = make_coef(d, a, bc_type, bc_c1);
+    const int npr = NPART * RC;
+    const size_t smem =
+        sizeof(double) * ((size_t)4 * d.nf * npr + (size_t)d.nf * NPART * 6) + (size_t)d.nf * npr;
+    cudaFuncSetAttribute(k_cn_part, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_cn_part<<<1, 256, smem, st>>>(c, RC, tabs, bcv, kind);
+    return cudaGetLastError();
+}
+
+CoefParams make_coef(const Dims& d, const CnArgs& a, const int* bc_type, const double* bc_c1) {
     CoefParams c;
     c.d = d;
     c.dy = a.dy;
@@ -314,12 +326,7 @@ cudaError_t launch_cn_part(const Dims& d, const CnArgs& a, double* tabs, double*
         c.bc_c1[f][0] = bc_c1[2 * f];
         c.bc_c1[f][1] = bc_c1[2 * f + 1];
     }
-    const int npr = NPART * RC;
-    const size_t smem =
-        sizeof(double) * ((size_t)4 * d.nf * npr + (size_t)d.nf * NPART * 6) + (size_t)d.nf * npr;
-    cudaFuncSetAttribute(k_cn_part, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_cn_part<<<1, 256, smem, st>>>(c, RC, tabs, bcv, kind);
-    return cudaGetLastError();
+    return c;
 }
 
 // ---------------------------------------------------------------------------
@@ -334,8 +341,8 @@ cudaError_t launch_cn_part(const Dims& d, const CnArgs& a, double* tabs, double*
 // each thread issuing the loads of all its rows before it uses any.
 // ---------------------------------------------------------------------------
 template <int NW, int RC, typename TN, bool PB>
-__global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 1)
-k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs, int tstride) {
+__device__ __forceinline__ void colpart_body(const ColArgs& A, const TN* __restrict__ nl,
+                                             const double* __restrict__ tabs, int tstride, unsigned bx) {
     constexpr int NROW = NPART * RC;
     constexpr int NT = 32 * NW;
     constexpr int NTHMAX = NW / 2 - 3 < 4 ? NW / 2 - 3 : 4;
@@ -355,7 +362,7 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const size_t ps = d.splane();
     const size_t fs = ps * nyp;
-    const size_t g0 = (size_t)blockIdx.x * 2;
+    const size_t g0 = (size_t)bx * 2;
     const bool proj = A.project != 0;
     const bool rk1 = a.rk_step > 1;
     auto slot = [](int f, int j, int c) { return ((size_t)f * NROW + j) * 2 + c; };
@@ -698,6 +705,21 @@ k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs,
     if (bad && A.nan_flag) atomicOr(A.nan_flag, 1);
 }
 
+template <int NW, int RC, typename TN, bool PB>
+__global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 1)
+k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs, int tstride) {
+    colpart_body<NW, RC, TN, PB>(A, nl, tabs, tstride, blockIdx.x);
+}
+
+// Batched form: instance blockIdx.y of a group of equal shape.
+template <int NW, int RC, typename TN, bool PB>
+__global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 1)
+k_colpart_b(const ColJob* __restrict__ jobs, int tstride) {
+    const ColJob& j = jobs[blockIdx.y];
+    const ColArgs A = j.A;
+    colpart_body<NW, RC, TN, PB>(A, reinterpret_cast<const TN*>(j.nl), j.tabs, tstride, blockIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // Partition factors of every column's phi system (the REM_DIV_CHAN rows,
 // which depend on the grid and on KX^2+KZ^2 only): the reduced system of
@@ -1016,6 +1038,37 @@ cudaError_t launch_colpart(const ColArgs& a, const TN* nl, const double* tabs, c
     return cudaGetLastError();
 }
 
+template <typename TN>
+cudaError_t launch_colpart_b(const Dims& d, const ColJob* jobs, int ninst, bool pair_blocked, cudaStream_t st) {
+    const int RC = part_rows(d.nyp);
+    const size_t smem = colpart_smem<TN>(d);
+    const int tstride = (int)part_table_doubles(d.nyp);
+    dim3 grid((unsigned)(d.splane() / 2), (unsigned)ninst);
+    auto go = [&](auto kern, int nw) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 32 * nw, smem, st>>>(jobs, tstride);
+    };
+#define DGPU_RC_PB(NW, R)                                                       \
+    if (pair_blocked) go(k_colpart_b<NW, R, TN, true>, NW);                     \
+    else go(k_colpart_b<NW, R, TN, false>, NW);
+#define DGPU_RC_CASES(NW)                                        \
+    switch (RC) {                                                \
+        case 3: DGPU_RC_PB(NW, 3) break;                         \
+        case 5: DGPU_RC_PB(NW, 5) break;                         \
+        case 9: DGPU_RC_PB(NW, 9) break;                         \
+        case 17: DGPU_RC_PB(NW, 17) break;                       \
+        default: return cudaErrorInvalidValue;                   \
+    }
+    if (d.nf <= 4) { DGPU_RC_CASES(8) }
+    else if (d.nf <= 8) { DGPU_RC_CASES(16) }
+    else return cudaErrorInvalidValue;
+#undef DGPU_RC_CASES
+#undef DGPU_RC_PB
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_colpart_b<cpx<float>>(const Dims&, const ColJob*, int, bool, cudaStream_t);
+template cudaError_t launch_colpart_b<cpx<double>>(const Dims&, const ColJob*, int, bool, cudaStream_t);
 template cudaError_t launch_colpart<cpx<float>>(const ColArgs&, const cpx<float>*, const double*, cudaStream_t);
 template cudaError_t launch_colpart<cpx<double>>(const ColArgs&, const cpx<double>*, const double*, cudaStream_t);
 template size_t colpart_smem<cpx<float>>(const Dims&);

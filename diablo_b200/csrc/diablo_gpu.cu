@@ -58,8 +58,12 @@ struct Handle {
     double* d_me = nullptr;       // [4][nyp] mean profiles for the statistics
     double* d_sums = nullptr;     // [9][nyp] plane sums of the statistics
     double* d_msums = nullptr;    // [4 + 3 N_TH][nyp] plane sums of the mean.h5 / tke.h5 profiles, then [nyp] 1/(GY(j+1)-GY(j-1))
-    double* bcv = nullptr;        // [nf][nyp] BC-row values of the (0,0) mode
-    double* d_tabs = nullptr;     // [nf][part_table_doubles] CN partition factors
+    double* bcv = nullptr;        // [3][nf][nyp] BC-row values of the (0,0) mode, per RK substage
+    double* d_tabs = nullptr;     // [3][nf][part_table_doubles] CN partition factors, per RK substage
+    // The CN rows depend on the grid, the parameters and TEMP1 = NU*H_BAR/2
+    // only: the factors of substage r stay valid while TEMP1 is tab_temp1[r].
+    bool tab_ok[3] = {false, false, false};
+    double tab_temp1[3] = {0.0, 0.0, 0.0};
     double* d_phitab = nullptr;   // [column][phi_table_doubles/column] phi partition factors
     int* d_nan = nullptr;         // set by the kernels that write CU when a value is not finite
     // user right-hand-side hooks (USER_RHS_CHAN_FOURIER / _PHYSICAL), their
@@ -490,11 +494,11 @@ int diablo_gpu_create(const diablo_params* p, const double* gy, const double* gy
     if (e == cudaSuccess) e = dmalloc((void**)&h->gsc, sb);
     if (e == cudaSuccess) e = dmalloc(&h->xb, sizeof(double2) * h->x_field * d.nf);
     if (e == cudaSuccess) e = dmalloc(&h->yb, sizeof(double2) * h->x_field * d.np);
-    if (e == cudaSuccess) e = dmalloc((void**)&h->d_tabs, sizeof(double) * part_table_doubles(d.nyp) * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->d_tabs, sizeof(double) * part_table_doubles(d.nyp) * d.nf * 3);
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_phitab, sizeof(double) * phi_table_doubles(d));
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_nan, sizeof(int));
-    if (e == cudaSuccess) e = dmalloc((void**)&h->bcv, sizeof(double) * nyp * d.nf);
-    if (e == cudaSuccess) e = dmalloc((void**)&h->kind, nyp * d.nf);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->bcv, sizeof(double) * nyp * d.nf * 3);
+    if (e == cudaSuccess) e = dmalloc((void**)&h->kind, nyp * d.nf * 3);
     if (e == cudaSuccess) e = dmalloc((void**)&h->dtmin, sizeof(double));
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_k2, sizeof(double) * d.splane());
     if (e == cudaSuccess) e = dmalloc((void**)&h->d_rows, sizeof(double) * RT_COUNT * nyp);
@@ -742,6 +746,48 @@ static CnArgs substage_args(Handle* h, int rk_step, double time, const double* h
     return a;
 }
 
+// The column kernel's arguments of one Fourier-space substage (no LES); with
+// cfl the projection waits until COURANT has run.
+static ColArgs dns_col_args(Handle* h, const CnArgs& a, bool cfl) {
+    ColArgs ca;
+    ca.cn = a;
+    ca.k2 = h->d_k2;
+    ca.rows = h->d_rows;
+    ca.phitab = h->d_phitab;
+    ca.phi = h->phi;
+    ca.inv_h = 1.0 / a.temp4;
+    ca.project = cfl ? 0 : 1;     // COURANT sees the velocity before the projection
+    ca.update_cp = 1;
+    ca.store_phi = 0;             // phi stays where REM_DIV_CHAN alone puts it
+    ca.nan_flag = h->d_nan;
+    ca.pair_blocked = h->pb ? 1 : 0;
+    ca.mean_split = h->fp32 ? 1 : 0;
+    ca.jlo_prod = h->jlo_prod;
+    return ca;
+}
+
+// CN rows and partition factors of substage r (k_cn_part) into that
+// substage's slot, unless the slot already holds them for this TEMP1; points
+// a.bcv / a.kind at the slot and returns the factor tables in *tabs.
+static int ensure_cn_tables(Handle* h, CnArgs& a, int r, const double** tabs) {
+    const Dims& d = h->d;
+    const size_t tsz = part_table_doubles(d.nyp) * d.nf, rsz = (size_t)d.nyp * d.nf;
+    double* t = h->d_tabs + (size_t)r * tsz;
+    a.bcv = h->bcv + (size_t)r * rsz;
+    a.kind = h->kind + (size_t)r * rsz;
+    *tabs = t;
+    if (h->tab_ok[r] && h->tab_temp1[r] == a.temp1) return DIABLO_OK;
+    {
+        ProfScope ps(h, DIABLO_KERNEL_CN_COEF);
+        CK(launch_cn_part(d, a, t, const_cast<double*>(a.bcv), const_cast<signed char*>(a.kind), h->bc_type, h->bc_c1,
+                          h->st));
+    }
+    h->launches += 1;
+    h->tab_ok[r] = true;
+    h->tab_temp1[r] = a.temp1;
+    return DIABLO_OK;
+}
+
 // Spectral fields [0,nfld) of S (stride s_field) -> physical fields of P
 // (stride pf), planes j0..j0+np-1, FP64.
 static cudaError_t les_to_phys(Handle* h, const double2* S, int nfld, double* P, int j0, int np) {
@@ -982,11 +1028,7 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
         const bool sgs = !p.create_new_flow || time_step > 100;
         if (sgs || h->nut_set) return les_substage(h, rk_step, time_step, time, delta_t, h_bar, beta_bar, zeta_bar, sgs);
     }
-    // constants of channel.f:77-81
-    const double TEMP1 = p.nu * h_bar[r] / 2.0;
-    const double TEMP3 = zeta_bar[r] * h_bar[r];
-    const double TEMP4 = h_bar[r];
-    const double TEMP5 = beta_bar[r] * h_bar[r];
+    const double TEMP4 = h_bar[r];       // channel.f:77-81; the others are formed by substage_args
     int rc;
     bool user = false;    // USER_RHS_CHAN_FOURIER / _PHYSICAL (channel.f:297, 578)
     if ((rc = user_rhs(h, rk_step, time_step, time, nullptr, &user))) return rc;
@@ -999,60 +1041,17 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
         CK(cudaGetLastError());
         h->launches += 1;
     }
-    CnArgs a;
-    a.d = d;
-    a.cu = h->cu;
-    a.cf = h->cf;
-    a.cp = h->cp;
-    a.kx = h->d_kx;
-    a.kz = h->d_kz;
-    a.dy = h->d_dy;
-    a.dyf = h->d_dyf;
-    a.bcv = h->bcv;
-    a.kind = h->kind;
-    for (int f = 0; f < MAXF; ++f) { a.cf_lo[f] = 2; a.cf_hi[f] = d.ny; a.cb_lo[f] = 1; }
-    for (int n = 0; n < d.nth; ++n) {
-        a.cf_lo[3 + n] = h->jstart_th[n];
-        a.cf_hi[3 + n] = h->jend_th[n];
-        a.cb_lo[3 + n] = h->jstart_th[n] - 1;
-    }
-    a.temp1 = TEMP1; a.temp3 = TEMP3; a.temp4 = TEMP4; a.temp5 = TEMP5;
-    a.nu = p.nu; a.beta = p.beta; a.nu_v_scale = p.nu_v_scale; a.i_ro = p.i_ro;
-    a.grav_x = p.grav_x; a.grav_y = p.grav_y; a.grav_z = p.grav_z;
-    for (int n = 0; n < 4; ++n) {
-        a.ri[n] = n < d.nth ? p.ri[n] : 0.0;
-        a.pr[n] = n < d.nth ? p.pr[n] : 1.0;
-        a.drhodx[n] = n < d.nth ? p.drhodx[n] : 0.0;
-        a.drhodz[n] = n < d.nth ? p.drhodz[n] : 0.0;
-    }
-    a.forcing = 0.0;
-    if (p.f_type == 1) a.forcing = TEMP4 * p.px0;
-    else if (p.f_type == 2) a.forcing = TEMP4 * (p.px0 + p.amp_omega0 * std::cos(p.omega0 * time));
-    a.rk_step = rk_step;
-    a.store_cf = 1;
-    { ProfScope ps(h, DIABLO_KERNEL_CN_COEF);
-      CK(launch_cn_part(d, a, h->d_tabs, h->bcv, h->kind, h->bc_type, h->bc_c1, h->st)); }
+    CnArgs a = substage_args(h, rk_step, time, h_bar, beta_bar, zeta_bar);
+    const double* tabs = nullptr;
+    if ((rc = ensure_cn_tables(h, a, r, &tabs))) return rc;
     const bool cfl = p.variable_dt && rk_step == 3 && (time_step % p.update_dt) == 0;
-    ColArgs ca;
-    ca.cn = a;
-    ca.k2 = h->d_k2;
-    ca.rows = h->d_rows;
-    ca.phitab = h->d_phitab;
-    ca.phi = h->phi;
-    ca.inv_h = 1.0 / TEMP4;
-    ca.project = cfl ? 0 : 1;     // COURANT sees the velocity before the projection
-    ca.update_cp = 1;
-    ca.store_phi = 0;             // phi stays where REM_DIV_CHAN alone puts it
-    ca.nan_flag = h->d_nan;
-    ca.mean_split = h->fp32 ? 1 : 0;
-    ca.pair_blocked = h->pb ? 1 : 0;
-    ca.jlo_prod = h->jlo_prod;
+    const ColArgs ca = dns_col_args(h, a, cfl);
     {
         ProfScope ps(h, DIABLO_KERNEL_COLUMN);
-        if (h->fp32) CK(launch_colpart<cpx<float>>(ca, (const cpx<float>*)h->nl, h->d_tabs, h->st));
-        else CK(launch_colpart<cpx<double>>(ca, (const cpx<double>*)h->nl, h->d_tabs, h->st));
+        if (h->fp32) CK(launch_colpart<cpx<float>>(ca, (const cpx<float>*)h->nl, tabs, h->st));
+        else CK(launch_colpart<cpx<double>>(ca, (const cpx<double>*)h->nl, tabs, h->st));
     }
-    h->launches += 2;
+    h->launches += 1;
     if (!cfl) return DIABLO_OK;
     // COURANT at the last substage (channel.f:1037-1040), then REM_DIV and the
     // pressure update with the h of this substage
@@ -1596,7 +1595,7 @@ int diablo_gpu_autotune(void* handle, int* prod_chunk, int* zf_planes) {
     if (e != cudaSuccess) rc = fail(DIABLO_ECUDA, std::string("autotune: ") + cudaGetErrorString(e));
     if (!rc) {
         // coordinate search: products chunk, then z-forward planes per block
-        const int chunks[] = {8, 16, 32, 64}, planes[] = {4, 8, 16};
+        const int chunks[] = {4, 8, 16, 32, 64}, planes[] = {4, 8, 16};
         float best = 1e30f;
         int bc = h->prod_chunk, bz = h->zf_planes;
         for (int c : chunks) {
@@ -1631,11 +1630,25 @@ int diablo_gpu_autotune(void* handle, int* prod_chunk, int* zf_planes) {
 }  // extern "C"
 
 namespace {
+// Instances of equal shape and precision advance together: each kernel of the
+// substage is one launch over the whole group, reading every instance's
+// arrays and parameters from device tables (InstPtrs, ColJob).
+struct BatchGroup {
+    std::vector<Handle*> hs;
+    std::vector<double> temp1;            // [n][3] TEMP1 of each instance's substages
+    std::vector<double> dt;               // [n] each instance's time step
+    InstPtrs* d_ip = nullptr;             // [n]
+    ColJob* d_col = nullptr;              // [3][n], one set per RK substage
+    int jlo_min = 0;
+    cudaStream_t st = nullptr;            // the group's branch of the graph
+    cudaEvent_t join = nullptr;
+};
+
 struct Batch {
     std::vector<Handle*> hs;
+    std::vector<BatchGroup> groups;
     cudaStream_t origin = nullptr;
     cudaEvent_t fork = nullptr;
-    std::vector<cudaEvent_t> join;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -1644,10 +1657,43 @@ void free_batch(Batch* b) {
     if (!b) return;
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
-    for (cudaEvent_t ev : b->join) if (ev) cudaEventDestroy(ev);
+    for (BatchGroup& g : b->groups) {
+        if (g.d_ip) cudaFree(g.d_ip);
+        if (g.d_col) cudaFree(g.d_col);
+        if (g.join) cudaEventDestroy(g.join);
+        if (g.st) cudaStreamDestroy(g.st);
+    }
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->origin) cudaStreamDestroy(b->origin);
     delete b;
+}
+
+// One RK3 step of a group on its stream: per substage the four kernels of the
+// Fourier-space path (channel.f:62-1073 without COURANT), each once for all
+// instances.  The CN factors of the batch's fixed time steps are built when
+// the batch is made (ensure_cn_tables) and checked before every launch.
+template <typename T>
+cudaError_t batch_group_step(BatchGroup& g) {
+    Handle* h0 = g.hs[0];
+    const Dims& d = h0->d;
+    const int n = (int)g.hs.size();
+    const bool f = std::is_same<T, float>::value;
+    const void* twn = f ? h0->twn_f : h0->twn_d;
+    const void* twm = f ? h0->twm_f : h0->twm_d;
+    const void* twz = f ? h0->twz_f : h0->twz_d;
+    cudaError_t e = cudaSuccess;
+    for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
+        e = launch_zinv_b<T>(d, g.d_ip, n, h0->s_field, h0->x_field, h0->pz, twz, g.st, f ? 1 : 0);
+        if (e != cudaSuccess) break;
+        if (f && products_hw_supported(d))
+            e = launch_products_hw_b(d, g.d_ip, n, g.jlo_min, d.ny, h0->prod_chunk, twm, twn, g.st, h0->s_field);
+        else
+            e = launch_products_b<T>(d, g.d_ip, n, g.jlo_min, d.ny, h0->prod_chunk, h0->pm, twm, twn, g.st, f ? 1 : 0,
+                                     h0->s_field);
+        if (e == cudaSuccess) e = launch_zfwd_nl_b<T>(d, g.d_ip, n, g.jlo_min, d.ny, h0->zf_planes, h0->pz, twz, g.st);
+        if (e == cudaSuccess) e = launch_colpart_b<cpx<T>>(d, g.d_col + (size_t)r * n, n, h0->pb, g.st);
+    }
+    return e;
 }
 }  // namespace
 
@@ -1665,34 +1711,82 @@ int diablo_gpu_batch_create(void* const* handles, const double* delta_t, int n, 
         if (h->urhs_fn[0] || h->urhs_fn[1]) return fail(DIABLO_ENOTSUP, "batched instances cannot have user right-hand sides");
         if (h->profiling) return fail(DIABLO_EINVAL, "batched instance with profiling on");
         if (!(delta_t[i] > 0.0)) return fail(DIABLO_EINVAL, "batched instance with delta_t <= 0");
+        for (int k = 0; k < i; ++k)
+            if (handles[k] == handles[i]) return fail(DIABLO_EINVAL, "an instance appears twice in the batch");
     }
     Batch* b = new Batch();
     auto bail = [&](int code, const std::string& msg) { free_batch(b); return fail(code, msg); };
-    for (int i = 0; i < n; ++i) b->hs.push_back((Handle*)handles[i]);
+    // groups of equal shape, number of scalars and precision, in first-seen order
+    std::vector<double> dts;
+    for (int i = 0; i < n; ++i) {
+        Handle* h = (Handle*)handles[i];
+        b->hs.push_back(h);
+        BatchGroup* g = nullptr;
+        for (BatchGroup& q : b->groups) {
+            const Handle* r = q.hs[0];
+            if (r->d.nx == h->d.nx && r->d.ny == h->d.ny && r->d.nz == h->d.nz && r->d.nth == h->d.nth &&
+                r->fp32 == h->fp32)
+                g = &q;
+        }
+        if (!g) { b->groups.emplace_back(); g = &b->groups.back(); }
+        g->hs.push_back(h);
+    }
     cudaError_t e = cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
-    b->join.assign(n, nullptr);
-    for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
     for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaStreamSynchronize(b->hs[i]->st);
-    if (e != cudaSuccess) return bail(DIABLO_ECUDA, std::string("batch set-up: ") + cudaGetErrorString(e));
+    const double bb[3] = {1.0, 25.0 / 8.0, 9.0 / 4.0}, zb[3] = {0.0, -17.0 / 8.0, -5.0 / 4.0};
+    for (BatchGroup& g : b->groups) {
+        if (e != cudaSuccess) break;
+        const int m = (int)g.hs.size();
+        std::vector<InstPtrs> ip(m);
+        std::vector<ColJob> col(3 * (size_t)m);
+        g.temp1.assign(3 * (size_t)m, 0.0);
+        g.dt.assign(m, 0.0);
+        g.jlo_min = g.hs[0]->jlo_prod;
+        for (int i = 0; i < m; ++i) {
+            Handle* h = g.hs[i];
+            ip[i] = InstPtrs{h->cu, h->xb, h->yb, h->nl, h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->jlo_prod};
+            if (h->jlo_prod < g.jlo_min) g.jlo_min = h->jlo_prod;
+            double dt = 0.0;
+            for (int k = 0; k < n; ++k)
+                if (handles[k] == h) dt = delta_t[k];
+            g.dt[i] = dt;
+            const double hb[3] = {dt * 8.0 / 15.0, dt * 2.0 / 15.0, dt * 5.0 / 15.0};
+            for (int r = 0; r < 3; ++r) {
+                CnArgs a = substage_args(h, r + 1, 0.0, hb, bb, zb);
+                const double* tabs = nullptr;
+                const int rc = ensure_cn_tables(h, a, r, &tabs);
+                if (rc) { free_batch(b); return rc; }
+                g.temp1[(size_t)i * 3 + r] = a.temp1;
+                col[(size_t)r * m + i] = ColJob{dns_col_args(h, a, false), h->nl, tabs};
+            }
+            if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+        }
+        if (e == cudaSuccess) e = cudaMalloc((void**)&g.d_ip, sizeof(InstPtrs) * m);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&g.d_col, sizeof(ColJob) * col.size());
+        // ordered on the batch's stream and waited for below, before any graph launch reads them
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(g.d_ip, ip.data(), sizeof(InstPtrs) * m, cudaMemcpyHostToDevice, b->origin);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(g.d_col, col.data(), sizeof(ColJob) * col.size(), cudaMemcpyHostToDevice, b->origin);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->origin);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess)
+        return bail(e == cudaErrorMemoryAllocation ? DIABLO_ENOMEM : DIABLO_ECUDA,
+                    std::string("batch set-up: ") + cudaGetErrorString(e));
     e = cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeRelaxed);
     if (e != cudaSuccess) return bail(DIABLO_ECUDA, std::string("batch capture: ") + cudaGetErrorString(e));
-    int rc = DIABLO_OK;
-    if ((e = cudaEventRecord(b->fork, b->origin)) != cudaSuccess) rc = DIABLO_ECUDA;
-    for (int i = 0; i < n && !rc; ++i)
-        if ((e = cudaStreamWaitEvent(b->hs[i]->st, b->fork, 0)) != cudaSuccess) rc = DIABLO_ECUDA;
-    const double bb[3] = {1.0, 25.0 / 8.0, 9.0 / 4.0}, zb[3] = {0.0, -17.0 / 8.0, -5.0 / 4.0};
-    for (int i = 0; i < n && !rc; ++i) {
-        double dt = delta_t[i];
-        double hb[3] = {dt * 8.0 / 15.0, dt * 2.0 / 15.0, dt * 5.0 / 15.0};
-        for (int rk = 1; rk <= 3 && !rc; ++rk) rc = diablo_gpu_rk_chan_1(b->hs[i], rk, 1, 0.0, &dt, hb, bb, zb);
-        if (!rc && (e = cudaEventRecord(b->join[i], b->hs[i]->st)) != cudaSuccess) rc = DIABLO_ECUDA;
-        if (!rc && (e = cudaStreamWaitEvent(b->origin, b->join[i], 0)) != cudaSuccess) rc = DIABLO_ECUDA;
+    e = cudaEventRecord(b->fork, b->origin);
+    for (BatchGroup& g : b->groups) {
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(g.st, b->fork, 0);
+        if (e == cudaSuccess) e = g.hs[0]->fp32 ? batch_group_step<float>(g) : batch_group_step<double>(g);
+        if (e == cudaSuccess) e = cudaEventRecord(g.join, g.st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->origin, g.join, 0);
     }
-    const std::string msg = rc ? g_err : std::string();
     cudaError_t ee = cudaStreamEndCapture(b->origin, &b->graph);
-    if (rc) return bail(rc == DIABLO_ECUDA && msg.empty() ? DIABLO_ECUDA : rc,
-                        msg.empty() ? std::string("batch capture: ") + cudaGetErrorString(e) : msg);
+    if (e != cudaSuccess) return bail(DIABLO_ECUDA, std::string("batch capture: ") + cudaGetErrorString(e));
     if (ee != cudaSuccess) return bail(DIABLO_ECUDA, std::string("batch end capture: ") + cudaGetErrorString(ee));
     e = cudaGraphInstantiate(&b->exec, b->graph, 0);
     if (e != cudaSuccess) return bail(DIABLO_ECUDA, std::string("batch instantiate: ") + cudaGetErrorString(e));
@@ -1703,6 +1797,25 @@ int diablo_gpu_batch_create(void* const* handles, const double* delta_t, int n, 
 int diablo_gpu_batch_step(void* batch, int nsteps) {
     Batch* b = (Batch*)batch;
     if (!b || nsteps < 0) return fail(DIABLO_EINVAL, "bad batch arguments");
+    // An instance stepped on its own with another time step since the last
+    // batch step holds other CN factors: rebuild those of the batch's time step.
+    const double bb[3] = {1.0, 25.0 / 8.0, 9.0 / 4.0}, zb[3] = {0.0, -17.0 / 8.0, -5.0 / 4.0};
+    for (BatchGroup& g : b->groups)
+        for (size_t i = 0; i < g.hs.size(); ++i) {
+            Handle* h = g.hs[i];
+            bool stale = false;
+            for (int r = 0; r < 3; ++r) stale = stale || !h->tab_ok[r] || h->tab_temp1[r] != g.temp1[i * 3 + r];
+            if (!stale) continue;
+            const double dt = g.dt[i];
+            const double hb[3] = {dt * 8.0 / 15.0, dt * 2.0 / 15.0, dt * 5.0 / 15.0};
+            for (int r = 0; r < 3; ++r) {
+                CnArgs a = substage_args(h, r + 1, 0.0, hb, bb, zb);
+                const double* tabs = nullptr;
+                int rc = ensure_cn_tables(h, a, r, &tabs);
+                if (rc) return rc;
+            }
+            CK(cudaStreamSynchronize(h->st));
+        }
     for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(b->exec, b->origin));
     CK(cudaStreamSynchronize(b->origin));
     return DIABLO_OK;

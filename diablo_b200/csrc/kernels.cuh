@@ -37,6 +37,21 @@ __host__ __device__ __forceinline__ size_t spec_at(const Dims& d, bool pair_bloc
     return pair_blocked ? (g >> 1) * (size_t)(2 * d.nyp) + (size_t)J * 2 + (g & 1) : (size_t)J * d.splane() + g;
 }
 
+// Per-instance arrays of a batched launch over a group of instances of equal
+// shape (the transform kernels' *_b entries): instance i of the group reads
+// its own state, scratch and grid tables through entry i.
+struct InstPtrs {
+    const double2* cu;    // state (S layout, nf fields)
+    void* xb;             // x spectra X
+    void* yb;             // product spectra Y
+    void* nl;             // nonlinear term NL
+    const double* dy;
+    const double* dyf;
+    const double* kx;
+    const double* kz;
+    int jlo_prod;         // first product plane
+};
+
 // Everything K4 (the column kernel) needs besides the arrays.
 struct CnArgs {
     Dims d;
@@ -101,6 +116,13 @@ struct ColArgs {
     int mean_split;       // the nonlinear term lacks the mean x mean products: add them to
                           // the (0,0) mode in FP64 on the product planes jlo_prod..NY
     int jlo_prod;
+};
+
+// One instance of a batched column launch (launch_colpart_b).
+struct ColJob {
+    ColArgs A;
+    const void* nl;       // nonlinear term, the transform type
+    const double* tabs;   // CN partition tables of the substage
 };
 
 struct RemDivArgs {

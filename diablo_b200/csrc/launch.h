@@ -42,6 +42,9 @@ size_t products_hw_smem(const Dims& d);
 cudaError_t launch_products_hw(const Dims& d, const void* X, void* Y, int jlo, int jhi, int chunk, const double* dy,
                                const double* dyf, const double* kx, const void* twm, const void* twn, cudaStream_t st,
                                const double2* means, size_t means_fstride);
+// Batched form (see launch_zinv_b); the state of each instance gives the plane means.
+cudaError_t launch_products_hw_b(const Dims& d, const InstPtrs* ip, int ninst, int jlo_min, int jhi, int chunk,
+                                 const void* twm, const void* twn, cudaStream_t st, size_t means_fstride);
 
 // Per plane (zp planes per block, 0 = default): forward z transform of the 2
 // product outputs of every field,
@@ -51,6 +54,20 @@ template <typename T>
 cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int jhi, int zp,
                            const double* kx, const double* kz, const FftPlan& pz, const void* twz,
                            cudaStream_t st);
+
+// Batched forms of the three transform kernels: one launch for the ninst
+// instances of a group of equal shape, whose arrays come from the device
+// table ip (InstPtrs).  jlo_min: the smallest first product plane of the group.
+template <typename T>
+cudaError_t launch_zinv_b(const Dims& d, const InstPtrs* ip, int ninst, size_t s_fstride, size_t x_fstride,
+                          const FftPlan& pz, const void* twz, cudaStream_t st, int skip_mean);
+template <typename T>
+cudaError_t launch_products_b(const Dims& d, const InstPtrs* ip, int ninst, int jlo_min, int jhi, int chunk,
+                              const FftPlan& pm, const void* twm, const void* twn, cudaStream_t st, int mean_split,
+                              size_t means_fstride);
+template <typename T>
+cudaError_t launch_zfwd_nl_b(const Dims& d, const InstPtrs* ip, int ninst, int jlo_min, int jhi, int zp,
+                             const FftPlan& pz, const void* twz, cudaStream_t st);
 
 // Transform-API helpers (one field at a time, FP64):
 // X -> physical rows P (c2r, unnormalised, Nyquist and kx > NKX zero).
@@ -81,6 +98,9 @@ template <typename TN>
 cudaError_t launch_colpart(const ColArgs& a, const TN* nl, const double* tabs, cudaStream_t st);
 template <typename TN>
 size_t colpart_smem(const Dims& d);
+// Batched form for a group of equal shape (ColJob table on the device).
+template <typename TN>
+cudaError_t launch_colpart_b(const Dims& d, const ColJob* jobs, int ninst, bool pair_blocked, cudaStream_t st);
 cudaError_t launch_remdiv(const RemDivArgs& a, cudaStream_t st);
 
 // CFL minimum (courant.f:35-47) over planes 1..NY of the physical velocity

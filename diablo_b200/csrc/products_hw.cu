@@ -135,12 +135,11 @@ __device__ __forceinline__ Role product_role(int pw, int h, int nth) {
     return r;
 }
 
-template <int NW>
-__global__ void __launch_bounds__(32 * NW, NW <= 8 ? 3 : 1)
-k_products_hw(Dims d, const c32* __restrict__ X, c32* __restrict__ Y, int jlo, int jhi, int chunk,
-              const double* __restrict__ dy, const double* __restrict__ dyf, const double* __restrict__ kxw,
-              const c32* __restrict__ twm, const c32* __restrict__ twn, const double2* __restrict__ means,
-              size_t means_fs) {
+__device__ __forceinline__ void products_hw_body(const Dims& d, const c32* __restrict__ X, c32* __restrict__ Y, int jlo,
+                                                 int jhi, int chunk, const double* __restrict__ dy,
+                                                 const double* __restrict__ dyf, const double* __restrict__ kxw,
+                                                 const c32* __restrict__ twm, const c32* __restrict__ twn,
+                                                 const double2* __restrict__ means, size_t means_fs, uint3 bid) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ float smean[HRING][MAXF];
     const int nf = d.nf, nth = d.nth, ldx = d.ldx;
@@ -160,9 +159,10 @@ k_products_hw(Dims d, const c32* __restrict__ X, c32* __restrict__ Y, int jlo, i
         stw[e] = twm[((e & 15) * (e >> 4)) & (HM - 1)];
         stn[e] = twn[e];
     }
-    const int z = blockIdx.x;
-    const int jb = jlo + blockIdx.y * chunk;
+    const int z = bid.x;
+    const int jb = jlo + bid.y * chunk;
     const int je = min(jb + chunk - 1, jhi);
+    if (jb > jhi) return;                          // batched form: past this instance's planes
     const size_t xrow = (size_t)d.nz * ldx;       // plane stride of X / Y
     const size_t xf = (size_t)d.nyp * xrow;       // field stride of X / Y
     const size_t ps = d.splane();
@@ -315,6 +315,25 @@ k_products_hw(Dims d, const c32* __restrict__ X, c32* __restrict__ Y, int jlo, i
     }
 }
 
+template <int NW>
+__global__ void __launch_bounds__(32 * NW, NW <= 8 ? 3 : 1)
+k_products_hw(Dims d, const c32* __restrict__ X, c32* __restrict__ Y, int jlo, int jhi, int chunk,
+              const double* __restrict__ dy, const double* __restrict__ dyf, const double* __restrict__ kxw,
+              const c32* __restrict__ twm, const c32* __restrict__ twn, const double2* __restrict__ means,
+              size_t means_fs) {
+    products_hw_body(d, X, Y, jlo, jhi, chunk, dy, dyf, kxw, twm, twn, means, means_fs, blockIdx);
+}
+
+// Batched form: instance blockIdx.z of a group of equal shape.
+template <int NW>
+__global__ void __launch_bounds__(32 * NW, NW <= 8 ? 3 : 1)
+k_products_hw_b(const InstPtrs* __restrict__ ip, Dims d, int jhi, int chunk, const c32* __restrict__ twm,
+                const c32* __restrict__ twn, size_t means_fs) {
+    const InstPtrs q = ip[blockIdx.z];
+    products_hw_body(d, reinterpret_cast<const c32*>(q.xb), reinterpret_cast<c32*>(q.yb), q.jlo_prod, jhi, chunk, q.dy,
+                     q.dyf, q.kx, twm, twn, q.cu, means_fs, make_uint3(blockIdx.x, blockIdx.y, 0));
+}
+
 }  // namespace
 
 bool products_hw_supported(const Dims& d) { return d.nx == 2 * HM && d.ldx == 16 * HD && d.nf <= MAXF; }
@@ -341,6 +360,22 @@ cudaError_t launch_products_hw(const Dims& d, const void* X, void* Y, int jlo, i
         return cudaGetLastError();
     };
     return nw <= 8 ? go(k_products_hw<8>) : go(k_products_hw<14>);
+}
+
+cudaError_t launch_products_hw_b(const Dims& d, const InstPtrs* ip, int ninst, int jlo_min, int jhi, int chunk,
+                                 const void* twm, const void* twn, cudaStream_t st, size_t means_fstride) {
+    if (jhi < jlo_min) return cudaSuccess;
+    if (!products_hw_supported(d)) return cudaErrorInvalidValue;
+    const size_t smem = products_hw_smem(d);
+    dim3 grid(d.nz, (jhi - jlo_min + chunk) / chunk, ninst);
+    const int nw = block_warps(d.nf);
+    auto go = [&](auto kern) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, 32 * nw, smem, st>>>(ip, d, jhi, chunk, (const c32*)twm, (const c32*)twn, means_fstride);
+        return cudaGetLastError();
+    };
+    return nw <= 8 ? go(k_products_hw_b<8>) : go(k_products_hw_b<14>);
 }
 
 }  // namespace dgpu

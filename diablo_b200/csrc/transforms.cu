@@ -76,16 +76,16 @@ __device__ __forceinline__ void col_fft(cpx<T>* buf, const FftPlan& P, const cpx
 // With skip_mean the (kx,kz) = (0,0) mode (the plane mean) is left out, so X
 // holds the fluctuation about each plane's mean.
 template <typename T, int NC, int TX>
-__global__ void __launch_bounds__(256) k_zinv(Dims d, const double2* __restrict__ S, size_t s_fstride,
-                                              cpx<T>* __restrict__ X, size_t x_fstride, int j0,
-                                              FftPlan pz, const cpx<T>* __restrict__ twz, int skip_mean) {
+__device__ __forceinline__ void zinv_body(const Dims& d, const double2* __restrict__ S, size_t s_fstride,
+                                          cpx<T>* __restrict__ X, size_t x_fstride, int j0, const FftPlan& pz,
+                                          const cpx<T>* __restrict__ twz, int skip_mean, uint3 bid) {
     extern __shared__ unsigned char smem_raw[];
     cpx<T>* buf = reinterpret_cast<cpx<T>*>(smem_raw);   // [nz][TX]
     const int nz = NC > 0 ? NC : d.nz;
     const int nkz = nz / 3, nkzt = 2 * nkz + 1;
-    const int kx0 = blockIdx.x * TX;
-    const int J = j0 + blockIdx.y;
-    const int f = blockIdx.z;
+    const int kx0 = bid.x * TX;
+    const int J = j0 + bid.y;
+    const int f = bid.z;
     const double2* src = S + (size_t)f * s_fstride + (size_t)J * d.splane();
     for (int e = threadIdx.x; e < nz * TX; e += 256) {
         const int z = e / TX, c = e % TX;
@@ -104,6 +104,23 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, const double2* __restrict_
         const int z = e / TX, c = e % TX;
         dst[(size_t)z * d.ldx + kx0 + c] = buf[e];
     }
+}
+
+template <typename T, int NC, int TX>
+__global__ void __launch_bounds__(256) k_zinv(Dims d, const double2* __restrict__ S, size_t s_fstride,
+                                              cpx<T>* __restrict__ X, size_t x_fstride, int j0,
+                                              FftPlan pz, const cpx<T>* __restrict__ twz, int skip_mean) {
+    zinv_body<T, NC, TX>(d, S, s_fstride, X, x_fstride, j0, pz, twz, skip_mean, blockIdx);
+}
+
+// Batched form: instance blockIdx.z / nfields of a group of equal shape.
+template <typename T, int NC, int TX>
+__global__ void __launch_bounds__(256) k_zinv_b(const InstPtrs* __restrict__ ip, int nfields, Dims d,
+                                                size_t s_fstride, size_t x_fstride, FftPlan pz,
+                                                const cpx<T>* __restrict__ twz, int skip_mean) {
+    const InstPtrs q = ip[blockIdx.z / nfields];
+    zinv_body<T, NC, TX>(d, q.cu, s_fstride, reinterpret_cast<cpx<T>*>(q.xb), x_fstride, 0, pz, twz, skip_mean,
+                         make_uint3(blockIdx.x, blockIdx.y, blockIdx.z % nfields));
 }
 
 // ---------------------------------------------------------------------------
@@ -184,14 +201,12 @@ __device__ __forceinline__ int field_sources(int q, int* sp, bool* sx) {
 }
 
 template <typename T, int MC>
-__global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __restrict__ X,
-                                                     cpx<T>* __restrict__ Y, int jlo, int jhi, int chunk,
-                                                     int group, const double* __restrict__ dy,
-                                                     const double* __restrict__ dyf,
-                                                     const double* __restrict__ kxw, FftPlan pm,
-                                                     const cpx<T>* __restrict__ twm,
-                                                     const cpx<T>* __restrict__ twn,
-                                                     const double2* __restrict__ means, size_t means_fs) {
+__device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __restrict__ X, cpx<T>* __restrict__ Y,
+                                              int jlo, int jhi, int chunk, int group, const double* __restrict__ dy,
+                                              const double* __restrict__ dyf, const double* __restrict__ kxw,
+                                              const FftPlan& pm, const cpx<T>* __restrict__ twm,
+                                              const cpx<T>* __restrict__ twn, const double2* __restrict__ means,
+                                              size_t means_fs, uint3 bid) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ T smean[RING][MAXF];   // plane means of the ring planes (zero without mean split)
     const int M = MC > 0 ? MC : d.nx / 2;
@@ -212,9 +227,10 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
     twm = stw;
     twn = stw + M;
     __syncthreads();
-    const int z = blockIdx.x;
-    const int jb = jlo + blockIdx.y * chunk;
+    const int z = bid.x;
+    const int jb = jlo + bid.y * chunk;
     const int je = min(jb + chunk - 1, jhi);
+    if (jb > jhi) return;                                 // batched form: past this instance's planes
     const size_t xrow = (size_t)d.nz * d.ldx;            // plane stride of X / Y
     const size_t xf = (size_t)d.nyp * xrow;              // field stride of X / Y
     const T inv_nx = T(1.0 / (double)nx);
@@ -397,6 +413,30 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
     }
 }
 
+template <typename T, int MC>
+__global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __restrict__ X,
+                                                     cpx<T>* __restrict__ Y, int jlo, int jhi, int chunk,
+                                                     int group, const double* __restrict__ dy,
+                                                     const double* __restrict__ dyf,
+                                                     const double* __restrict__ kxw, FftPlan pm,
+                                                     const cpx<T>* __restrict__ twm,
+                                                     const cpx<T>* __restrict__ twn,
+                                                     const double2* __restrict__ means, size_t means_fs) {
+    products_body<T, MC>(d, X, Y, jlo, jhi, chunk, group, dy, dyf, kxw, pm, twm, twn, means, means_fs, blockIdx);
+}
+
+// Batched form: instance blockIdx.z of a group of equal shape.
+template <typename T, int MC>
+__global__ void __launch_bounds__(256, 2) k_products_b(const InstPtrs* __restrict__ ip, Dims d, int jhi, int chunk,
+                                                       int group, FftPlan pm, const cpx<T>* __restrict__ twm,
+                                                       const cpx<T>* __restrict__ twn, int mean_split,
+                                                       size_t means_fs) {
+    const InstPtrs q = ip[blockIdx.z];
+    products_body<T, MC>(d, reinterpret_cast<const cpx<T>*>(q.xb), reinterpret_cast<cpx<T>*>(q.yb), q.jlo_prod, jhi,
+                         chunk, group, q.dy, q.dyf, q.kx, pm, twm, twn, mean_split ? q.cu : nullptr, means_fs,
+                         make_uint3(blockIdx.x, blockIdx.y, 0));
+}
+
 // ---------------------------------------------------------------------------
 // K3: per plane, kx tile and field: forward z transform of the two product
 // outputs that feed the field, kz packing with 1/NZ, and the derivative
@@ -427,21 +467,21 @@ template <>
 struct ZfTile<double> { static constexpr int TX = 4; };
 
 template <typename T, int NC, int TX>
-__global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __restrict__ Y,
-                                                    cpx<T>* __restrict__ NL, int jlo, int jhi, int zp,
-                                                    const double* __restrict__ kxw,
-                                                    const double* __restrict__ kzw, FftPlan pz,
-                                                    const cpx<T>* __restrict__ twz) {
+__device__ __forceinline__ void zfwd_nl_body(const Dims& d, const cpx<T>* __restrict__ Y, cpx<T>* __restrict__ NL,
+                                             int jlo, int jhi, int zp, const double* __restrict__ kxw,
+                                             const double* __restrict__ kzw, const FftPlan& pz,
+                                             const cpx<T>* __restrict__ twz, uint3 bid) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nz = NC > 0 ? NC : d.nz;
     const int nkz = nz / 3, nkzt = 2 * nkz + 1;
     constexpr int QA = NC > 0 ? ((2 * (NC / 3) + 1) * TX + 255) / 256 : 1;
     cpx<T>* bufs = reinterpret_cast<cpx<T>*>(smem_raw);          // [2][nz][TX]
     cpx<T>* sacc = bufs + 2 * (size_t)nz * TX;                    // run-time path: [nkzt][TX]
-    const int kx0 = blockIdx.x * TX;
-    const int f = blockIdx.z;
-    const int J0 = jlo + blockIdx.y * zp;
+    const int kx0 = bid.x * TX;
+    const int f = bid.z;
+    const int J0 = jlo + bid.y * zp;
     const int nplanes = min(zp, jhi - J0 + 1);
+    if (nplanes <= 0) return;                             // batched form: past this instance's planes
     const size_t xrow = (size_t)nz * d.ldx;
     const size_t xf = (size_t)d.nyp * xrow;
     const T inv_nz = T(1.0 / (double)nz);
@@ -524,6 +564,24 @@ __global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __rest
         }
         __syncthreads();   // buffer t&1 is refilled by the load issued next iteration
     }
+}
+
+template <typename T, int NC, int TX>
+__global__ void __launch_bounds__(256, 2) k_zfwd_nl(Dims d, const cpx<T>* __restrict__ Y,
+                                                    cpx<T>* __restrict__ NL, int jlo, int jhi, int zp,
+                                                    const double* __restrict__ kxw,
+                                                    const double* __restrict__ kzw, FftPlan pz,
+                                                    const cpx<T>* __restrict__ twz) {
+    zfwd_nl_body<T, NC, TX>(d, Y, NL, jlo, jhi, zp, kxw, kzw, pz, twz, blockIdx);
+}
+
+// Batched form: instance blockIdx.z / nf of a group of equal shape.
+template <typename T, int NC, int TX>
+__global__ void __launch_bounds__(256, 2) k_zfwd_nl_b(const InstPtrs* __restrict__ ip, Dims d, int jhi, int zp,
+                                                      FftPlan pz, const cpx<T>* __restrict__ twz) {
+    const InstPtrs q = ip[blockIdx.z / d.nf];
+    zfwd_nl_body<T, NC, TX>(d, reinterpret_cast<const cpx<T>*>(q.yb), reinterpret_cast<cpx<T>*>(q.nl), q.jlo_prod,
+                            jhi, zp, q.kx, q.kz, pz, twz, make_uint3(blockIdx.x, blockIdx.y, blockIdx.z % d.nf));
 }
 
 // ---------------------------------------------------------------------------
@@ -611,6 +669,90 @@ cudaError_t launch_zfwd_nl(const Dims& d, const void* Y, void* NL, int jlo, int 
     }
     return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------
+// Batched launchers: one launch covers the instances ip[0..ninst) of a group
+// of equal shape; the instance is a grid coordinate and its arrays come from
+// the device-side table ip.
+// ---------------------------------------------------------------------------
+template <typename T>
+cudaError_t launch_zinv_b(const Dims& d, const InstPtrs* ip, int ninst, size_t s_fstride, size_t x_fstride,
+                          const FftPlan& pz, const void* twz, cudaStream_t st, int skip_mean) {
+    constexpr int TX = ZTile<T>::TX;
+    const size_t smem = sizeof(cpx<T>) * (size_t)d.nz * TX;
+    dim3 grid(d.ldx / TX, d.nyp, d.nf * ninst);
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 256, smem, st>>>(ip, d.nf, d, s_fstride, x_fstride, pz, (const cpx<T>*)twz, skip_mean);
+    };
+    switch (d.nz) {
+#define CASE(N) case N: go(k_zinv_b<T, N, TX>); break;
+        DGPU_NZ_LIST(CASE)
+#undef CASE
+        default: go(k_zinv_b<T, 0, TX>); break;
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_products_b(const Dims& d, const InstPtrs* ip, int ninst, int jlo_min, int jhi, int chunk,
+                              const FftPlan& pm, const void* twm, const void* twn, cudaStream_t st, int mean_split,
+                              size_t means_fstride) {
+    if (jhi < jlo_min) return cudaSuccess;
+    const int group = products_group(d.nx);
+    if (group < 1) return cudaErrorInvalidValue;
+    const int M = d.nx / 2;
+    const int rows = group < d.nf + d.np ? group : d.nf + d.np;
+    const size_t smem = sizeof(T) * (size_t)RING * d.nf * d.nx + sizeof(cpx<T>) * (size_t)rows * row_pitch(M) +
+                        sizeof(cpx<T>) * 3 * (size_t)M + sizeof(cpx<T>) * 2 * (size_t)d.nf * d.ldx + 16;
+    dim3 grid(d.nz, (jhi - jlo_min + chunk) / chunk, ninst);
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 256, smem, st>>>(ip, d, jhi, chunk, group, pm, (const cpx<T>*)twm, (const cpx<T>*)twn, mean_split,
+                                      means_fstride);
+    };
+    switch (M) {
+#define CASE(N) case N: go(k_products_b<T, N>); break;
+        DGPU_M_LIST(CASE)
+#undef CASE
+        default: go(k_products_b<T, 0>); break;
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_zfwd_nl_b(const Dims& d, const InstPtrs* ip, int ninst, int jlo_min, int jhi, int zp,
+                             const FftPlan& pz, const void* twz, cudaStream_t st) {
+    constexpr int TX = ZfTile<T>::TX;
+    if (jhi < jlo_min) return cudaSuccess;
+    if (zp < 1) zp = ZF_PLANES;
+    dim3 grid(d.ldx / TX, (jhi - jlo_min + zp) / zp, d.nf * ninst);
+    auto go = [&](auto kern, bool ct) {
+        const size_t smem = sizeof(cpx<T>) * (2 * (size_t)d.nz * TX + (ct ? 0 : (size_t)d.nkzt * TX));
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 256, smem, st>>>(ip, d, jhi, zp, pz, (const cpx<T>*)twz);
+    };
+    switch (d.nz) {
+#define CASE(N) case N: go(k_zfwd_nl_b<T, N, TX>, true); break;
+        DGPU_NZ_LIST(CASE)
+#undef CASE
+        default: go(k_zfwd_nl_b<T, 0, TX>, false); break;
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_zinv_b<float>(const Dims&, const InstPtrs*, int, size_t, size_t, const FftPlan&,
+                                          const void*, cudaStream_t, int);
+template cudaError_t launch_zinv_b<double>(const Dims&, const InstPtrs*, int, size_t, size_t, const FftPlan&,
+                                           const void*, cudaStream_t, int);
+template cudaError_t launch_products_b<float>(const Dims&, const InstPtrs*, int, int, int, int, const FftPlan&,
+                                              const void*, const void*, cudaStream_t, int, size_t);
+template cudaError_t launch_products_b<double>(const Dims&, const InstPtrs*, int, int, int, int, const FftPlan&,
+                                               const void*, const void*, cudaStream_t, int, size_t);
+template cudaError_t launch_zfwd_nl_b<float>(const Dims&, const InstPtrs*, int, int, int, int, const FftPlan&,
+                                             const void*, cudaStream_t);
+template cudaError_t launch_zfwd_nl_b<double>(const Dims&, const InstPtrs*, int, int, int, int, const FftPlan&,
+                                              const void*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Transform-API helpers (FP64, one field).  Rows r = (J - j0)*NZ + z; a block
