@@ -176,16 +176,21 @@ __device__ __forceinline__ void products_hw_body(const Dims& d, const c32* __res
     if (inv_active) stage(jb - 1);
     __syncthreads();                               // twiddle tables
     for (int J = jb - 1; J <= je + 2; ++J) {
-        if (inv_active && J <= je + 1) {
+        const int jp = J - 2;
+        const bool do_inv = inv_active && J <= je + 1;             // field f of plane J to physical space
+        const bool do_prod = !inv && jp >= jb && role.prod >= 0;   // product role.prod of plane jp
+        const int s = (J - jb + 1) & (HRING - 1);
+        c32 v[16];
+        if (do_inv) {
             // ---- field f of plane J to physical space ---------------------------
-            const int s = (J - jb + 1) & (HRING - 1);
             cp_async_wait_all();
             __syncwarp(mask);
             if (lane == 0) smean[s][f] = means ? (float)means[(size_t)f * means_fs + (size_t)J * ps].x : 0.0f;
             // Zc_k = (X_k + conj X_{M-k}) + i W512^-k (X_k - conj X_{M-k}) at
             // k = lane + 16 r; its backward 256-point transform is
-            // x_{2m} + i x_{2m+1} (DC imaginary part and Nyquist dropped)
-            c32 v[16];
+            // x_{2m} + i x_{2m+1} (DC imaginary part and Nyquist dropped).  One
+            // transform routine (forward sign) serves both kinds of half-warp,
+            // so their code stays in the instruction cache together.
 #pragma unroll
             for (int r = 0; r < 16; ++r) {
                 const int k = lane + 16 * r;
@@ -198,17 +203,12 @@ __device__ __forceinline__ void products_hw_body(const Dims& d, const c32* __res
                 if (kk <= nkx) xc = conjg(stg[kk]);
                 const c32 A = xa + xc;
                 const c32 B = cmul(xa - xc, conjg(stn[k]));
-                v[r] = mk<float>(A.x - B.y, A.y + B.x);
+                v[r] = mk<float>(A.x - B.y, -(A.y + B.x));      // conjugated: the backward
+                                                                 // transform as conj(forward(conj))
             }
             __syncwarp(mask);                      // the row is consumed: stage the next one
             if (J + 1 <= je + 1) stage(J + 1);
-            fft256<+1>(v, tb, stw, lane, mask);
-            c32* dst = ring + ((size_t)s * nf + f) * HM + lane;
-#pragma unroll
-            for (int r = 0; r < 16; ++r) dst[r * 16] = v[r];
-        }
-        const int jp = J - 2;
-        if (!inv && jp >= jb && role.prod >= 0) {
+        } else if (do_prod) {
             // ---- product role.prod of plane jp from ring planes jp-1..jp+1 ----
             const int sm = (jp - jb) & (HRING - 1), s0 = (jp - jb + 1) & (HRING - 1), sp = (jp - jb + 2) & (HRING - 1);
             const c32* Rm = ring + (size_t)sm * nf * HM + lane;
@@ -219,7 +219,6 @@ __device__ __forceinline__ void products_hw_body(const Dims& d, const c32* __res
             const float m2m = smean[sm][1], m2 = smean[s0][1], m2p = smean[sp][1];
             const float m3m = smean[sm][2], m3 = smean[s0][2], m3p = smean[sp][2];
             const int p = role.prod;
-            c32 v[16];
             // lower-case: fluctuation about the plane mean mN; each product is
             // its part beyond the mean x mean product
             if (p == 0 || p == 1 || p == 2 || p >= 8 && (p - 8) % 3 != 2) {
@@ -287,7 +286,13 @@ __device__ __forceinline__ void products_hw_body(const Dims& d, const c32* __res
                     v[r] = mk<float>(flux(qm.x, q0.x, qp.x, u2.x, u2p.x), flux(qm.y, q0.y, qp.y, u2.y, u2p.y));
                 }
             }
-            fft256<-1>(v, tb, stw, lane, mask);
+        }
+        if (do_inv || do_prod) fft256<-1>(v, tb, stw, lane, mask);
+        if (do_inv) {
+            c32* dst = ring + ((size_t)s * nf + f) * HM + lane;
+#pragma unroll
+            for (int r = 0; r < 16; ++r) dst[r * 16] = conjg(v[r]);
+        } else if (do_prod) {
             c32 o[HD];
             extract(v, o, tb, stn, lane, mask, nkx, inv_nx);
             c32* yrow = Y + (size_t)jp * xrow + (size_t)z * ldx + lane;
