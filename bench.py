@@ -44,10 +44,10 @@ FALLBACK_HBM_GBS = 6650.0
 # each kernel at 512x257x384, FP32-split; scaled to other grids by their
 # number of planes.
 TRAFFIC_PER_PLANE = {
-    "zinv": (749.9e6 + 513.2e6) / 259.0,
-    "products": (570.4e6 + 1052.9e6) / 259.0,
-    "zfwd_nl": (1114.4e6 + 360.0e6) / 259.0,
-    "column": (2257.0e6 + 1629.2e6) / 259.0,
+    "zinv": (749.9e6 + 513.5e6) / 259.0,
+    "products": (562.9e6 + 1052.9e6) / 259.0,
+    "zfwd_nl": (1114.5e6 + 359.9e6) / 259.0,
+    "column": (2293.7e6 + 1630.3e6) / 259.0,
 }
 
 
