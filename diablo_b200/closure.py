@@ -95,6 +95,16 @@ def eddy_viscosity_basis(x: np.ndarray) -> np.ndarray:
     return -2.0 * smag[:, None] * sv
 
 
+def dissipation(x: np.ndarray, t: np.ndarray) -> np.ndarray:
+    """Subgrid dissipation Pi = -tau_ij S_ij of dimensionless stresses t from
+    the dimensionless gradient features x (S_ij the symmetric part of g_ij)."""
+    g = np.asarray(x[:, :9], dtype=np.float64).reshape(-1, 3, 3)
+    s = 0.5 * (g + g.transpose(0, 2, 1))
+    sv = np.stack([s[:, a, b] for a, b in _PAIRS], axis=1)
+    c = np.array([1.0, 1.0, 1.0, 2.0, 2.0, 2.0])
+    return -np.sum(c * sv * np.asarray(t, dtype=np.float64), axis=1)
+
+
 def plane_coefficients(x: np.ndarray, t: np.ndarray, s: np.ndarray) -> dict:
     """Least-squares C for each plane (keyed by its y+ feature) from samples,
     minimising the error of the dimensional stresses (weights s^2)."""
@@ -145,11 +155,16 @@ class ClosureReport:
 
 
 def train_and_evaluate(data: Snapshots, seed: int, steps: int, batch: int = 1024, lr: float = 2e-3,
-                       frac: float = 0.8, max_stats: int = 2_000_000) -> ClosureReport:
+                       frac: float = 0.8, max_stats: int = 2_000_000, diss_weight: float = 0.0) -> ClosureReport:
     """Train on the training snapshots (seeded split and shuffle) and compare
     the network with the best per-plane eddy viscosity on the held-out ones.
     The normalisation, the per-plane coefficients and the held-out errors use
-    seeded subsamples of at most max_stats samples (training uses all)."""
+    seeded subsamples of at most max_stats samples (training uses all).
+    diss_weight > 0 adds the subgrid-dissipation term to the loss
+    (SgsMlp.set_dissipation_weight), measured against the spread of the
+    training targets' dissipation: the weight passed on is
+    diss_weight / var(Pi(t)), so that diss_weight = 1 weighs a dissipation
+    error of one standard deviation like a stress error of one output scale."""
     count = int(data.snap.max()) + 1
     tr, te = split(count, seed, frac)
     mtr = np.isin(data.snap, tr)
@@ -165,6 +180,9 @@ def train_and_evaluate(data: Snapshots, seed: int, steps: int, batch: int = 1024
     mean, scale, osc = normalisation(xtr[st].astype(np.float64), ttr[st].astype(np.float64))
     t0 = _time.perf_counter()
     with SgsMlp(init_params(seed, mean, scale, osc)) as m:
+        if diss_weight:
+            pi_t = dissipation(xtr[st], ttr[st])
+            m.set_dissipation_weight(diss_weight / max(float(np.var(pi_t)), 1e-300))
         losses = m.train(xtr, ttr, batch, steps, lr)
         train_seconds = _time.perf_counter() - t0
         pred = m.forward(xte[se]).astype(np.float64)

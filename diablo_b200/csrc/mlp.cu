@@ -306,8 +306,8 @@ constexpr size_t grad_smem() {
 
 __global__ void __launch_bounds__(32 * NW) k_mlp_grad(MlpDev m, const float* __restrict__ x,
                                                        const float* __restrict__ tgt, long long s_begin,
-                                                       long long n, float inv_batch, float* __restrict__ grad,
-                                                       double* __restrict__ loss) {
+                                                       long long n, float inv_batch, float lam,
+                                                       float* __restrict__ grad, double* __restrict__ loss) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint16_t* sw = reinterpret_cast<uint16_t*>(smem);
     uint16_t* tiles = sw + SWN;
@@ -349,21 +349,49 @@ __global__ void __launch_bounds__(32 * NW) k_mlp_grad(MlpDev m, const float* __r
         __syncwarp();
         float o[4];
         forward_tile(sw, sb, w, o, g, t);
-        // output deltas
+        // output deltas.  With the dissipation weight lam the loss adds
+        // lam/2 (Pi(y) - Pi(t))^2 per sample, Pi = -sum c_k tau_k S_k the
+        // subgrid dissipation of the dimensionless stresses (c_k = 1 for the
+        // diagonal, 2 for the off-diagonal ones, S_k from the sample's
+        // gradient features): Pi(y) - Pi(t) = sum_k pe_k e_k with
+        // pe_k = -c_k out_scale_k S_k, reduced over the quad of lanes that
+        // holds a row's outputs.
+        float e4[4], pe4[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = g + (q >> 1) * 8, c = 2 * t + (q & 1);
+            float e = 0.0f, pe = 0.0f;
+            if (c < NOUT && s0 + r < n) {
+                e = o[q] - tgt[(s_begin + s0 + r) * NOUT + c] / m.p[OOUT + c];
+                if (lam != 0.0f) {
+                    const float* xr = x + (s_begin + s0 + r) * NIN;
+                    const int ia = c < 3 ? c : (c == 5 ? 1 : 0), ib = c < 3 ? c : (c == 3 ? 1 : 2);
+                    const float S = 0.5f * (xr[3 * ia + ib] + xr[3 * ib + ia]);
+                    pe = -(c < 3 ? 1.0f : 2.0f) * m.p[OOUT + c] * S;
+                }
+            }
+            e4[q] = e;
+            pe4[q] = pe;
+        }
+        float dpi[2] = {pe4[0] * e4[0] + pe4[1] * e4[1], pe4[2] * e4[2] + pe4[3] * e4[3]};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            dpi[h] += __shfl_xor_sync(0xffffffffu, dpi[h], 1);
+            dpi[h] += __shfl_xor_sync(0xffffffffu, dpi[h], 2);
+        }
         float d[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int r = g + (q >> 1) * 8, c = 2 * t + (q & 1);
-            float v = 0.0f;
-            if (c < NOUT && s0 + r < n) {
-                const float e = o[q] - tgt[(s_begin + s0 + r) * NOUT + c] / m.p[OOUT + c];
-                lsum += 0.5 * (double)e * (double)e * (double)inv_batch;
-                v = e * inv_batch;
-            }
+            const float e = e4[q];
+            const float v = (e + lam * dpi[q >> 1] * pe4[q]) * inv_batch;
+            lsum += 0.5 * (double)e * (double)e * (double)inv_batch;
             d[q] = v;
             d4[r * LD1 + c] = bf(v);
             d4[r * LD1 + c + 8] = 0;
         }
+        if (t == 0)
+            lsum += 0.5 * (double)lam * ((double)dpi[0] * dpi[0] + (double)dpi[1] * dpi[1]) * (double)inv_batch;
         bias_grad(d, sg + GB + 3 * NH, NOUT);
         __syncwarp();
         // dW4 = d4^T H3 (rows 0..5 kept)
@@ -491,6 +519,7 @@ struct Mlp {
     float* xbuf = nullptr;    // staged host data
     float* tbuf = nullptr;
     size_t cap = 0;
+    float diss_weight = 0.0f;  // weight of the subgrid-dissipation term of the loss
     long long adam_t = 0;
     int nblocks = 148;
     cudaStream_t st = nullptr;
@@ -526,7 +555,8 @@ int run_grad(Mlp* m, long long s_begin, long long n, float inv_batch) {
     const long long tiles = (n + TS - 1) / TS;
     long long nb = (tiles + NW - 1) / NW;
     if (nb > m->nblocks) nb = m->nblocks;
-    k_mlp_grad<<<(unsigned)nb, 32 * NW, smem, m->st>>>(md, m->xbuf, m->tbuf, s_begin, n, inv_batch, m->g, m->loss);
+    k_mlp_grad<<<(unsigned)nb, 32 * NW, smem, m->st>>>(md, m->xbuf, m->tbuf, s_begin, n, inv_batch, m->diss_weight,
+                                                        m->g, m->loss);
     MCK(cudaGetLastError());
     return DIABLO_OK;
 }
@@ -614,6 +644,14 @@ int diablo_mlp_set_params(void* mlp, const float* params) {
     MCK(cudaMemsetAsync(m->g, 0, sizeof(float) * NTRAIN, m->st));
     m->adam_t = 0;
     MCK(cudaStreamSynchronize(m->st));
+    return DIABLO_OK;
+}
+
+int diablo_mlp_set_dissipation_weight(void* mlp, float weight) {
+    Mlp* m = (Mlp*)mlp;
+    if (!m) return mfail(DIABLO_EINVAL, "null MLP");
+    if (!(weight >= 0.0f) || !std::isfinite(weight)) return mfail(DIABLO_EINVAL, "dissipation weight must be >= 0");
+    m->diss_weight = weight;
     return DIABLO_OK;
 }
 

@@ -30,6 +30,7 @@ def _bind(L):
     L.diablo_mlp_forward.argtypes = [vp, fp, ll, fp]
     L.diablo_mlp_gradient.argtypes = [vp, fp, fp, ll, dp, fp]
     L.diablo_mlp_train.argtypes = [vp, fp, fp, ll, ctypes.c_int, ctypes.c_int, ctypes.c_float, dp]
+    L.diablo_mlp_set_dissipation_weight.argtypes = [vp, ctypes.c_float]
     L._mlp_bound = True
     return L
 
@@ -108,6 +109,11 @@ class SgsMlp:
         p = _f32(p)
         assert p.size == NPARAM
         _check(self.L.diablo_mlp_set_params(self._h, _fp(p)), "diablo_mlp_set_params")
+
+    def set_dissipation_weight(self, w: float) -> None:
+        """Weight of the subgrid-dissipation term of the training loss:
+        w/2 (Pi(y) - Pi(t))^2 per sample, Pi = -tau_ij S_ij."""
+        _check(self.L.diablo_mlp_set_dissipation_weight(self._h, float(w)), "diablo_mlp_set_dissipation_weight")
 
     def params(self) -> np.ndarray:
         p = np.zeros(NPARAM, dtype=np.float32)

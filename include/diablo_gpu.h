@@ -360,8 +360,18 @@ int diablo_mlp_get_params(void* mlp, float* params);
  * in the closure's use). */
 int diablo_mlp_forward(void* mlp, const float* x, long long n, float* y);
 /* Loss sum_samples sum_outputs (y/out_scale - t/out_scale)^2 / (2n) and its
- * gradient with respect to the DIABLO_MLP_NTRAIN trained parameters. */
+ * gradient with respect to the DIABLO_MLP_NTRAIN trained parameters.  With a
+ * dissipation weight w (diablo_mlp_set_dissipation_weight, default 0) the
+ * loss adds w/(2n) sum_samples (Pi(y) - Pi(t))^2, Pi(tau) = -sum_ij tau_ij
+ * S_ij the subgrid dissipation of the dimensionless stresses, S_ij the
+ * symmetric part of the sample's gradient features x[0..8] (g_ij, i-major):
+ * it trains the network to transfer the right energy between the resolved
+ * and subgrid scales, not only to match the stresses. */
 int diablo_mlp_gradient(void* mlp, const float* x, const float* t, long long n, double* loss, float* grad);
+/* Weight w >= 0 of the dissipation term of the loss (used by
+ * diablo_mlp_gradient and diablo_mlp_train).  No counterpart in the
+ * reference, like the rest of the closure. */
+int diablo_mlp_set_dissipation_weight(void* mlp, float weight);
 /* steps Adam steps (beta 0.9, 0.999, eps 1e-8, learning rate lr) on
  * consecutive mini-batches of `batch` samples, cycling through the n
  * samples as given (the caller shuffles); losses[s] (may be NULL) receives

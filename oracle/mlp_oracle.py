@@ -77,16 +77,36 @@ def forward(p: np.ndarray, x: np.ndarray, emulate_bf16: bool = False, keep: bool
     return y * q["oscale"]
 
 
-def loss_grad(p: np.ndarray, x: np.ndarray, t: np.ndarray):
+_PAIRS = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+
+
+def dissipation_weights(x: np.ndarray, oscale: np.ndarray) -> np.ndarray:
+    """pe[n][6]: Pi(tau) = sum_k pe_k y_k for tau_k = out_scale_k y_k,
+    Pi = -sum_ij tau_ij S_ij with S_ij the symmetric part of the gradient
+    features g_ij = x[3i+j] (off-diagonal pairs counted twice)."""
+    g = np.asarray(x, dtype=np.float64)[:, :9].reshape(-1, 3, 3)
+    s = 0.5 * (g + g.transpose(0, 2, 1))
+    sv = np.stack([s[:, a, b] for a, b in _PAIRS], axis=1)
+    c = np.array([1.0, 1.0, 1.0, 2.0, 2.0, 2.0])
+    return -c * np.asarray(oscale, dtype=np.float64) * sv
+
+
+def loss_grad(p: np.ndarray, x: np.ndarray, t: np.ndarray, diss_weight: float = 0.0):
     """Loss sum (y - t/out_scale)^2 / (2n) over samples and outputs (y the
-    normalised output) and its gradient with respect to the trained
-    parameters, FP64."""
+    normalised output), plus diss_weight/(2n) sum (Pi(y) - Pi(t))^2 over
+    samples (the subgrid dissipation, dissipation_weights), and its gradient
+    with respect to the trained parameters, FP64."""
     q = unpack(p)
     n = x.shape[0]
     y, hs, zs = forward(p, x, keep=True)
     e = y - np.asarray(t, dtype=np.float64) / q["oscale"]
     loss = 0.5 * float(np.sum(e * e)) / n
     d = e / n
+    if diss_weight:
+        pe = dissipation_weights(x, q["oscale"])
+        dpi = np.sum(pe * e, axis=1)
+        loss += 0.5 * diss_weight * float(np.sum(dpi * dpi)) / n
+        d = d + diss_weight * dpi[:, None] * pe / n
     grads = {"W4": d.T @ hs[3], "b4": d.sum(axis=0)}
     g = d @ q["W4"]
     for l in (3, 2, 1):

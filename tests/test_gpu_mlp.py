@@ -58,6 +58,25 @@ def test_gradient_matches_oracle():
     assert abs(loss2 - loss) <= 1e-6 * loss and relerr(g2, g) < 1e-5
 
 
+def test_gradient_with_dissipation_term_matches_oracle():
+    """The loss with the subgrid-dissipation term and its gradient against
+    the FP64 oracle, at the bars of the plain gradient.  The weight is 5 over
+    the variance of the targets' dissipation, as closure.train_and_evaluate
+    sets it."""
+    from diablo_b200.closure import dissipation
+
+    x, t, p = data(6, 4000)
+    w = 5.0 / float(np.var(dissipation(x, t)))
+    with ML.SgsMlp(p) as m:
+        m.set_dissipation_weight(w)
+        loss, g = m.gradient(x, t)
+    lo, go = M.loss_grad(p.astype(np.float64), x, t, diss_weight=w)
+    lo0, go0 = M.loss_grad(p.astype(np.float64), x, t)
+    assert relerr(go, go0) > 0.05                  # the term changes the gradient
+    assert abs(loss - lo) <= 2e-2 * lo
+    assert relerr(g, go) < 3e-2
+
+
 def test_training_lowers_loss():
     x, t, p = data(7, 20000)
     rng = np.random.default_rng(8)

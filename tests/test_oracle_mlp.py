@@ -61,3 +61,34 @@ def test_adam_first_step_moves_by_lr():
     nz = np.abs(g) > 1e-4      # |g|/(|g|+eps) within 1e-4 of 1
     assert np.allclose(d[nz], -1e-3 * np.sign(g[nz]), rtol=1e-3)
     assert np.array_equal(q[M.NTRAIN:], p[M.NTRAIN:])
+
+
+def test_dissipation_term_gradient_and_definition():
+    """The subgrid-dissipation term of the loss: its value from the stresses
+    and gradient features directly (Pi = -tau_ij S_ij, off-diagonals twice),
+    and the analytic gradient of the whole loss against central differences."""
+    p, x, t = sample(5)
+    w = 0.7
+    q = M.unpack(p)
+    y = M.forward(p, x)                          # physical stresses
+    g = x[:, :9].reshape(-1, 3, 3)
+    s = 0.5 * (g + g.transpose(0, 2, 1))
+
+    def pi(tau):
+        full = np.zeros((tau.shape[0], 3, 3))
+        for k, (a, b) in enumerate([(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]):
+            full[:, a, b] = full[:, b, a] = tau[:, k]
+        return -np.einsum("nij,nij->n", full, s)
+
+    e = (y - t) / q["oscale"]
+    want = 0.5 * np.sum(e * e) / x.shape[0] + 0.5 * w * np.sum((pi(y) - pi(t)) ** 2) / x.shape[0]
+    loss, grad = M.loss_grad(p, x, t, diss_weight=w)
+    assert np.isclose(loss, want, rtol=1e-12)
+    rng = np.random.default_rng(6)
+    h = 1e-6
+    for i in rng.choice(M.NTRAIN, 40, replace=False):
+        q1, q2 = p.copy(), p.copy()
+        q1[i] += h
+        q2[i] -= h
+        fd = (M.loss_grad(q1, x, t, w)[0] - M.loss_grad(q2, x, t, w)[0]) / (2 * h)
+        assert abs(fd - grad[i]) <= 1e-7 + 1e-5 * abs(grad[i]), (i, fd, grad[i])
