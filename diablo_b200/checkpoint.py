@@ -1,20 +1,24 @@
 """Flow checkpoints with the reference's SAVE_FLOW / READ_FLOW semantics
 (for/diablo_io.f:201-418) in its two file formats.
 
-HDF5 datasets (WriteHDF5 / ReadHDF5, for/hdf5.f:5-295, 297-546).  The image
-has no HDF5 library, so `write` / `read` keep the datasets of start.h5 /
-out.h5 / end.h5 -- names, array layout and interpolation -- in a numpy .npz
-container:
+HDF5 files (WriteHDF5 / ReadHDF5, for/hdf5.f:5-295, 297-546), written and
+read by diablo_b200.h5 (no HDF5 library in the image) in WriteHDF5's layout:
 
-* ``U``, ``W``, ``TH01``.., ``P``: physical fields on rows J = 1..NY as
-  SWAPZY writes them (hdf5.f:1243-1262), i.e. the Fortran array
-  out(1:NX,1:NY,1:NZ), stored in numpy C order with shape (NZ, NY, NX) --
-  the byte layout of the reference's dataset;
+* file attributes ``Resolution`` (int32 [NX, NY, NZ]), ``Date`` and ``Info``
+  (20 and 80 one-character strings);
+* group ``/Timestep`` with attribute ``Time`` (scalar float64) and this
+  library's ``TimeStep`` (scalar int32, TIME_STEP, which the reference's
+  reader does not look for);
+* its datasets ``U``, ``W``, ``TH01``.., ``P``: physical fields on rows
+  J = 1..NY as SWAPZY writes them (hdf5.f:1243-1262), i.e. the Fortran array
+  out(1:NX,1:NY,1:NZ) -- float64 with shape (NZ, NY, NX) in C order, the
+  reference's dataset byte for byte;
 * ``V``: U2 moved to GYF points by G2GF before it is written and moved back
   by GF2G when read (hdf5.f:1177-1241), which also imposes V(1) = -V(2),
-  V(NY+1) = -V(NY);
-* ``Time`` (the Timestep group's attribute), ``Timestep`` and
-  ``Resolution`` = (NX, NY, NZ).
+  V(NY+1) = -V(NY).
+
+`read` also takes the .npz container earlier versions of this library
+wrote.
 
 The reference's writer names the scalars ``TH01``.. (hdf5.f:211-213) and its
 reader asks for ``TH1``.. (hdf5.f:426-427), so it cannot read back its own
@@ -45,8 +49,12 @@ wrote the file.
 """
 from __future__ import annotations
 
+import os
+import time as _time
+
 import numpy as np
 
+from . import h5
 from .layout import new_fourier, new_physical
 from .params import DiabloParams
 
@@ -87,24 +95,44 @@ def write(path: str, p: DiabloParams, fields: dict, time: float, time_step: int,
           th_reader_names: bool = False) -> None:
     """WriteHDF5's datasets from physical [J][K][I] fields (NY+2, NZ, NX)
     keyed U, V, W, TH01.. and, with SAVE_PRESSURE, P."""
-    out = {"Time": np.float64(time), "Timestep": np.int64(time_step),
-           "Resolution": np.array([p.nx, p.ny, p.nz], dtype=np.int64)}
+    root = h5.Group()
+    root.attrs["Resolution"] = np.array([p.nx, p.ny, p.nz], dtype=np.int32)
+    root.attrs["Date"] = np.frombuffer(_time.strftime("%Y-%m-%d %H:%M:%S").ljust(20)[:20].encode(), dtype="S1")
+    root.attrs["Info"] = np.frombuffer(" (Put here what you want) ".ljust(80).encode(), dtype="S1")
+    ts = root.group("Timestep")
+    ts.attrs["Time"] = np.float64(time)
+    ts.attrs["TimeStep"] = np.int32(time_step)
     for name in ["U", "V", "W"] + scalar_names(p) + (["P"] if "P" in fields else []):
         a = np.asarray(fields[name], dtype=np.float64)
         if a.shape != (p.ny + 2, p.nz, p.nx):
             raise ValueError(f"{name}: shape {a.shape}, expected {(p.ny + 2, p.nz, p.nx)}")
         d = g2gf(a) if name == "V" else a
         key = f"TH{int(name[2:])}" if th_reader_names and name.startswith("TH") else name
-        out[key] = np.ascontiguousarray(d[1 : p.ny + 1].transpose(1, 0, 2))    # SWAPZY
-    np.savez(path, **out)
+        ts.children[key] = h5.Dataset(np.ascontiguousarray(d[1 : p.ny + 1].transpose(1, 0, 2)))   # SWAPZY
+    h5.write(path, root)
+
+
+def datasets(path: str) -> dict:
+    """The file's datasets by name, with ``Time``, ``Timestep`` (0 when the
+    file has none) and ``Resolution``."""
+    if h5.is_hdf5(path):
+        root = h5.read(path)
+        ts = root.children["Timestep"]
+        out = {k: v.data for k, v in ts.children.items()}
+        out["Time"] = np.float64(ts.attrs["Time"])
+        out["Timestep"] = np.int64(ts.attrs["TimeStep"]) if "TimeStep" in ts.attrs else np.int64(0)
+        if "Resolution" in root.attrs:
+            out["Resolution"] = np.asarray(root.attrs["Resolution"], dtype=np.int64)
+        return out
+    with np.load(path if os.path.exists(path) else path + ".npz") as f:
+        return {k: f[k] for k in f.files}
 
 
 def read(path: str, p: DiabloParams, new_scalars=()) -> dict:
     """ReadHDF5's datasets as physical [J][K][I] fields (rows 0 and NY+1
     zero).  Scalars listed in `new_scalars` (0-based; CREATE_NEW_TH) are not
     read.  Returns {"fields", "time", "time_step", "pressure"}."""
-    with np.load(path) as f:
-        data = {k: f[k] for k in f.files}
+    data = datasets(path)
     if "Resolution" in data:
         res = tuple(int(v) for v in data["Resolution"])
         if res != (p.nx, p.ny, p.nz):

@@ -6,12 +6,12 @@ datasets ``0001``, ``0002``, .. of NY float64 values (rows 1..NY), each with
 a ``Time`` attribute (the ``time`` group holds one value per dataset and no
 attribute).
 
-The image has no HDF5 library, so a file is a zip archive of .npy members
-that numpy reads with ``np.load``: dataset ``<group>/<NNNN>`` and its
-attribute ``<group>/<NNNN>@Time``.  A dataset is appended as a new member,
-so a call costs the size of what it adds, as with HDF5.  ``SAMPLES`` is not
-stored: it is the number of datasets in the group, the value the reference
-keeps (it increments it once per dataset written).
+The files are HDF5 (diablo_b200.h5, written without an HDF5 library): group
+``<name>`` with its scalar int32 ``SAMPLES`` attribute, datasets ``<NNNN>``
+of float64 with a scalar float64 ``Time`` attribute, as WriteStatH5 creates
+them.  An append reads the file's tree, adds the call's datasets and writes
+it again, so a caller groups the datasets of one SAVE_STATS call into one
+write_many.
 
 The reference writes omega_y into mean.h5's ``omega_z`` group
 (save_stats.f:421-423); ``StatsWriter(omega_z_quirk=True)``, the default,
@@ -30,52 +30,39 @@ TIME, DELTA_T and UBULK) follow gfortran's list-directed style: integers in
 """
 from __future__ import annotations
 
-import io
 import os
-import re
-import zipfile
 
 import numpy as np
 
+from . import h5
 from .channel import MEAN_NAMES, SCAL_NAMES
-
-_MEMBER = re.compile(r"^(?P<g>[^/]+)/(?P<n>\d{4,})(?P<a>@Time)?\.npy$")
 
 
 class StatFile:
-    """One mean.h5-style file, opened for appending.  Every append rewrites
-    the archive's central directory, so a caller groups the datasets of one
-    SAVE_STATS call into one write_many."""
+    """One mean.h5-style HDF5 file, opened for appending.  Every append
+    rewrites the file, so a caller groups the datasets of one SAVE_STATS call
+    into one write_many."""
 
     def __init__(self, path: str):
         self.path = path
-        self._samples: dict[str, int] = {}
-        if os.path.exists(path):
-            with zipfile.ZipFile(path) as z:
-                for name in z.namelist():
-                    m = _MEMBER.match(name)
-                    if m and not m["a"]:
-                        self._samples[m["g"]] = max(self._samples.get(m["g"], 0), int(m["n"]))
+        self.root = h5.read(path) if os.path.exists(path) else h5.Group()
 
     def samples(self, gname: str) -> int:
-        return self._samples.get(gname, 0)
+        g = self.root.children.get(gname)
+        return int(g.attrs["SAMPLES"]) if g is not None and "SAMPLES" in g.attrs else 0
 
     def write_many(self, entries) -> list[int]:
-        """Append datasets (gname, value, time or None) in one pass over the
-        archive: each gets the group's next number; returns them."""
-        members, numbers = [], []
+        """Append datasets (gname, value, time or None): each gets the group's
+        next number; returns them."""
+        numbers = []
         for gname, value, time in entries:
+            g = self.root.group(gname)
             n = self.samples(gname) + 1                   # NSAMP = NSAMP + 1; dname = '(I0.4)'
-            self._samples[gname] = n
+            g.attrs["SAMPLES"] = np.int32(n)
+            attrs = {} if time is None else {"Time": np.float64(time)}
+            g.children[f"{n:04d}"] = h5.Dataset(np.asarray(value, dtype="<f8"), attrs)
             numbers.append(n)
-            members.append((f"{gname}/{n:04d}.npy", np.ascontiguousarray(value, dtype="<f8")))
-            if time is not None:
-                members.append((f"{gname}/{n:04d}@Time.npy", np.array(time, dtype="<f8")))
-        with zipfile.ZipFile(self.path, "a") as z:
-            for name, a in members:
-                buf = io.BytesIO()
-                np.lib.format.write_array(buf, a, allow_pickle=False)
-                z.writestr(name, buf.getvalue())
+        h5.write(self.path, self.root)
         return numbers
 
     def write_real(self, gname: str, value: float) -> int:
@@ -90,19 +77,14 @@ class StatFile:
 def read(path: str) -> dict:
     """{group: {"SAMPLES": n, "data": [n][...] float64, "Time": [n] or None}}."""
     out: dict = {}
-    with np.load(path) as f:
-        keys = f.files
-        groups: dict[str, list[int]] = {}
-        for k in keys:
-            m = _MEMBER.match(k + ".npy")
-            if m and not m["a"]:
-                groups.setdefault(m["g"], []).append(int(m["n"]))
-        for g, ns in groups.items():
-            ns.sort()
-            data = np.stack([f[f"{g}/{n:04d}"] for n in ns])
-            has_t = f"{g}/{ns[0]:04d}@Time" in keys
-            t = np.array([float(f[f"{g}/{n:04d}@Time"]) for n in ns]) if has_t else None
-            out[g] = {"SAMPLES": len(ns), "data": data, "Time": t}
+    for gname, g in h5.read(path).children.items():
+        names = sorted(k for k in g.children if k.isdigit())
+        if not names:
+            continue
+        data = np.stack([g.children[k].data for k in names])
+        has_t = "Time" in g.children[names[0]].attrs
+        t = np.array([float(g.children[k].attrs["Time"]) for k in names]) if has_t else None
+        out[gname] = {"SAMPLES": int(g.attrs.get("SAMPLES", len(names))), "data": data, "Time": t}
     return out
 
 

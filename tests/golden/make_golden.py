@@ -7,6 +7,8 @@
                        HDF5 file's contiguous data block.
 * KH_test_input.dat, KH_test_input_chan.dat -- the reference's KH_test run
                        parameters, byte for byte (input-file parser tests).
+* KH_test_grid.h5    -- the reference's KH_test/grid.h5, byte for byte: a file
+                       the HDF5 library wrote, for the tests of diablo_b200.h5.
 * oracle_kh_small.npz -- CPU-oracle regression vectors: a 24x17x16 shear
                        layer, initial Fourier state and the state after 3
                        time steps (dealiased block), plus the statistics.
@@ -63,6 +65,7 @@ def main() -> None:
     np.savetxt(os.path.join(HERE, "kh_grid_y.txt"), gy, fmt="%.17e")
     shutil.copyfile(os.path.join(kh, "input.dat"), os.path.join(HERE, "KH_test_input.dat"))
     shutil.copyfile(os.path.join(kh, "input_chan.dat"), os.path.join(HERE, "KH_test_input_chan.dat"))
+    shutil.copyfile(os.path.join(kh, "grid.h5"), os.path.join(HERE, "KH_test_grid.h5"))
     oracle_fixture(os.path.join(HERE, "oracle_kh_small.npz"))
     print("fixtures written to", HERE)
 

@@ -4,7 +4,7 @@ reference's restart semantics run on the CPU oracle."""
 import numpy as np
 import pytest
 
-from diablo_b200 import checkpoint as ck, grid as G, ics, layout, params as P
+from diablo_b200 import checkpoint as ck, grid as G, h5, ics, layout, params as P
 from oracle.oracle import ORC_CTH, ORC_P, ORC_U1, ORC_U2, ORC_U3, Oracle
 
 
@@ -103,9 +103,14 @@ def test_write_read_layout_and_round_trip(tmp_path):
     p, _, _, _ = kh(12, 9, 10)
     rng = np.random.default_rng(1)
     f = {k: rng.standard_normal((p.ny + 2, p.nz, p.nx)) for k in ("U", "V", "W", "TH01", "P")}
-    path = str(tmp_path / "out.npz")
+    path = str(tmp_path / "out.h5")
     ck.write(path, p, f, 1.25, 17)
-    raw = np.load(path)
+    raw = ck.datasets(path)
+    tree = h5.read(path)                               # WriteHDF5's layout
+    assert list(tree.attrs["Resolution"]) == [p.nx, p.ny, p.nz] and tree.attrs["Resolution"].dtype == np.int32
+    assert tree.attrs["Date"].shape == (20,) and tree.attrs["Info"].shape == (80,)
+    assert float(tree.children["Timestep"].attrs["Time"]) == 1.25
+    assert sorted(tree.children["Timestep"].children) == ["P", "TH01", "U", "V", "W"]
     # SWAPZY: dataset (NZ, NY, NX) in C order = Fortran out(1:NX,1:NY,1:NZ)
     assert raw["U"].shape == (p.nz, p.ny, p.nx)
     assert raw["U"][3, 4, 5] == f["U"][5, 3, 5]
@@ -122,24 +127,27 @@ def test_write_read_layout_and_round_trip(tmp_path):
 def test_read_names_and_errors(tmp_path):
     p, _, _, _ = kh(12, 9, 10)
     f = {k: np.ones((p.ny + 2, p.nz, p.nx)) for k in ("U", "V", "W", "TH01")}
-    path = str(tmp_path / "a.npz")
+    path = str(tmp_path / "a.h5")
     ck.write(path, p, f, 0.0, 0)
-    d = dict(np.load(path))
-    d["TH1"] = 2 * d.pop("TH01")                               # the reader's name (hdf5.f:426-427)
-    np.savez(str(tmp_path / "b.npz"), **d)
-    r = ck.read(str(tmp_path / "b.npz"), p)
+    tree = h5.read(path)
+    ts = tree.children["Timestep"]
+    th = ts.children.pop("TH01")
+    ts.children["TH1"] = h5.Dataset(2 * th.data)               # the reader's name (hdf5.f:426-427)
+    h5.write(str(tmp_path / "b.h5"), tree)
+    r = ck.read(str(tmp_path / "b.h5"), p)
     assert np.all(r["fields"]["TH01"][1:-1] == 2) and not r["pressure"]
-    d.pop("TH1")
-    np.savez(str(tmp_path / "c.npz"), **d)
+    ts.children.pop("TH1")
+    h5.write(str(tmp_path / "c.h5"), tree)
     with pytest.raises(KeyError):
-        ck.read(str(tmp_path / "c.npz"), p)
-    assert "TH01" not in ck.read(str(tmp_path / "c.npz"), p, new_scalars=(0,))["fields"]
+        ck.read(str(tmp_path / "c.h5"), p)
+    assert "TH01" not in ck.read(str(tmp_path / "c.h5"), p, new_scalars=(0,))["fields"]
     q = p.copy()
     q.nx = 16
     with pytest.raises(ValueError):
         ck.read(path, q)
-    ck.write(str(tmp_path / "d.npz"), p, f, 0.0, 0, th_reader_names=True)
-    assert "TH1" in np.load(str(tmp_path / "d.npz")).files and "TH01" not in np.load(str(tmp_path / "d.npz")).files
+    ck.write(str(tmp_path / "d.h5"), p, f, 0.0, 0, th_reader_names=True)
+    names = ck.datasets(str(tmp_path / "d.h5"))
+    assert "TH1" in names and "TH01" not in names
 
 
 def test_legacy_bytes_and_round_trip(tmp_path):
@@ -204,7 +212,7 @@ def test_oracle_restart_is_reference_restart(tmp_path, save_pressure):
     o = Oracle(p, g, 0.01)
     o.init_from_physical(u, th)
     o.step(4)
-    path = str(tmp_path / "out.npz")
+    path = str(tmp_path / "out.h5")
     oracle_save(o, path, save_pressure)
     if not save_pressure:
         o.poisson_p_chan()
@@ -225,7 +233,7 @@ def test_oracle_restart_variable_dt_runs_courant(tmp_path):
     o = Oracle(p, g, 1e-3)
     o.init_from_physical(u, th)
     o.step(3)
-    path = str(tmp_path / "out.npz")
+    path = str(tmp_path / "out.h5")
     oracle_save(o, path)
     o2 = Oracle(p, g, 5e-2)                                   # a DELTA_T that COURANT replaces
     oracle_load(o2, path, reset_time=True)
@@ -276,7 +284,7 @@ def test_scalar_counts_round_trip(tmp_path, n_th):
         p.pr[1], p.ri[1] = 2.0, 0.0
     rng = np.random.default_rng(5)
     f = {k: rng.standard_normal((p.ny + 2, p.nz, p.nx)) for k in ["U", "V", "W"] + ck.scalar_names(p)}
-    path = str(tmp_path / "out.npz")
+    path = str(tmp_path / "out.h5")
     ck.write(path, p, f, 0.5, 3)
     r = ck.read(path, p)
     assert sorted(r["fields"]) == sorted(["U", "V", "W"] + ck.scalar_names(p))

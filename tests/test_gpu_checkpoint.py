@@ -34,10 +34,10 @@ def test_save_matches_oracle(tmp_path):
     p, g, u, th = kh(48, 33, 36)
     o = oracle_run(p, g, u, th, 0.01, 3)
     with to_gpu(o) as c:
-        ck.save(c, str(tmp_path / "gpu.npz"), save_pressure=True)
-    oracle_save(o, str(tmp_path / "cpu.npz"), save_pressure=True)
-    a, b = np.load(str(tmp_path / "gpu.npz")), np.load(str(tmp_path / "cpu.npz"))
-    assert sorted(a.files) == sorted(b.files)
+        ck.save(c, str(tmp_path / "gpu.h5"), save_pressure=True)
+    oracle_save(o, str(tmp_path / "cpu.h5"), save_pressure=True)
+    a, b = ck.datasets(str(tmp_path / "gpu.h5")), ck.datasets(str(tmp_path / "cpu.h5"))
+    assert sorted(a) == sorted(b)
     for k in ("U", "V", "W", "TH01", "P"):
         assert a[k].shape == (p.nz, p.ny, p.nx)
         assert rel(a[k], b[k]) < 1e-13, k
@@ -50,7 +50,7 @@ def test_load_and_continue_matches_oracle(tmp_path, save_pressure):
     without P) and APPLY_BC_VEL after the read, then three steps."""
     p, g, u, th = channel(48, 33, 40)
     o = oracle_run(p, g, u, th, 1e-3, 3)
-    path = str(tmp_path / "out.npz")
+    path = str(tmp_path / "out.h5")
     oracle_save(o, path, save_pressure)
     o2 = Oracle(p, g, 1e-3)
     oracle_load(o2, path)

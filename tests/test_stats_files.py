@@ -4,7 +4,7 @@ layout of WriteStatH5 / WriteHDF5_real (for/hdf5.f:1345-1622)."""
 import numpy as np
 import pytest
 
-from diablo_b200 import grid as G, params as P, statsfile
+from diablo_b200 import grid as G, h5, params as P, statsfile
 from diablo_b200.channel import MEAN_NAMES, SCAL_NAMES
 from oracle.oracle import Oracle
 
@@ -61,8 +61,12 @@ def test_statfile_layout(tmp_path):
     f2 = statsfile.StatFile(path)                    # reopened: SAMPLES continues
     assert f2.samples("ume") == 2 and f2.samples("time") == 1 and f2.samples("vme") == 0
     f2.write_real("time", 0.75)
-    raw = np.load(path)                              # plain numpy reads the datasets
-    assert np.array_equal(raw["ume/0002"], np.arange(5.0) + 1) and float(raw["ume/0002@Time"]) == 0.75
+    raw = h5.read(path)                              # the HDF5 tree WriteStatH5 creates
+    ume = raw.children["ume"]
+    assert int(ume.attrs["SAMPLES"]) == 2 and ume.attrs["SAMPLES"].shape == ()
+    assert np.array_equal(ume.children["0002"].data, np.arange(5.0) + 1)
+    assert ume.children["0002"].data.dtype == np.dtype("<f8")
+    assert float(ume.children["0002"].attrs["Time"]) == 0.75 and ume.children["0002"].attrs["Time"].shape == ()
     r = statsfile.read(path)
     assert r["ume"]["SAMPLES"] == 2 and r["ume"]["data"].shape == (2, 5)
     assert list(r["ume"]["Time"]) == [0.5, 0.75]
