@@ -14,6 +14,16 @@ so that the dimensionless loss weighs samples as the error of the
 dimensional stresses does (otherwise the quiescent regions, where tau/s is
 noise over a small G^2, would dominate it).
 
+For an LES, the stresses the model must supply are those of the filter the
+LES itself applies: the spectral cutoff at its resolved modes, not a
+top-hat.  cutoff_snapshots collects those: the DNS state truncated to the
+LES modes is put on an LES-grid instance, whose sampler (width 1) gives the
+features the LES computes at run time at every LES point, and the targets
+tau_ij = T(u_i u_j) - T(T(u_i) T(u_j)) (T the truncation) are formed on the
+host by FFT from the DNS velocity.  Trained on these, the closure improves
+the LES a posteriori (a_posteriori); trained on top-hat stresses, which are
+larger than the cutoff's at the same width, it over-dissipates.
+
 The method without the network is an eddy viscosity: tau^d_ij = -2 C Delta^2
 |S| S_ij for the deviatoric stresses.  Its a-priori error is bounded below
 by the best coefficient for each y-plane fitted by least squares to the
@@ -29,6 +39,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from .channel import Channel
+from .layout import dealiased
 from .mlp import NIN, NOUT, SgsMlp, init_params, normalisation
 
 _PAIRS = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
@@ -59,6 +70,98 @@ def dns_snapshots(p, grid, dt, u, th, count: int, every: int, warmup: int = 0, w
             xs.append(x)
             ts.append(t)
             ss.append(s)
+    m = xs[0].shape[0]
+    snap = np.repeat(np.arange(count), m)
+    return Snapshots(np.concatenate(xs), np.concatenate(ts), np.concatenate(ss), snap, m,
+                     _time.perf_counter() - t0)
+
+
+def _to_physical(spec: np.ndarray, nx: int, nz: int) -> np.ndarray:
+    """Dealiased Fourier block [planes][2 nkz + 1][nkx + 1] (kz = -k at index
+    2 nkz + 1 - k, coefficients normalised by NX NZ) to physical values
+    [planes][nz][nx] on an nx x nz grid: the plain sum over the modes."""
+    nkz, nkx = (spec.shape[1] - 1) // 2, spec.shape[2] - 1
+    full = np.zeros((spec.shape[0], nz, nx // 2 + 1), dtype=np.complex128)
+    full[:, : nkz + 1, : nkx + 1] = spec[:, : nkz + 1]
+    for k in range(1, nkz + 1):
+        full[:, nz - k, : nkx + 1] = spec[:, 2 * nkz + 1 - k]
+    return np.fft.irfft(np.fft.ifft(full, axis=1, norm="forward"), n=nx, axis=2, norm="forward")
+
+
+def _to_fourier(f: np.ndarray, nkx: int, nkz: int) -> np.ndarray:
+    """Physical [planes][nz][nx] to the dealiased block of modes |kx| <= nkx,
+    |kz| <= nkz (the inverse of _to_physical on those modes)."""
+    nz = f.shape[1]
+    full = np.fft.fft(np.fft.rfft(f, axis=2, norm="forward"), axis=1, norm="forward")
+    out = np.zeros((f.shape[0], 2 * nkz + 1, nkx + 1), dtype=np.complex128)
+    out[:, : nkz + 1] = full[:, : nkz + 1, : nkx + 1]
+    for k in range(1, nkz + 1):
+        out[:, 2 * nkz + 1 - k] = full[:, nz - k, : nkx + 1]
+    return out
+
+
+def cutoff_stresses(p, q, s: dict) -> np.ndarray:
+    """Subgrid stresses of the spectral cutoff that an LES on q's grid
+    resolves (the modes coarsen keeps), at q's physical points of planes
+    J = 2..NY-1 in the sampler's order [J][z][x][6]:
+    tau_ij = T(u_i u_j) - T(T(u_i) T(u_j)), T the truncation to the LES modes
+    and u the DNS velocity of state s (U2 averaged to GYF, as the sampler
+    does).  The DNS products are formed on p's grid, where the 2/3 rule
+    keeps their aliases off the LES modes; the resolved products on q's
+    grid, likewise."""
+    ny = p.ny
+    nkx, nkz = q.nx // 3, q.nz // 3
+    cu = s["cu"]
+
+    def dns(k, lo, hi):
+        return _to_physical(dealiased(p, cu[k])[lo:hi], p.nx, p.nz)
+
+    def les(k, lo, hi):
+        return _to_physical(dealiased(p, cu[k])[lo:hi][:, _les_kz(p, nkz)][:, :, : nkx + 1], q.nx, q.nz)
+
+    u = [dns(0, 2, ny), 0.5 * (dns(1, 2, ny) + dns(1, 3, ny + 1)), dns(2, 2, ny)]
+    uc = [les(0, 2, ny), 0.5 * (les(1, 2, ny) + les(1, 3, ny + 1)), les(2, 2, ny)]
+    out = np.empty((ny - 2, q.nz, q.nx, 6), dtype=np.float64)
+    for n, (a, b) in enumerate(_PAIRS):
+        full = _to_physical(_to_fourier(u[a] * u[b], nkx, nkz), q.nx, q.nz)
+        res = _to_physical(_to_fourier(uc[a] * uc[b], nkx, nkz), q.nx, q.nz)
+        out[..., n] = full - res
+    return out
+
+
+def _les_kz(p, nkz: int) -> np.ndarray:
+    """Indices, in p's dealiased kz order, of the modes |kz| <= nkz in the
+    same order for the smaller grid (0..nkz, then -nkz..-1)."""
+    tf = 2 * (p.nz // 3)
+    return np.array(list(range(nkz + 1)) + [tf + 1 - k for k in range(nkz, 0, -1)])
+
+
+def cutoff_snapshots(p, grid, dt, u, th, count: int, every: int, warmup: int = 0, factor: int = 3) -> Snapshots:
+    """Run the DNS on the GPU and collect `count` snapshots for an LES on the
+    grid `factor` times coarser in x and z, one every `every` steps after
+    `warmup`: the features at every LES point of planes 2..NY-1 are those
+    the LES computes at run time (Channel.sgs_samples with width 1 on an LES
+    grid instance holding the DNS state truncated to the LES modes), and the
+    targets are the spectral-cutoff stresses (cutoff_stresses) in the same
+    dimensionless form."""
+    t0 = _time.perf_counter()
+    q = p.copy()
+    q.nx, q.nz = p.nx // factor, p.nz // factor
+    xs, ts, ss = [], [], []
+    with Channel(p, grid, dt) as c, Channel(q, grid, dt) as lc:
+        c.init_from_physical(u, th)
+        c.step(warmup)
+        for _ in range(count):
+            c.step(every)
+            s = c.download()
+            lc.upload([coarsen(p, s["cu"][k], q) for k in range(3)], coarsen(p, s["cp"], q),
+                      np.stack([coarsen(p, s["cth"][n], q) for n in range(p.n_th)]) if p.n_th else None)
+            x, _, sc = lc.sgs_samples(1, 1)
+            tau = cutoff_stresses(p, q, s).reshape(-1, 6)
+            inv = np.where(sc > 0, 1.0 / np.maximum(sc.astype(np.float64), 1e-300), 0.0)
+            xs.append(x)
+            ts.append((tau * inv[:, None]).astype(np.float32))
+            ss.append(sc)
     m = xs[0].shape[0]
     snap = np.repeat(np.arange(count), m)
     return Snapshots(np.concatenate(xs), np.concatenate(ts), np.concatenate(ss), snap, m,
