@@ -64,7 +64,7 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-les", action="store_true")
     ap.add_argument("--no-closure", action="store_true")
-    ap.add_argument("--closure-snapshots", type=int, default=400)
+    ap.add_argument("--closure-snapshots", type=int, default=60)
     ap.add_argument("--closure-steps", type=int, default=20000)
     ap.add_argument("--only", choices=["les", "closure"], default=None,
                     help="run one leg alone and print its JSON (for profiling captures)")
@@ -368,32 +368,20 @@ def les_rates(w, u, th, steps: int, warmup: int, torch, cpu: bool) -> dict:
     return out
 
 
-def closure_rates(snapshots: int, steps: int, seed: int = 41, every: int = 5) -> dict:
-    """The learned closure on this solver's DNS: Kelvin-Helmholtz layer
-    96x65x96 (amp 0.2 seeded noise, dt 0.01) and an LES on 32x65x32.
-    `snapshots` snapshots, one every `every` steps after 10, of the stresses
-    of the spectral cutoff the LES resolves, at every LES point, with the
-    features the LES computes at run time (closure.cutoff_snapshots); seeded
-    80/20 split by snapshot, `steps` Adam steps of 4096 samples; a-priori
+def closure_rates(snapshots: int, steps: int) -> dict:
+    """The learned closure in a channel LES (closure.channel_les_study):
+    Re_tau 180 channel DNS 192x65x192 and LES 64x65x64, `snapshots`
+    spectral-cutoff snapshots, `steps` Adam steps of 4096 samples, a-priori
     errors on the held-out snapshots against the best per-plane eddy
-    viscosity; then the a-posteriori comparison over the same steps: the
-    LES with no model, the dynamic model and the trained closure against
-    the truncated DNS."""
-    from diablo_b200 import closure, grid as G, ics, params as P
+    viscosity, then 2000 LES steps with no model, the dynamic model and the
+    trained closure against the truncated DNS, profiles averaged every 100
+    steps."""
+    from diablo_b200 import closure
 
-    p = P.kelvin_helmholtz(96, 65, 96)
-    g = G.channel_grid(G.uniform_gy(p.ny, -10.0, 10.0))
-    u, th = ics.shear_layer(p, g, seed=seed, amp=0.2)
-    data = closure.cutoff_snapshots(p, g, 0.01, u, th, count=snapshots, every=every, warmup=10)
-    rep = closure.train_and_evaluate(data, seed=seed + 1, steps=steps, batch=4096, lr=2e-3)
-    out = rep.summary()
+    out = closure.channel_les_study(snapshots=snapshots, adam_steps=steps)
     flop_per_sample = 3 * 2 * (11 * 64 + 2 * 64 * 64 + 64 * 6)     # forward + backward
-    out.update({"snapshots": snapshots, "snapshot_seconds": data.seconds, "adam_steps": steps, "batch": 4096,
-                "train_samples_per_s": steps * 4096 / rep.train_seconds,
-                "train_tflops": steps * 4096 * flop_per_sample / rep.train_seconds / 1e12,
-                "workload": f"KH 96x65x96 DNS, amp 0.2, dt 0.01; LES 32x65x32; spectral-cutoff stresses at every "
-                            f"LES point, one snapshot every {every} steps; seeded 80/20 split by snapshot"})
-    out["a_posteriori"] = closure.a_posteriori(p, g, 0.01, u, th, snapshots * every + 10, rep.params)
+    out.update({"train_samples_per_s": steps * 4096 / out["train_seconds"],
+                "train_tflops": steps * 4096 * flop_per_sample / out["train_seconds"] / 1e12})
     return out
 
 

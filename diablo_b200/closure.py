@@ -136,20 +136,28 @@ def _les_kz(p, nkz: int) -> np.ndarray:
     return np.array(list(range(nkz + 1)) + [tf + 1 - k for k in range(nkz, 0, -1)])
 
 
-def cutoff_snapshots(p, grid, dt, u, th, count: int, every: int, warmup: int = 0, factor: int = 3) -> Snapshots:
+def cutoff_snapshots(p, grid, dt, u, th, count: int, every: int, warmup: int = 0, factor: int = 3,
+                     start: dict | None = None) -> Snapshots:
     """Run the DNS on the GPU and collect `count` snapshots for an LES on the
     grid `factor` times coarser in x and z, one every `every` steps after
     `warmup`: the features at every LES point of planes 2..NY-1 are those
     the LES computes at run time (Channel.sgs_samples with width 1 on an LES
     grid instance holding the DNS state truncated to the LES modes), and the
     targets are the spectral-cutoff stresses (cutoff_stresses) in the same
-    dimensionless form."""
+    dimensionless form.  The DNS starts from `start` (a downloaded state)
+    when given, else from the physical fields u, th."""
+    from .params import PREC_FP64
+
     t0 = _time.perf_counter()
     q = p.copy()
     q.nx, q.nz = p.nx // factor, p.nz // factor
+    q.precision = PREC_FP64
     xs, ts, ss = [], [], []
     with Channel(p, grid, dt) as c, Channel(q, grid, dt) as lc:
-        c.init_from_physical(u, th)
+        if start is None:
+            c.init_from_physical(u, th)
+        else:
+            c.upload(start["cu"], start["cp"], start["cth"] if p.n_th else None)
         c.step(warmup)
         for _ in range(count):
             c.step(every)
@@ -249,9 +257,11 @@ class ClosureReport:
     params: np.ndarray = field(repr=False, default=None)
 
     def summary(self) -> dict:
+        # mini-batch losses of heavy-tailed targets are noisy: window means
         return {"train_samples": self.train_samples, "test_samples": self.test_samples,
-                "train_seconds": self.train_seconds, "final_loss": float(self.losses[-1]),
-                "first_loss": float(self.losses[0]),
+                "train_seconds": self.train_seconds, "final_loss": float(np.mean(self.losses[-1000:])),
+                "first_loss": float(np.mean(self.losses[:10])),
+                "loss_windows": "first: mean of the first 10 mini-batches; final: of the last 1000",
                 "mlp_test_error": self.mlp_test_error,
                 "mlp_test_error_deviatoric": self.mlp_test_error_deviatoric,
                 "eddy_viscosity_best_plane_fit_test_error": self.eddy_viscosity_test_error}
@@ -325,26 +335,27 @@ def _profiles(stats: np.ndarray) -> dict:
     return {k: stats[STAT_INDEX[k]] for k in ("ume", "urms", "vrms", "wrms", "uv")}
 
 
-def a_posteriori(p, grid, dt, u, th, steps: int, params: np.ndarray, factor: int = 3) -> dict:
+def a_posteriori(p, grid, dt, u, th, steps: int, params: np.ndarray, factor: int = 3, start: dict | None = None,
+                 average_every: int = 0) -> dict:
     """DNS on p's grid and LES on the grid coarsened `factor` times in x and
     z, from the DNS's initial state truncated to the LES modes, `steps`
     steps each; mean-velocity and Reynolds-stress profiles of each LES (no
     model, the dynamic model, the closure with `params`) against the
-    filtered DNS (the final DNS state truncated the same way) as relative L2
-    errors over the planes."""
+    filtered DNS (the DNS state truncated the same way) as relative L2
+    errors over the planes.  The initial state is `start` (a downloaded DNS
+    state) when given, else the physical fields u, th.  With average_every
+    > 0 the profiles are means over the states every average_every steps
+    (a turbulent flow's instantaneous plane averages fluctuate); else those
+    of the final states.  p's dt must be fixed, so that the runs meet at the
+    same times."""
     from .mlp import SgsMlp
+    from .params import PREC_FP64
 
     q = p.copy()
     q.nx, q.nz = p.nx // factor, p.nz // factor
     q.les, q.create_new_flow = 1, 0
-    with Channel(p, grid, dt) as c:
-        c.init_from_physical(u, th)
-        s0 = c.download()
-        t0 = _time.perf_counter()
-        c.step(steps)
-        c.synchronize()
-        dns_seconds = _time.perf_counter() - t0
-        s1 = c.download()
+    q.precision = PREC_FP64          # the LES branch runs in FP64
+    chunk = average_every if average_every > 0 else steps
 
     def coarse_channel(s, model):
         r = q.copy()
@@ -357,10 +368,29 @@ def a_posteriori(p, grid, dt, u, th, steps: int, params: np.ndarray, factor: int
                   np.stack([coarsen(p, s["cth"][n], q) for n in range(p.n_th)]) if p.n_th else None)
         return ch
 
-    with coarse_channel(s1, 0) as ref:
-        target = _profiles(ref.stats())
+    def mean_profiles(samples):
+        return {k: np.mean([smp[k] for smp in samples], axis=0) for k in samples[0]}
+
+    targets = []
+    with Channel(p, grid, dt) as c:
+        if start is None:
+            c.init_from_physical(u, th)
+        else:
+            c.upload(start["cu"], start["cp"], start["cth"] if p.n_th else None)
+        s0 = c.download()
+        t0 = _time.perf_counter()
+        done = 0
+        while done < steps:
+            n = min(chunk, steps - done)
+            c.step(n)
+            done += n
+            with coarse_channel(c.download(), 0) as ref:
+                targets.append(_profiles(ref.stats()))
+        c.synchronize()
+        dns_seconds = _time.perf_counter() - t0
+    target = mean_profiles(targets)
     out = {"dns_grid": [p.nx, p.ny, p.nz], "les_grid": [q.nx, q.ny, q.nz], "steps": steps, "dt": dt,
-           "dns_seconds": dns_seconds}
+           "dns_seconds": dns_seconds, "profile_samples": len(targets)}
     for name, model in (("no_model", 0), ("dynamic", 2), ("closure", 4)):
         ch = coarse_channel(s0, model)
         m = None
@@ -368,10 +398,15 @@ def a_posteriori(p, grid, dt, u, th, steps: int, params: np.ndarray, factor: int
             m = SgsMlp(params)
             ch.set_sgs_mlp(m)
         t0 = _time.perf_counter()
-        ch.step(steps)
+        samples, done = [], 0
+        while done < steps:
+            n = min(chunk, steps - done)
+            ch.step(n)
+            done += n
+            samples.append(_profiles(ch.stats()))
         ch.synchronize()
         el = _time.perf_counter() - t0
-        prof = _profiles(ch.stats())
+        prof = mean_profiles(samples)
         ch.close()
         if m is not None:
             m.close()
@@ -380,4 +415,39 @@ def a_posteriori(p, grid, dt, u, th, steps: int, params: np.ndarray, factor: int
             d = np.linalg.norm(prof[k] - ref_prof)
             err[k] = float(d / max(np.linalg.norm(ref_prof), 1e-300)) if np.isfinite(d) else float("inf")
         out[name] = {"profile_errors": err, "seconds": el}
+    return out
+
+
+def channel_les_study(snapshots: int = 60, every: int = 30, spin: int = 20000, adam_steps: int = 20000,
+                      les_steps: int = 2000, seed: int = 42, dt: float = 1.2e-3) -> dict:
+    """The learned closure in a channel LES: turbulent channel at Re_tau 180,
+    DNS on 192x65x192 (FP32-split, fixed dt), LES on 64x65x64 (the DNS grid
+    coarsened 3 times in x and z, same y grid).  The DNS starts from
+    ics.tripped_poiseuille and runs `spin` steps to a turbulent state S;
+    after 4000 more steps `snapshots` cutoff snapshots are taken one every
+    `every` steps (cutoff_snapshots), the closure is trained on them
+    (`adam_steps` Adam steps of 4096, seeded 80/20 split by snapshot), and
+    from S -- before the training window -- the LES with no model, the
+    dynamic model and the closure run `les_steps` steps beside the DNS, with
+    the profiles averaged every 100 steps (a_posteriori)."""
+    from . import grid as G, ics, params as P
+
+    p = P.turbulent_channel(192, 65, 192, re_tau=180.0, precision=P.PREC_FP32SPLIT, variable_dt=False)
+    g = G.channel_grid(G.create_grid(1, 65, 2.0, 1.75))
+    u, th = ics.tripped_poiseuille(p, g, 18.0, seed=5)
+    t0 = _time.perf_counter()
+    with Channel(p, g, dt) as c:
+        c.init_from_physical(u, th)
+        c.step(spin)
+        start = c.download()
+    spin_seconds = _time.perf_counter() - t0
+    data = cutoff_snapshots(p, g, dt, None, None, count=snapshots, every=every, warmup=4000, start=start)
+    rep = train_and_evaluate(data, seed=seed, steps=adam_steps, batch=4096, lr=2e-3)
+    out = rep.summary()
+    out.update({"snapshots": snapshots, "snapshot_every": every, "snapshot_seconds": data.seconds,
+                "spin_up_steps": spin, "spin_up_seconds": spin_seconds, "adam_steps": adam_steps, "batch": 4096,
+                "workload": f"channel Re_tau 180: DNS 192x65x192 FP32-split, LES 64x65x64, dt {dt}; tripped "
+                            f"Poiseuille, {spin} spin-up steps; {snapshots} spectral-cutoff snapshots one every "
+                            f"{every} steps after 4000 more; seeded 80/20 split by snapshot"})
+    out["a_posteriori"] = a_posteriori(p, g, dt, None, None, les_steps, rep.params, start=start, average_every=100)
     return out

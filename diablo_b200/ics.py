@@ -82,3 +82,26 @@ def poiseuille(p: DiabloParams, grid: ChannelGrid, u_center: float, seed: int = 
         prof = (hi - lo) * (y[1: ny + 1] + 1.0) / 2.0 + lo
         th[n, 1: ny + 1, :nz, :nx] = prof[:, None, None]
     return u, th[: p.n_th]
+
+
+def tripped_poiseuille(p: DiabloParams, grid: ChannelGrid, u_center: float, seed: int = 1234,
+                       amp: float = 0.3, kx_max: int = 3, kz_max: int = 6) -> tuple[np.ndarray, np.ndarray]:
+    """The Poiseuille field of `poiseuille` without its white noise, plus a
+    large-scale perturbation that trips a channel to turbulence: seeded
+    normals low-pass filtered to |kx| <= kx_max, |kz| <= kz_max, scaled to
+    unit RMS over planes 1..NY and then by amp*u_center*(1-GYF^2), on every
+    component (the projection that follows makes it divergence-free).  White
+    noise of the same amplitude decays before the flow transitions; this one
+    gives a Re_tau 180 channel its turbulent statistics after about 25 time
+    units."""
+    u, th = poiseuille(p, grid, u_center, seed=seed, noise=0.0)
+    nx, nz, ny = p.nx, p.nz, p.ny
+    env = np.clip(1.0 - grid.gyf ** 2, 0.0, None)[:, None, None]
+    kz = np.abs(np.fft.fftfreq(nz, 1.0 / nz))[:, None]
+    keep = (kz <= kz_max) & (np.arange(nx // 2 + 1)[None, :] <= kx_max)
+    for c in range(3):
+        r = normals(seed + 104729 * (c + 1), (ny + 2) * nz * nx).reshape(ny + 2, nz, nx)
+        lp = np.fft.irfft2(np.fft.rfft2(r, axes=(1, 2)) * keep[None], s=(nz, nx), axes=(1, 2))
+        lp /= lp[1: ny + 1].std()
+        u[c, :, :nz, :nx] += amp * u_center * env * lp
+    return u, th
