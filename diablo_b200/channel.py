@@ -43,7 +43,7 @@ EXPORTS = [
     "diablo_gpu_rem_div_chan_noalloc", "diablo_gpu_autotune", "diablo_gpu_batch_create",
     "diablo_gpu_batch_step", "diablo_gpu_batch_destroy", "diablo_gpu_filter_chan", "diablo_gpu_download_nu_t",
     "diablo_gpu_mean_stats", "diablo_gpu_set_user_rhs",
-    "diablo_gpu_sgs_samples", "diablo_gpu_set_sgs_mlp",
+    "diablo_gpu_sgs_samples", "diablo_gpu_set_sgs_mlp", "diablo_gpu_step_graph",
 ]
 KERNEL_NAMES = ["zinv", "products", "zfwd_nl", "cn_coef", "column", "remdiv", "cfl", "other"]
 
@@ -108,6 +108,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.diablo_gpu_autotune.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
     L.diablo_gpu_batch_create.argtypes = [ctypes.POINTER(vp), dp, ip, ctypes.POINTER(vp)]
     L.diablo_gpu_batch_step.argtypes = [vp, ip]
+    L.diablo_gpu_step_graph.argtypes = [vp, ip, ip, dp, dp, dp]
     L.diablo_gpu_batch_destroy.argtypes = [vp]
     L.diablo_gpu_filter_chan.argtypes = [vp, ip]
     L.diablo_gpu_download_nu_t.argtypes = [vp, dp]
@@ -289,6 +290,27 @@ class Channel:
             for rk in (1, 2, 3):
                 self.rk_chan_1(rk)
             self.time += self.delta_t
+
+    def step_graph(self, n: int = 1) -> bool:
+        """n time steps as replays of one CUDA graph of a whole RK3 step
+        (diablo_gpu_step_graph): the same results as step(n), with one
+        launch per step instead of one per kernel.  Falls back to step(n) and
+        returns False when the step is not static (variable dt, time-dependent
+        forcing, a user right-hand side, profiling, or an LES whose subgrid
+        model starts within these steps)."""
+        if n <= 0:
+            return True
+        hb = np.ascontiguousarray(self.h_bar, dtype=np.float64)
+        bb = np.ascontiguousarray(self.beta_bar, dtype=np.float64)
+        zb = np.ascontiguousarray(self.zeta_bar, dtype=np.float64)
+        rc = self.L.diablo_gpu_step_graph(self._h, int(n), self.time_step, _dp(hb), _dp(bb), _dp(zb))
+        if rc == DIABLO_ENOTSUP:
+            self.step(n)
+            return False
+        _check(rc, "diablo_gpu_step_graph")
+        self.time_step += n
+        self.time += n * self.delta_t
+        return True
 
     def synchronize(self) -> None:
         _check(self.L.diablo_gpu_synchronize(self._h), "diablo_gpu_synchronize")

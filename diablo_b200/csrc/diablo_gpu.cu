@@ -100,6 +100,14 @@ struct Handle {
     bool profiling = false;
     struct Rec { int kind; cudaEvent_t a, b; };
     std::vector<Rec> recs;
+    // one RK3 step as a CUDA graph (diablo_gpu_step_graph) and what it was
+    // captured with: H_BAR, BETA_BAR, ZETA_BAR, the launch shapes, the network
+    cudaGraph_t sg_graph = nullptr;
+    cudaGraphExec_t sg_exec = nullptr;
+    double sg_coef[9] = {};
+    int sg_prod = 0, sg_zf = 0;
+    void* sg_mlp = nullptr;
+    long long sg_launches = 0;    // kernel launches of one captured step
 };
 
 // Bracket a launch with events when profiling (kinds: DIABLO_KERNEL_*).
@@ -149,6 +157,8 @@ void* make_twiddles(int n, cudaStream_t st, cudaError_t* err) {
 
 void free_handle(Handle* h) {
     if (!h) return;
+    if (h->sg_exec) cudaGraphExecDestroy(h->sg_exec);
+    if (h->sg_graph) cudaGraphDestroy(h->sg_graph);
     for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     void* ptrs[] = {h->d_dy, h->d_dyf, h->d_kx, h->d_kz, h->cu, h->cf, h->cp, h->phi, h->api_s,
                     h->nl, h->xb, h->yb, h->bsc, h->gsc, h->phys, h->d_gyf, h->pw, h->d_me, h->d_sums, h->d_msums, h->d_nan, h->ufa, h->uphys, h->d_tabs, h->d_phitab,
@@ -1057,6 +1067,72 @@ int diablo_gpu_rk_chan_1(void* handle, int rk_step, int time_step, double time, 
     // pressure update with the h of this substage
     if ((rc = courant(h, delta_t, h_bar))) return rc;
     return rem_div(h, 1, 1.0 / TEMP4);
+}
+
+// n RK3 steps as replays of one captured step.  The step is static when its
+// launches and their arguments do not change from step to step: a fixed time
+// step (COURANT reads DELTA_T back to the host), no user right-hand side (host
+// callbacks), forcing that does not depend on time, and, on the LES branch,
+// the subgrid model running from the first of these steps on.  The first
+// call after a change of H_BAR/BETA_BAR/ZETA_BAR, of the launch shapes or of
+// the attached network runs one step directly (it sets up the lazily
+// allocated buffers and the cached CN factors) and captures the next.
+int diablo_gpu_step_graph(void* handle, int nsteps, int time_step, const double* h_bar, const double* beta_bar,
+                          const double* zeta_bar) {
+    Handle* h = (Handle*)handle;
+    if (!h || !h_bar || !beta_bar || !zeta_bar) return fail(DIABLO_EINVAL, "null pointer argument");
+    if (nsteps < 0) return fail(DIABLO_EINVAL, "nsteps must be >= 0");
+    const diablo_params& p = h->p;
+    if (p.variable_dt) return fail(DIABLO_ENOTSUP, "step graph: VARIABLE_DT reads DELTA_T back every step");
+    if (p.f_type == 2) return fail(DIABLO_ENOTSUP, "step graph: the forcing depends on time");
+    if (h->urhs_fn[0] || h->urhs_fn[1]) return fail(DIABLO_ENOTSUP, "step graph: a user right-hand side is set");
+    if (h->profiling) return fail(DIABLO_ENOTSUP, "step graph: kernel profiling is on");
+    if (p.les && p.create_new_flow && time_step + 1 <= 100)
+        return fail(DIABLO_ENOTSUP, "step graph: the subgrid model starts within these steps");
+    if (nsteps == 0) return DIABLO_OK;
+    double coef[9];
+    for (int r = 0; r < 3; ++r) { coef[r] = h_bar[r]; coef[3 + r] = beta_bar[r]; coef[6 + r] = zeta_bar[r]; }
+    bool same = h->sg_exec && h->sg_prod == h->prod_chunk && h->sg_zf == h->zf_planes && h->sg_mlp == h->mlp;
+    for (int q = 0; q < 9 && same; ++q) same = h->sg_coef[q] == coef[q];
+    double hb[3] = {h_bar[0], h_bar[1], h_bar[2]}, dt = 0.0;
+    int rc;
+    if (!same) {
+        if (h->sg_exec) { cudaGraphExecDestroy(h->sg_exec); h->sg_exec = nullptr; }
+        if (h->sg_graph) { cudaGraphDestroy(h->sg_graph); h->sg_graph = nullptr; }
+        for (int r = 1; r <= 3; ++r)
+            if ((rc = diablo_gpu_rk_chan_1(handle, r, time_step + 1, 0.0, &dt, hb, beta_bar, zeta_bar))) return rc;
+        nsteps -= 1;
+        const long long l0 = h->launches;
+        CK(cudaStreamSynchronize(h->st));
+        cudaError_t e = cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed);
+        if (e != cudaSuccess) return fail(DIABLO_ECUDA, std::string("step graph capture: ") + cudaGetErrorString(e));
+        rc = DIABLO_OK;
+        for (int r = 1; r <= 3 && rc == DIABLO_OK; ++r)
+            rc = diablo_gpu_rk_chan_1(handle, r, time_step + 2, 0.0, &dt, hb, beta_bar, zeta_bar);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(h->st, &g);
+        if (rc != DIABLO_OK || ee != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc != DIABLO_OK ? rc : fail(DIABLO_ECUDA, std::string("step graph end capture: ") + cudaGetErrorString(ee));
+        }
+        e = cudaGraphInstantiate(&h->sg_exec, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            h->sg_exec = nullptr;
+            return fail(DIABLO_ECUDA, std::string("step graph instantiate: ") + cudaGetErrorString(e));
+        }
+        h->sg_graph = g;
+        h->sg_launches = h->launches - l0;
+        h->launches = l0;
+        for (int q = 0; q < 9; ++q) h->sg_coef[q] = coef[q];
+        h->sg_prod = h->prod_chunk;
+        h->sg_zf = h->zf_planes;
+        h->sg_mlp = h->mlp;
+    }
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(h->sg_exec, h->st));
+    h->launches += h->sg_launches * nsteps;
+    return DIABLO_OK;
 }
 
 int diablo_gpu_download_nu_t(void* handle, double* nu_t) {

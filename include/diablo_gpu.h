@@ -308,6 +308,25 @@ int diablo_gpu_filter_chan(void* handle, int n);
  * temporary copy of the state. */
 int diablo_gpu_autotune(void* handle, int* prod_chunk, int* zf_planes);
 
+/* nsteps RK3 steps (the three RK_CHAN_1 substages each, as in diablo.f:66-111
+ * without statistics or I/O) of one instance, replayed from one CUDA graph of
+ * a whole step.  Small grids spend most of a step launching kernels; the
+ * graph launches a step at once.  No counterpart in the reference, whose time
+ * loop calls the substages one by one.  The step must be static: VARIABLE_DT
+ * 0, F_TYPE != 2, no user right-hand side, profiling off and, on the LES
+ * branch, the subgrid model running (after the CREATE_NEW_FLOW spin-up of
+ * 100 steps); otherwise DIABLO_ENOTSUP and the caller steps with
+ * diablo_gpu_rk_chan_1.  h_bar, beta_bar, zeta_bar are the substage
+ * coefficients of the fixed time step; time_step is the number of the step
+ * before the first one taken.  The first call, and any call after a change of
+ * the coefficients, of diablo_gpu_autotune's launch shapes or of the attached
+ * network, runs one step directly and captures the next; later calls only
+ * launch the graph.  Asynchronous on the handle's stream (diablo_gpu_synchronize
+ * waits and reports DIABLO_ENAN).  The results equal nsteps calls of the
+ * three substages. */
+int diablo_gpu_step_graph(void* handle, int nsteps, int time_step, const double* h_bar, const double* beta_bar,
+                          const double* zeta_bar);
+
 /* Batched instances (configuration of many independent channels of uneven
  * sizes; the reference's ensemble driver, dummy_code/ensem_dummy.f, is an
  * empty stub).  diablo_gpu_batch_create captures one full RK3 step (the three
