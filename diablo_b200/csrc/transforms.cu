@@ -163,12 +163,19 @@ __device__ __forceinline__ cpx<T> extract_real_forward(const cpx<T>* buf, const 
 constexpr int PROD_G = 16;          // rows transformed together by the products kernel
 constexpr int RT_VMAX = 12;         // run-time path: values per thread
 
-template <typename T, int MC, int S, class L>
+// nrows <= PROD_G * ZB rows of length M (MC at compile time, else the plan's)
+template <typename T, int MC, int S, int ZB = 1, class L>
 __device__ __forceinline__ void row_fft(cpx<T>* buf, int nrows, const L& lay, const FftPlan& P,
                                         const cpx<T>* __restrict__ tw) {
-    if constexpr (MC > 0) fft_ct<T, MC, S, L, PROD_G, 256>(buf, nrows, lay, tw);
+    if constexpr (MC > 0) fft_ct<T, MC, S, L, PROD_G * ZB, 256>(buf, nrows, lay, tw);
     else smem_fft<T, RT_VMAX>(buf, nrows, lay, P, tw, S);
 }
+
+// z-rows per products block: several at small NX, where one row's transforms
+// leave most of the 256 threads idle between barriers (shared memory of four
+// FP32 rows or two FP64 rows at NX = 128: 76 KB)
+template <typename T, int MC>
+__host__ __device__ constexpr int products_zb() { return (MC > 0 && MC <= 64) ? (sizeof(T) == 4 ? 4 : 2) : 1; }
 
 // ---------------------------------------------------------------------------
 // K2: per z-row, marching over planes.  Iteration J transforms, in one
@@ -200,7 +207,9 @@ __device__ __forceinline__ int field_sources(int q, int* sp, bool* sx) {
     return 2;
 }
 
-template <typename T, int MC>
+// ZB z-rows per block (rows z0 .. z0+ZB-1 side by side in every buffer): at
+// small NX one row's transforms leave most of the block idle between barriers.
+template <typename T, int MC, int ZB>
 __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __restrict__ X, cpx<T>* __restrict__ Y,
                                               int jlo, int jhi, int chunk, int group, const double* __restrict__ dy,
                                               const double* __restrict__ dyf, const double* __restrict__ kxw,
@@ -215,19 +224,20 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
     using Lay = typename std::conditional<(MC > 0), RowLayoutCT<MC>, RowLayoutRT>::type;
     Lay lay;
     if constexpr (MC == 0) lay.pitch = row_pitch(M);
-    T* ring = reinterpret_cast<T*>(smem_raw);                                 // [RING][nf][nx]
-    cpx<T>* stw = reinterpret_cast<cpx<T>*>(ring + (size_t)RING * nf * nx);  // twiddles: M then NX
-    cpx<T>* buf = stw + 3 * M;                                                // [group][pitch]
+    const size_t ringz = (size_t)RING * nf * nx;                              // one z-row's ring
+    T* ring0 = reinterpret_cast<T*>(smem_raw);                                // [ZB][RING][nf][nx]
+    cpx<T>* stw = reinterpret_cast<cpx<T>*>(ring0 + ringz * ZB);              // twiddles: M then NX
+    cpx<T>* buf = stw + 3 * M;                                                // [ZB * group][pitch]
     T* tbuf = reinterpret_cast<T*>(buf);
-    // [2][nf][ldx] x spectra of the fields, the next plane's in flight
+    // [2][ZB][nf][ldx] x spectra of the fields, the next plane's in flight
     cpx<T>* xs = reinterpret_cast<cpx<T>*>(
-        (reinterpret_cast<uintptr_t>(buf + (size_t)min(group, nrow) * (lay.at(0, 1) - lay.at(0, 0))) + 15) &
+        (reinterpret_cast<uintptr_t>(buf + (size_t)ZB * min(group, nrow) * (lay.at(0, 1) - lay.at(0, 0))) + 15) &
         ~(uintptr_t)15);                                                      // 16-byte aligned
     for (int e = threadIdx.x; e < 3 * M; e += 256) stw[e] = e < M ? twm[e] : twn[e - M];
     twm = stw;
     twn = stw + M;
     __syncthreads();
-    const int z = bid.x;
+    const int z0 = bid.x * ZB;
     const int jb = jlo + bid.y * chunk;
     const int je = min(jb + chunk - 1, jhi);
     if (jb > jhi) return;                                 // batched form: past this instance's planes
@@ -237,12 +247,13 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
     auto slot = [&](int j) { return (j - (jb - 1)) % RING; };
     constexpr int CPC = 16 / (int)sizeof(cpx<T>);      // complex numbers per 16-byte copy
     auto stage = [&](int Jn) {
-        cpx<T>* dst = xs + (size_t)(Jn & 1) * nf * d.ldx;
+        cpx<T>* dst = xs + (size_t)(Jn & 1) * ZB * nf * d.ldx;
         const int nch = d.ldx / CPC;
-        for (int e = threadIdx.x; e < nf * nch; e += 256) {
-            const int f = e / nch, q = e % nch;
-            cp_async16(dst + (size_t)f * d.ldx + q * CPC,
-                       X + (size_t)f * xf + (size_t)Jn * xrow + (size_t)z * d.ldx + q * CPC);
+        for (int e = threadIdx.x; e < ZB * nf * nch; e += 256) {
+            const int zz = e / (nf * nch), rem = e % (nf * nch);
+            const int f = rem / nch, q = rem % nch;
+            cp_async16(dst + ((size_t)zz * nf + f) * d.ldx + q * CPC,
+                       X + (size_t)f * xf + (size_t)Jn * xrow + (size_t)(z0 + zz) * d.ldx + q * CPC);
         }
         cp_async_commit();
     };
@@ -274,11 +285,13 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
             const int nr = min(group, r1 - c0);
             // ---- fill: conjugated half spectra of the fields, products ----
             const int nfill = max(0, min(nf, c0 + nr) - c0);        // inverse rows in this chunk
-            for (int e = threadIdx.x; e < nfill * M; e += 256) {
-                const int r = e / M, k = e % M;
-                const cpx<T>* xr = xs + ((size_t)(J & 1) * nf + c0 + r) * d.ldx;
-                fill_real_inverse(buf, lay, r, xr, M, d.nkx, twn, k);
-                buf[lay.at(k, r)].y = -buf[lay.at(k, r)].y;
+            // buffer row of (z-row zz, row r of this chunk): zz * nr + r
+            for (int e = threadIdx.x; e < ZB * nfill * M; e += 256) {
+                const int zz = e / (nfill * M), rem = e % (nfill * M);
+                const int r = rem / M, k = rem % M, row = zz * nr + r;
+                const cpx<T>* xr = xs + (((size_t)(J & 1) * ZB + zz) * nf + c0 + r) * d.ldx;
+                fill_real_inverse(buf, lay, row, xr, M, d.nkx, twn, k);
+                buf[lay.at(k, row)].y = -buf[lay.at(k, row)].y;
             }
             const int p0 = max(c0, nf) - nf, p1 = c0 + nr - nf;       // products p0..p1-1 here
             if (p1 > p0) {
@@ -292,7 +305,9 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
                 const T m1m = smean[sm][0], m1 = smean[s0][0], m1p = smean[sp][0];
                 const T m2m = smean[sm][1], m2 = smean[s0][1], m2p = smean[sp][1];
                 const T m3m = smean[sm][2], m3 = smean[s0][2], m3p = smean[sp][2];
-                for (int x = threadIdx.x; x < nx; x += 256) {
+                for (int ex = threadIdx.x; ex < ZB * nx; ex += 256) {
+                    const int zz = ex / nx, x = ex % nx;
+                    const T* ring = ring0 + ringz * zz;
                     const T* r_m = ring + (size_t)sm * nf * nx + x;
                     const T* r_c = ring + (size_t)s0 * nf * nx + x;
                     const T* r_p = ring + (size_t)sp * nf * nx + x;
@@ -312,7 +327,7 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
                     // (U2(j) + U2(j+1))^2/4 - (U2(j) + U2(j-1))^2/4, over DY(j)
                     const T s1 = u2 + u2p, s2 = u2 + u2m, S1 = m2 + m2p, S2 = m2 + m2m;
                     v[7] = T(0.25) * (s1 * (s1 + T(2) * S1) - s2 * (s2 + T(2) * S2)) * idy;
-                    const int eoff = 2 * lay.at(x >> 1, 0) + (x & 1);
+                    const int eoff = 2 * lay.at(x >> 1, zz * nr) + (x & 1);
                     const int rstride = 2 * (lay.at(0, 1) - lay.at(0, 0));
 #pragma unroll
                     for (int p = 0; p < 8; ++p)
@@ -333,14 +348,15 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
                 }
             }
             __syncthreads();
-            row_fft<T, MC, -1>(buf, nr, lay, pm, twm);
+            row_fft<T, MC, -1, ZB>(buf, ZB * nr, lay, pm, twm);
             // ---- unpack the fields of plane J, write the products of jp --------
             if (nfill > 0) {
                 const int sl = slot(J);
-                for (int e = threadIdx.x; e < nfill * M; e += 256) {
-                    const int r = e / M, m = e % M;
-                    const cpx<T> v = buf[lay.at(m, r)];
-                    T* dst = ring + ((size_t)sl * nf + c0 + r) * nx + 2 * m;
+                for (int e = threadIdx.x; e < ZB * nfill * M; e += 256) {
+                    const int zz = e / (nfill * M), rem = e % (nfill * M);
+                    const int r = rem / M, m = rem % M;
+                    const cpx<T> v = buf[lay.at(m, zz * nr + r)];
+                    T* dst = ring0 + ringz * zz + ((size_t)sl * nf + c0 + r) * nx + 2 * m;
                     dst[0] = v.x;
                     dst[1] = -v.y;
                 }
@@ -349,8 +365,9 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
                 // every product is in this batch (N_TH <= 1): one thread per kx
                 // extracts each product spectrum once and forms the 2 outputs of
                 // every field (field_sources)
-                for (int k = threadIdx.x; k < d.ldx; k += 256) {
-                    cpx<T>* yk = Y + (size_t)jp * xrow + (size_t)z * d.ldx + k;
+                for (int ek = threadIdx.x; ek < ZB * d.ldx; ek += 256) {
+                    const int zz = ek / d.ldx, k = ek % d.ldx;
+                    cpx<T>* yk = Y + (size_t)jp * xrow + (size_t)(z0 + zz) * d.ldx + k;
                     if (k > d.nkx) {
                         for (int q = 0; q < 2 * nf; ++q) yk[(size_t)q * xf] = mk<T>(0, 0);
                         continue;
@@ -361,7 +378,7 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
                     const int ok = lay.at(k, 0), om = lay.at(km, 0);
                     const int rs = lay.at(0, 1) - lay.at(0, 0);
                     auto X = [&](int p) -> cpx<T> {
-                        const int row = (nf + p - c0) * rs;
+                        const int row = (zz * nr + nf + p - c0) * rs;
                         const cpx<T> zk = buf[row + ok], zm = buf[row + om];
                         const cpx<T> E = mk<T>(zk.x + zm.x, zk.y - zm.y);
                         const cpx<T> O = mk<T>(zk.y + zm.y, zm.x - zk.x);
@@ -385,27 +402,28 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
                 // outputs of field f: 2f = ikx*Pa + Pflux, 2f+1 = Pz (field_sources);
                 // an output whose sources span two batches is completed by adding to
                 // what the earlier batch stored
-                for (int e = threadIdx.x; e < nf * d.ldx; e += 256) {
+                for (int e3 = threadIdx.x; e3 < ZB * nf * d.ldx; e3 += 256) {
+                    const int zz = e3 / (nf * d.ldx), e = e3 % (nf * d.ldx);
                     const int f = e / d.ldx, k = e % d.ldx;
                     int sp[2];
                     bool sx[2];
                     field_sources(2 * f, sp, sx);
                     const int pz = field_pz(f);
-                    cpx<T>* ya = Y + (size_t)(2 * f) * xf + (size_t)jp * xrow + (size_t)z * d.ldx + k;
+                    cpx<T>* ya = Y + (size_t)(2 * f) * xf + (size_t)jp * xrow + (size_t)(z0 + zz) * d.ldx + k;
                     const bool ina = sp[0] >= p0 && sp[0] < p1, inf = sp[1] >= p0 && sp[1] < p1;
                     if (ina || inf) {
                         cpx<T> v = mk<T>(0, 0);
                         if (ina) {
-                            const cpx<T> x = extract_real_forward(buf, lay, nf + sp[0] - c0, M, d.nkx, twn, k, inv_nx);
+                            const cpx<T> x = extract_real_forward(buf, lay, zz * nr + nf + sp[0] - c0, M, d.nkx, twn, k, inv_nx);
                             const T K = (T)kxw[k];
                             v = mk<T>(-K * x.y, K * x.x);
                         }
-                        if (inf) v = v + extract_real_forward(buf, lay, nf + sp[1] - c0, M, d.nkx, twn, k, inv_nx);
+                        if (inf) v = v + extract_real_forward(buf, lay, zz * nr + nf + sp[1] - c0, M, d.nkx, twn, k, inv_nx);
                         if ((!ina && sp[0] < p0) || (!inf && sp[1] < p0)) v = v + *ya;
                         *ya = v;
                     }
                     if (pz >= p0 && pz < p1)
-                        ya[xf] = extract_real_forward(buf, lay, nf + pz - c0, M, d.nkx, twn, k, inv_nx);
+                        ya[xf] = extract_real_forward(buf, lay, zz * nr + nf + pz - c0, M, d.nkx, twn, k, inv_nx);
                 }
             }
             __syncthreads();
@@ -413,7 +431,7 @@ __device__ __forceinline__ void products_body(const Dims& d, const cpx<T>* __res
     }
 }
 
-template <typename T, int MC>
+template <typename T, int MC, int ZB>
 __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __restrict__ X,
                                                      cpx<T>* __restrict__ Y, int jlo, int jhi, int chunk,
                                                      int group, const double* __restrict__ dy,
@@ -422,19 +440,19 @@ __global__ void __launch_bounds__(256, 2) k_products(Dims d, const cpx<T>* __res
                                                      const cpx<T>* __restrict__ twm,
                                                      const cpx<T>* __restrict__ twn,
                                                      const double2* __restrict__ means, size_t means_fs) {
-    products_body<T, MC>(d, X, Y, jlo, jhi, chunk, group, dy, dyf, kxw, pm, twm, twn, means, means_fs, blockIdx);
+    products_body<T, MC, ZB>(d, X, Y, jlo, jhi, chunk, group, dy, dyf, kxw, pm, twm, twn, means, means_fs, blockIdx);
 }
 
 // Batched form: instance blockIdx.z of a group of equal shape.
-template <typename T, int MC>
+template <typename T, int MC, int ZB>
 __global__ void __launch_bounds__(256, 2) k_products_b(const InstPtrs* __restrict__ ip, Dims d, int jhi, int chunk,
                                                        int group, FftPlan pm, const cpx<T>* __restrict__ twm,
                                                        const cpx<T>* __restrict__ twn, int mean_split,
                                                        size_t means_fs) {
     const InstPtrs q = ip[blockIdx.z];
-    products_body<T, MC>(d, reinterpret_cast<const cpx<T>*>(q.xb), reinterpret_cast<cpx<T>*>(q.yb), q.jlo_prod, jhi,
-                         chunk, group, q.dy, q.dyf, q.kx, pm, twm, twn, mean_split ? q.cu : nullptr, means_fs,
-                         make_uint3(blockIdx.x, blockIdx.y, 0));
+    products_body<T, MC, ZB>(d, reinterpret_cast<const cpx<T>*>(q.xb), reinterpret_cast<cpx<T>*>(q.yb), q.jlo_prod,
+                             jhi, chunk, group, q.dy, q.dyf, q.kx, pm, twm, twn, mean_split ? q.cu : nullptr,
+                             means_fs, make_uint3(blockIdx.x, blockIdx.y, 0));
 }
 
 // ---------------------------------------------------------------------------
@@ -619,6 +637,17 @@ int products_group(int nx) {
     return g > PROD_G ? PROD_G : g;
 }
 
+// Dynamic shared memory of a products block of zb z-rows: rings, twiddles,
+// transform rows, staged x spectra (products_body's carve-up).
+template <typename T>
+size_t products_smem(const Dims& d, int group, int zb) {
+    const int M = d.nx / 2;
+    const int rows = group < d.nf + d.np ? group : d.nf + d.np;
+    return zb * (sizeof(T) * (size_t)RING * d.nf * d.nx + sizeof(cpx<T>) * (size_t)rows * row_pitch(M) +
+                 sizeof(cpx<T>) * 2 * (size_t)d.nf * d.ldx) +
+           sizeof(cpx<T>) * 3 * (size_t)M + 16;
+}
+
 template <typename T>
 cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int jhi, int chunk,
                             const double* dy, const double* dyf, const double* kx, const FftPlan& pm,
@@ -628,21 +657,23 @@ cudaError_t launch_products(const Dims& d, const void* X, void* Y, int jlo, int 
     const int group = products_group(d.nx);
     if (group < 1) return cudaErrorInvalidValue;
     const int M = d.nx / 2;
-    const int rows = group < d.nf + d.np ? group : d.nf + d.np;
-    const size_t smem = sizeof(T) * (size_t)RING * d.nf * d.nx + sizeof(cpx<T>) * (size_t)rows * row_pitch(M) +
-                        sizeof(cpx<T>) * 3 * (size_t)M + sizeof(cpx<T>) * 2 * (size_t)d.nf * d.ldx + 16;
     const int nchunks = (jhi - jlo + chunk) / chunk;
-    dim3 grid(d.nz, nchunks);
-    auto go = [&](auto kern) {
+    auto go = [&](auto kern, int zb) {
+        const size_t smem = products_smem<T>(d, group, zb);
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, 256, smem, st>>>(d, (const cpx<T>*)X, (cpx<T>*)Y, jlo, jhi, chunk, group, dy, dyf, kx, pm,
-                                      (const cpx<T>*)twm, (const cpx<T>*)twn, means, means_fstride);
+        kern<<<dim3(d.nz / zb, nchunks), 256, smem, st>>>(d, (const cpx<T>*)X, (cpx<T>*)Y, jlo, jhi, chunk, group, dy,
+                                                          dyf, kx, pm, (const cpx<T>*)twm, (const cpx<T>*)twn, means,
+                                                          means_fstride);
     };
     switch (M) {
-#define CASE(N) case N: go(k_products<T, N>); break;
+#define CASE(N)                                                                   \
+    case N:                                                                       \
+        if (d.nz % products_zb<T, N>() == 0) go(k_products<T, N, products_zb<T, N>()>, products_zb<T, N>()); \
+        else go(k_products<T, N, 1>, 1);                                          \
+        break;
         DGPU_M_LIST(CASE)
 #undef CASE
-        default: go(k_products<T, 0>); break;
+        default: go(k_products<T, 0, 1>, 1); break;
     }
     return cudaGetLastError();
 }
@@ -702,20 +733,21 @@ cudaError_t launch_products_b(const Dims& d, const InstPtrs* ip, int ninst, int 
     const int group = products_group(d.nx);
     if (group < 1) return cudaErrorInvalidValue;
     const int M = d.nx / 2;
-    const int rows = group < d.nf + d.np ? group : d.nf + d.np;
-    const size_t smem = sizeof(T) * (size_t)RING * d.nf * d.nx + sizeof(cpx<T>) * (size_t)rows * row_pitch(M) +
-                        sizeof(cpx<T>) * 3 * (size_t)M + sizeof(cpx<T>) * 2 * (size_t)d.nf * d.ldx + 16;
-    dim3 grid(d.nz, (jhi - jlo_min + chunk) / chunk, ninst);
-    auto go = [&](auto kern) {
+    auto go = [&](auto kern, int zb) {
+        const size_t smem = products_smem<T>(d, group, zb);
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, 256, smem, st>>>(ip, d, jhi, chunk, group, pm, (const cpx<T>*)twm, (const cpx<T>*)twn, mean_split,
-                                      means_fstride);
+        kern<<<dim3(d.nz / zb, (jhi - jlo_min + chunk) / chunk, ninst), 256, smem, st>>>(
+            ip, d, jhi, chunk, group, pm, (const cpx<T>*)twm, (const cpx<T>*)twn, mean_split, means_fstride);
     };
     switch (M) {
-#define CASE(N) case N: go(k_products_b<T, N>); break;
+#define CASE(N)                                                                   \
+    case N:                                                                       \
+        if (d.nz % products_zb<T, N>() == 0) go(k_products_b<T, N, products_zb<T, N>()>, products_zb<T, N>()); \
+        else go(k_products_b<T, N, 1>, 1);                                        \
+        break;
         DGPU_M_LIST(CASE)
 #undef CASE
-        default: go(k_products_b<T, 0>); break;
+        default: go(k_products_b<T, 0, 1>, 1); break;
     }
     return cudaGetLastError();
 }
