@@ -705,18 +705,21 @@ __device__ __forceinline__ void colpart_body(const ColArgs& A, const TN* __restr
     if (bad && A.nan_flag) atomicOr(A.nan_flag, 1);
 }
 
+// Blocks per SM: three at up to 5 rows per lane (80 registers; the few rows
+// of a small NY leave the phases short, so more pairs in flight pay), two
+// at 9 and 17 rows, whose solve holds more values.
 template <int NW, int RC, typename TN, bool PB>
-__global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 1)
+__global__ void __launch_bounds__(32 * NW, NW == 8 ? (RC <= 5 ? 3 : 2) : 1)
 k_colpart(ColArgs A, const TN* __restrict__ nl, const double* __restrict__ tabs, int tstride) {
     colpart_body<NW, RC, TN, PB>(A, nl, tabs, tstride, blockIdx.x);
 }
 
 // Batched form: instance blockIdx.y of a group of equal shape.
 template <int NW, int RC, typename TN, bool PB>
-__global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 1)
+__global__ void __launch_bounds__(32 * NW, NW == 8 ? (RC <= 5 ? 3 : 2) : 1)
 k_colpart_b(const ColJob* __restrict__ jobs, int tstride) {
     const ColJob& j = jobs[blockIdx.y];
-    const ColArgs A = j.A;
+    const ColArgs& A = j.A;     // read in place: a copy would sit in every thread's stack
     colpart_body<NW, RC, TN, PB>(A, reinterpret_cast<const TN*>(j.nl), j.tabs, tstride, blockIdx.x);
 }
 
