@@ -1757,6 +1757,10 @@ cudaError_t batch_group_step(BatchGroup& g) {
     const void* twn = f ? h0->twn_f : h0->twn_d;
     const void* twm = f ? h0->twm_f : h0->twm_d;
     const void* twz = f ? h0->twz_f : h0->twz_d;
+    // The groups of a batch fill the GPU together, so the block-wide products
+    // kernel takes chunks of at least 32 planes: a chunk tuned for one
+    // instance's latency recomputes more halo planes than a batch can spare.
+    const int bchunk = h0->prod_chunk > 32 ? h0->prod_chunk : 32;
     cudaError_t e = cudaSuccess;
     for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
         e = launch_zinv_b<T>(d, g.d_ip, n, h0->s_field, h0->x_field, h0->pz, twz, g.st, f ? 1 : 0);
@@ -1764,7 +1768,7 @@ cudaError_t batch_group_step(BatchGroup& g) {
         if (f && products_hw_supported(d))
             e = launch_products_hw_b(d, g.d_ip, n, g.jlo_min, d.ny, h0->prod_chunk, twm, twn, g.st, h0->s_field);
         else
-            e = launch_products_b<T>(d, g.d_ip, n, g.jlo_min, d.ny, h0->prod_chunk, h0->pm, twm, twn, g.st, f ? 1 : 0,
+            e = launch_products_b<T>(d, g.d_ip, n, g.jlo_min, d.ny, bchunk, h0->pm, twm, twn, g.st, f ? 1 : 0,
                                      h0->s_field);
         if (e == cudaSuccess) e = launch_zfwd_nl_b<T>(d, g.d_ip, n, g.jlo_min, d.ny, h0->zf_planes, h0->pz, twz, g.st);
         if (e == cudaSuccess) e = launch_colpart_b<cpx<T>>(d, g.d_col + (size_t)r * n, n, h0->pb, g.st);
